@@ -1,0 +1,222 @@
+/*
+ * poisson_b200 — C ABI of the B200 (sm_100a) screened-Poisson reconstruction kernels.
+ *
+ * Drop-in boundary for mojo-poissonrecon's native library.  The reference
+ * binds eleven `mpr_*` symbols through ctypes (python/mojo_poissonrecon/
+ * _lib.py:20-32) over caller-owned NumPy buffers.  Every function here keeps
+ * the argument order and meaning of the symbol it replaces, with four changes
+ * that a GPU boundary needs:
+ *
+ *   - buffers are DEVICE pointers (e.g. torch.Tensor.data_ptr()), C-contiguous,
+ *     [z][y][x] row-major grids of side n (index (z*n + y)*n + x);
+ *   - each call is asynchronous on the given cudaStream_t (passed as void*;
+ *     NULL = the legacy default stream) and returns an int status (PB_OK = 0);
+ *   - values the reference returns (accepted count, residual norm, iso-value,
+ *     vertex/face counts) are written to a DEVICE int64/double the caller
+ *     passes, so no call synchronises the host;
+ *   - functions that need scratch take a caller-owned device workspace whose
+ *     size the matching *_workspace_size() reports.  Like the reference
+ *     (README.md:84-95) the library never allocates or retains memory.
+ *
+ * Errors: a non-zero status leaves a message in pb_last_error() (thread-local).
+ * Arguments are validated on the host before any launch (PB_ERR_INVALID).
+ */
+#ifndef POISSON_B200_H
+#define POISSON_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    PB_OK = 0,
+    PB_ERR_INVALID = 1,   /* bad size, null pointer, unsupported argument */
+    PB_ERR_CUDA = 2,      /* a CUDA launch or API call failed */
+    PB_ERR_WORKSPACE = 3, /* workspace missing or smaller than *_workspace_size() */
+    PB_ERR_DEVICE = 4,    /* no usable sm_100 device */
+    PB_ERR_TIMEOUT = 5    /* a bounded wait gave up */
+};
+
+/* Message of the last failing call on this host thread ("" if none). */
+const char *pb_last_error(void);
+/* ABI version, major*10000 + minor*100 + patch. */
+int pb_version(void);
+
+/* Replaces mpr_parallel_init (_lib.py:21; capi.mojo:36-38): selects `device`
+ * and checks it is an sm_100 part.  Optional; every call works without it. */
+int pb_init(int device);
+
+/* ---- octree (a1, a2) ------------------------------------------------------ */
+
+/* mpr_octree_codes_f64 (_lib.py:22; capi.mojo:62-99): codes[i*(depth+1)+l] is
+ * point i's Morton child-index chain down to level l (codes[i*(depth+1)] = 0).
+ * 0 <= depth <= 19.  Bit-exact. */
+int pb_octree_codes_f64(const double *points, int64_t point_count, int64_t depth,
+                        int64_t *codes, void *stream);
+
+/* build_octree (core.py:86-127) on the device, in two phases sharing one
+ * workspace.  pb_octree_count sorts the leaf codes and writes the number of
+ * distinct codes per level to level_counts[0..depth] (device int64).  After
+ * the caller has read them and allocated node_count = sum(level_counts)
+ * entries per node array, pb_octree_emit fills the breadth-first flat octree:
+ * depth, morton, parent (-1 at the root), child_start (-1 for leaves),
+ * child_count, and point_leaf[point_count].  Bit-exact with the reference.
+ * 1 <= point_count, 0 <= depth <= 19. */
+size_t pb_octree_workspace_size(int64_t point_count, int64_t depth);
+int pb_octree_count(const double *points, int64_t point_count, int64_t depth,
+                    int64_t *level_counts, void *workspace, size_t workspace_bytes, void *stream);
+int pb_octree_emit(int64_t point_count, int64_t depth, const int64_t *level_counts,
+                   int64_t node_count, int64_t *node_depth, int64_t *morton, int64_t *parent,
+                   int64_t *child_start, int64_t *child_count, int64_t *point_leaf,
+                   void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---- splat and assembly (a5-a7) ----------------------------------------- */
+
+/* mpr_splat_f64 (_lib.py:23; capi.mojo:104-224): adds the two-pass trilinear
+ * splat into density, screen, vx, vy, vz (callers zero them first, as the
+ * reference does) and writes the accepted-sample count to *accepted (device).
+ * Each grid node sums its contributions in point order, exactly as the serial
+ * reference does, so the grids are bit-identical to it.  n >= 2,
+ * n^3 < 2^31, 8*point_count < 2^32. */
+size_t pb_splat_workspace_size(int64_t point_count, int64_t n);
+int pb_splat_f64(const double *points, const double *normals, int64_t point_count, int64_t n,
+                 int64_t confidence, double *density, double *vx, double *vy, double *vz,
+                 double *screen, double samples_per_node, int64_t *accepted,
+                 void *workspace, size_t workspace_bytes, void *stream);
+
+/* mpr_assemble_f64 (_lib.py:24; capi.mojo:228-279):
+ * rhs = -div(V) + point_weight * screen * (n-1)^2 * target_value. Bit-exact. */
+int pb_assemble_f64(const double *vx, const double *vy, const double *vz, const double *screen,
+                    double *rhs, int64_t n, double point_weight, double target_value,
+                    void *stream);
+
+/* ---- multigrid operators, FP64 (a9-a12) ------------------------------------ */
+
+/* mpr_relax_f64 (_lib.py:25; capi.mojo:310-410): `iterations` red-black
+ * Gauss-Seidel sweeps in place.  Bit-exact. */
+int pb_relax_f64(double *solution, const double *rhs, const double *screen, int64_t n,
+                 double point_weight, int64_t iterations, void *stream);
+
+/* mpr_residual_f64 (_lib.py:26; capi.mojo:474-553): residual = rhs - A x
+ * (bit-exact) and *norm = ||residual||_2 (device; summation order differs
+ * from the serial reference by rounding only). */
+size_t pb_residual_workspace_size(int64_t n);
+int pb_residual_f64(const double *solution, const double *rhs, const double *screen,
+                    double *residual, int64_t n, double point_weight, double *norm,
+                    void *workspace, size_t workspace_bytes, void *stream);
+
+/* ||values||_2 into *norm (device) — the scale of the relative residual
+ * ||rhs - A x|| / ||rhs|| that the tolerance-driven solves stop on (the
+ * reference runs a fixed number of cycles and has no such loop). */
+int pb_norm_f64(const double *values, int64_t count, double *norm, void *workspace,
+                size_t workspace_bytes, void *stream);
+
+/* mpr_restrict_f64 (_lib.py:27; capi.mojo:557-673): boundary-normalised full
+ * weighting onto coarse_n = (fine_n+1)/2.  Bit-exact. */
+int pb_restrict_f64(const double *fine, double *coarse, int64_t fine_n, void *stream);
+
+/* mpr_prolong_add_f64 (_lib.py:28; capi.mojo:677-742): fine += trilinear(coarse).
+ * Bit-exact. */
+int pb_prolong_add_f64(const double *coarse, double *fine, int64_t fine_n, void *stream);
+
+/* ---- iso-value (a14) -------------------------------------------------------- */
+
+/* mpr_iso_value_f64 (_lib.py:29; capi.mojo:746-795): *iso (device) = weighted
+ * mean of the trilinear field at the samples (0 when the weights sum to 0). */
+size_t pb_iso_value_workspace_size(int64_t point_count);
+int pb_iso_value_f64(const double *field, const double *points, const double *normals,
+                     int64_t point_count, int64_t n, int64_t confidence, double *iso,
+                     void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---- dual contouring (a15-a17) ------------------------------------------------ */
+
+/* mpr_dual_vertices_f64 (_lib.py:30; capi.mojo:841-1041).  capacity <= 0:
+ * count the active cells into *count (device); cell_map, vertices and
+ * vertex_density are not touched.  capacity > 0: cell_map[(n-1)^3] gets the
+ * vertex id of each active cell in z,y,x order (-1 for inactive cells; active
+ * cells past `capacity` keep 0, as in the reference), the first `capacity`
+ * vertices and their densities are written, and *count gets the total.
+ * Topology and coordinates are bit-exact.
+ * The _isoptr variant reads the iso-value from device memory instead. */
+size_t pb_dual_workspace_size(int64_t n);
+int pb_dual_vertices_f64(const double *field, const double *density, int64_t n, double iso,
+                         int64_t *cell_map, double *vertices, double *vertex_density,
+                         int64_t capacity, int64_t *count, void *workspace,
+                         size_t workspace_bytes, void *stream);
+int pb_dual_vertices_f64_isoptr(const double *field, const double *density, int64_t n,
+                                const double *iso, int64_t *cell_map, double *vertices,
+                                double *vertex_density, int64_t capacity, int64_t *count,
+                                void *workspace, size_t workspace_bytes, void *stream);
+
+/* mpr_dual_faces_f64 (_lib.py:31; capi.mojo:1076-1129): two triangles per
+ * sign-changing interior edge (x-edges, then y-edges, then z-edges, each in
+ * z,y,x order); faces are written while 2 more fit in `capacity`; *count
+ * (device) gets the total.  Bit-exact. */
+int pb_dual_faces_f64(const double *field, int64_t n, double iso, const int64_t *cell_map,
+                      int64_t *faces, int64_t capacity, int64_t *count, void *workspace,
+                      size_t workspace_bytes, void *stream);
+int pb_dual_faces_f64_isoptr(const double *field, int64_t n, const double *iso,
+                             const int64_t *cell_map, int64_t *faces, int64_t capacity,
+                             int64_t *count, void *workspace, size_t workspace_bytes,
+                             void *stream);
+
+/* ---- FP32 inner multigrid for FP64 defect correction ----------------------------
+ * No counterpart in the reference, which solves in FP64 only (capi.mojo:310-742).
+ * FP32 level arrays use a padded layout: side n with a zero ghost layer on
+ * every face, x offset 4, row pitch P = pb_level_geometry(n):
+ *   index(x, y, z) = ((z+1)*(n+2) + (y+1))*P + (x+4),   x, y, z in [-1, n].
+ * Callers allocate them zero-filled; kernels write interior nodes only. */
+int pb_level_geometry(int64_t n, int64_t *pitch, int64_t *padded_count);
+/* D = (degree + pw*screen)*(n-1)^2 and 1/D per node from the dense FP64 screen. */
+int pb_level_setup_f32(const double *screen, int64_t n, double point_weight, float *D, float *invD,
+                       void *stream);
+/* r32 = b - A x in FP64 (dense x, b, screen; r32 padded), *norm2 = ||b - A x||^2.
+ * With e != NULL the iterate is first updated: x_new = x_old + e (written). */
+size_t pb_defect_workspace_size(int64_t n);
+int pb_defect_f64(const double *x_old, const float *e, double *x_new, const double *rhs,
+                  const double *screen, int64_t n, double point_weight, float *r32, double *norm2,
+                  void *workspace, size_t workspace_bytes, void *stream);
+/* One red-black Gauss-Seidel sweep (colour 0 then colour 1), out of place.
+ * mode 0: from e_in; 1: from zero (e_in unused); 2: from e_in + trilinear
+ * prolongation of `coarse` (side (n+1)/2).  n = 2^k + 1. */
+int pb_sweep_f32(const float *e_in, float *e_out, const float *rhs, const float *invD,
+                 const float *coarse, int64_t n, int64_t mode, int64_t z_chunk, void *stream);
+int pb_residual_f32(const float *e, const float *rhs, const float *D, float *residual, int64_t n,
+                    void *stream);
+int pb_restrict_f32(const float *fine, float *coarse, int64_t fine_n, void *stream);
+/* The V-cycle below a level of side <= 17 in one block: count levels, finest
+ * first (host arrays of device pointers); rhs[0] holds the right-hand side,
+ * e[0] receives the correction. */
+int pb_coarse_cycle_f32(int64_t count, const int64_t *sizes, float *const *e, float *const *rhs,
+                        float *const *res, const float *const *D, const float *const *invD,
+                        int64_t pre, int64_t post, int64_t coarsest_sweeps, void *stream);
+
+/* ---- host-orchestration helpers (core.py steps done on the device) ---------- */
+
+/* core.py:73-83 + :377-385: keep the rows of (points, normals) with a finite
+ * point and a finite non-zero normal, in order, into out_points/out_normals;
+ * *kept (device int64) = their number.  scale > 0: also map the kept points
+ * into the unit cube in place, map[0..2] = origin, map[3] = width (device).
+ * Bit-identical to the reference's NumPy arithmetic. */
+size_t pb_prepare_workspace_size(int64_t point_count);
+int pb_prepare_points_f64(const double *points, const double *normals, int64_t point_count, double scale,
+                          double *out_points, double *out_normals, int64_t *kept, double *map,
+                          void *workspace, size_t workspace_bytes, void *stream);
+/* core.py:225-227: *outside (device int, zeroed by the caller) = 1 if any
+ * coordinate lies outside [0, 1]. */
+int pb_unit_cube_check_f64(const double *points, int64_t point_count, int *outside, void *stream);
+/* core.py:425: vertices = vertices * map[3] + map[0..2]. */
+int pb_map_vertices_f64(double *vertices, int64_t vertex_count, const double *map, void *stream);
+/* core.py:255 (density /= samples_per_node), :269 (screen * 4), :270/:287 (fill). */
+int pb_divide_f64(double *values, int64_t count, double divisor, void *stream);
+int pb_scale_f64(double *values, int64_t count, double factor, void *stream);
+int pb_fill_f64(double *values, int64_t count, double value, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* POISSON_B200_H */

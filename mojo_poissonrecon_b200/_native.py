@@ -1,0 +1,141 @@
+"""ctypes binding of libpoisson_b200.so (the sm_100a C ABI in include/poisson_b200.h).
+
+This is the GPU counterpart of the reference's loader
+(python/mojo_poissonrecon/_lib.py): a signature table, a lazy `lib()`, and the
+buffer guards.  Buffers are CUDA torch tensors passed by `data_ptr()`; every
+call is queued on the current torch CUDA stream.  There is no CPU fallback:
+without the built library or a CUDA device every entry point raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import torch
+
+from . import buildlib as _build
+
+I = ctypes.c_int64
+F = ctypes.c_double
+P = ctypes.c_void_p
+S = ctypes.c_size_t
+C = ctypes.c_int
+
+_SIGNATURES = {
+    "pb_last_error": ([], ctypes.c_char_p),
+    "pb_version": ([], C),
+    "pb_init": ([C], C),
+    "pb_octree_codes_f64": ([P, I, I, P, P], C),
+    "pb_octree_workspace_size": ([I, I], S),
+    "pb_octree_count": ([P, I, I, P, P, S, P], C),
+    "pb_octree_emit": ([I, I, P, I, P, P, P, P, P, P, P, S, P], C),
+    "pb_splat_workspace_size": ([I, I], S),
+    "pb_splat_f64": ([P, P, I, I, I, P, P, P, P, P, F, P, P, S, P], C),
+    "pb_assemble_f64": ([P, P, P, P, P, I, F, F, P], C),
+    "pb_relax_f64": ([P, P, P, I, F, I, P], C),
+    "pb_residual_workspace_size": ([I], S),
+    "pb_residual_f64": ([P, P, P, P, I, F, P, P, S, P], C),
+    "pb_norm_f64": ([P, I, P, P, S, P], C),
+    "pb_restrict_f64": ([P, P, I, P], C),
+    "pb_prolong_add_f64": ([P, P, I, P], C),
+    "pb_iso_value_workspace_size": ([I], S),
+    "pb_iso_value_f64": ([P, P, P, I, I, I, P, P, S, P], C),
+    "pb_dual_workspace_size": ([I], S),
+    "pb_dual_vertices_f64": ([P, P, I, F, P, P, P, I, P, P, S, P], C),
+    "pb_dual_vertices_f64_isoptr": ([P, P, I, P, P, P, P, I, P, P, S, P], C),
+    "pb_dual_faces_f64": ([P, I, F, P, P, I, P, P, S, P], C),
+    "pb_dual_faces_f64_isoptr": ([P, I, P, P, P, I, P, P, S, P], C),
+    "pb_scale_f64": ([P, I, F, P], C),
+    "pb_divide_f64": ([P, I, F, P], C),
+    "pb_fill_f64": ([P, I, F, P], C),
+    "pb_prepare_workspace_size": ([I], S),
+    "pb_prepare_points_f64": ([P, P, I, F, P, P, P, P, P, S, P], C),
+    "pb_unit_cube_check_f64": ([P, I, P, P], C),
+    "pb_map_vertices_f64": ([P, I, P, P], C),
+    "pb_level_geometry": ([I, P, P], C),
+    "pb_level_setup_f32": ([P, I, F, P, P, P], C),
+    "pb_defect_workspace_size": ([I], S),
+    "pb_defect_f64": ([P, P, P, P, P, I, F, P, P, P, S, P], C),
+    "pb_sweep_f32": ([P, P, P, P, P, I, I, I, P], C),
+    "pb_residual_f32": ([P, P, P, P, I, P], C),
+    "pb_restrict_f32": ([P, P, I, P], C),
+    "pb_coarse_cycle_f32": ([I, P, P, P, P, P, P, I, I, I, P], C),
+}
+
+LIBRARY_PATH = _build.LIBRARY
+_loaded: ctypes.CDLL | None = None
+
+
+class NativeError(RuntimeError):
+    """A libpoisson_b200 call returned a non-zero status."""
+
+
+def library_path() -> str:
+    return LIBRARY_PATH
+
+
+def lib() -> ctypes.CDLL:
+    """Load (building first if the in-tree library is missing) and bind the C ABI."""
+    global _loaded
+    if _loaded is None:
+        path = LIBRARY_PATH
+        if not os.path.exists(path):
+            path = _build.build()
+        cdll = ctypes.CDLL(path)
+        for name, (argtypes, restype) in _SIGNATURES.items():
+            fn = getattr(cdll, name)
+            fn.argtypes = argtypes
+            fn.restype = restype
+        _loaded = cdll
+    return _loaded
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGNATURES)
+
+
+def check(status: int, what: str = "") -> None:
+    if status != 0:
+        message = lib().pb_last_error().decode(errors="replace")
+        raise NativeError(f"{what or 'libpoisson_b200'} failed (status {status}): {message}")
+
+
+def require_cuda() -> torch.device:
+    if not torch.cuda.is_available():
+        raise RuntimeError(
+            "mojo_poissonrecon_b200 runs only on a CUDA (sm_100) device; no CUDA device is visible"
+        )
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def stream_handle(stream: torch.cuda.Stream | None = None) -> int:
+    s = torch.cuda.current_stream() if stream is None else stream
+    return int(s.cuda_stream)
+
+
+def dptr(t: torch.Tensor | None) -> int | None:
+    """Device address of a contiguous CUDA tensor (None passes through as NULL)."""
+    if t is None:
+        return None
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError("device buffers must be CUDA tensors")
+    if not t.is_contiguous():
+        raise ValueError("device buffers must be contiguous")
+    if t.dtype not in (torch.float64, torch.int64, torch.float32, torch.uint8, torch.int32):
+        raise TypeError(f"unsupported device buffer dtype {t.dtype}")
+    return t.data_ptr() or None
+
+
+class Workspace:
+    """A growable device scratch buffer reused across calls on one stream."""
+
+    def __init__(self, device: torch.device):
+        self.device = device
+        self.buffer = torch.empty(0, dtype=torch.uint8, device=device)
+
+    def get(self, nbytes: int) -> tuple[int, int]:
+        nbytes = max(int(nbytes), 256)
+        if self.buffer.numel() < nbytes:
+            self.buffer = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        return self.buffer.data_ptr(), self.buffer.numel()

@@ -1,0 +1,469 @@
+"""Screened Poisson surface reconstruction on a B200 — the drop-in public API.
+
+Same names, signatures, defaults, dataclasses, array shapes, [z, y, x] grid
+layout, error types and messages as python/mojo_poissonrecon/core.py, so code
+written against the reference runs unchanged.  Inputs may be NumPy arrays
+(as in the reference) or torch tensors (CPU, pinned or CUDA); outputs are
+NumPy arrays, or CUDA tensors with ``device_out=True``.
+
+Extensions (keyword-only, defaults keep the reference's behaviour):
+``precision`` ("fp64" | "fp32_refined"), ``tol`` (stop on the relative
+residual instead of a fixed cycle count), ``max_cycles``, ``device_out``.
+The depth cap is lifted from 8 to 10.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _native as nat
+from . import solver
+from ._convert import f64, i64
+
+MAX_DEPTH = 10
+PRECISIONS = ("fp64", "fp32_refined")
+
+
+@dataclass(frozen=True)
+class FlatOctree:
+    depth: np.ndarray
+    morton: np.ndarray
+    parent: np.ndarray
+    child_start: np.ndarray
+    child_count: np.ndarray
+    point_leaf: np.ndarray
+
+    @property
+    def node_count(self) -> int:
+        return int(self.depth.shape[0])
+
+
+@dataclass(frozen=True)
+class GridSolution:
+    field: np.ndarray
+    density: np.ndarray
+    screen: np.ndarray
+    rhs: np.ndarray
+    iso_value: float
+    residual_norm: float
+    octree: FlatOctree | None
+    cycles: int = 0
+    relative_residual: float = float("nan")
+    precision: str = "fp64"
+
+
+@dataclass(frozen=True)
+class Mesh:
+    vertices: np.ndarray
+    faces: np.ndarray
+    density: np.ndarray
+    iso_value: float = 0.0
+    residual_norm: float = 0.0
+
+    @property
+    def is_empty(self) -> bool:
+        return self.vertices.shape[0] == 0
+
+
+# ---- validation (core.py:50-83, 207-227) --------------------------------------
+
+def _points(values):
+    result = f64(values)
+    if result.ndim != 2 or result.shape[1] != 3:
+        raise ValueError("points must have shape (n, 3)")
+    return result
+
+
+def _integer_parameter(name: str, value) -> int:
+    if isinstance(value, (bool, np.bool_)) or not isinstance(value, (int, np.integer)):
+        raise TypeError(f"{name} must be an integer")
+    return int(value)
+
+
+def _finite_parameter(name: str, value) -> float:
+    try:
+        result = float(value)
+    except (TypeError, ValueError, OverflowError) as error:
+        raise TypeError(f"{name} must be a real number") from error
+    if not np.isfinite(result):
+        raise ValueError(f"{name} must be finite")
+    return result
+
+
+def _precision(value: str) -> str:
+    if value not in PRECISIONS:
+        raise ValueError(f"precision must be one of {PRECISIONS}")
+    return value
+
+
+def _tolerance(tol) -> float | None:
+    if tol is None:
+        return None
+    tol = _finite_parameter("tol", tol)
+    if tol <= 0:
+        raise ValueError("tol must be positive")
+    return tol
+
+
+class _Context:
+    """Per-call device state: the device, a workspace and the stream handle."""
+
+    def __init__(self):
+        self.device = nat.require_cuda()
+        self.lib = nat.lib()
+        self.ws = nat.Workspace(self.device)
+        self.stream = nat.stream_handle()
+
+    def check(self, status: int, what: str) -> None:
+        nat.check(status, what)
+
+
+def _to_device(array, device: torch.device) -> torch.Tensor:
+    if isinstance(array, torch.Tensor):
+        return array.to(device=device, dtype=torch.float64, non_blocking=True).contiguous()
+    return torch.from_numpy(np.ascontiguousarray(array, dtype=np.float64)).to(device, non_blocking=True)
+
+
+def _host(t: torch.Tensor, device_out: bool):
+    return t if device_out else t.cpu().numpy()
+
+
+def _prepare(ctx: _Context, points: torch.Tensor, normals: torch.Tensor, scale: float):
+    """Valid rows (core.py:73-83), optionally mapped to the unit cube (:377-385).
+    Returns (points, normals, kept, map) with the kept rows only."""
+    count = points.shape[0]
+    out_p = torch.empty_like(points)
+    out_n = torch.empty_like(normals)
+    kept = torch.empty(1, dtype=torch.int64, device=ctx.device)
+    fmap = torch.empty(4, dtype=torch.float64, device=ctx.device)
+    ptr, size = ctx.ws.get(ctx.lib.pb_prepare_workspace_size(count))
+    ctx.check(ctx.lib.pb_prepare_points_f64(points.data_ptr(), normals.data_ptr(), count, scale, out_p.data_ptr(),
+                                            out_n.data_ptr(), kept.data_ptr(), fmap.data_ptr(), ptr, size,
+                                            ctx.stream), "prepare points")
+    k = int(kept.item())
+    return out_p[:k], out_n[:k], k, fmap
+
+
+# ---- octree (core.py:86-127) ---------------------------------------------------
+
+def _octree_device(ctx: _Context, points: torch.Tensor, depth: int) -> dict:
+    count = points.shape[0]
+    L = ctx.lib
+    if count == 0:
+        z = torch.zeros(1, dtype=torch.int64, device=ctx.device)
+        m1 = torch.full((1,), -1, dtype=torch.int64, device=ctx.device)
+        return dict(depth=z, morton=z.clone(), parent=m1, child_start=m1.clone(), child_count=z.clone(),
+                    point_leaf=torch.empty(0, dtype=torch.int64, device=ctx.device))
+    ws = nat.Workspace(ctx.device)  # kept alive across the two phases
+    ptr, size = ws.get(L.pb_octree_workspace_size(count, depth))
+    counts = torch.empty(depth + 1, dtype=torch.int64, device=ctx.device)
+    ctx.check(L.pb_octree_count(points.data_ptr(), count, depth, counts.data_ptr(), ptr, size, ctx.stream),
+              "octree count")
+    nodes = int(counts.sum().item())
+    arrays = {k: torch.empty(nodes, dtype=torch.int64, device=ctx.device)
+              for k in ("depth", "morton", "parent", "child_start", "child_count")}
+    arrays["point_leaf"] = torch.empty(count, dtype=torch.int64, device=ctx.device)
+    ctx.check(L.pb_octree_emit(count, depth, counts.data_ptr(), nodes, arrays["depth"].data_ptr(),
+                               arrays["morton"].data_ptr(), arrays["parent"].data_ptr(),
+                               arrays["child_start"].data_ptr(), arrays["child_count"].data_ptr(),
+                               arrays["point_leaf"].data_ptr(), ptr, size, ctx.stream), "octree emit")
+    return arrays
+
+
+def _octree_out(arrays: dict, device_out: bool) -> FlatOctree:
+    return FlatOctree(*(_host(arrays[k], device_out) for k in
+                        ("depth", "morton", "parent", "child_start", "child_count", "point_leaf")))
+
+
+def build_octree(points, depth: int = 6, *, device_out: bool = False) -> FlatOctree:
+    """Build a compact breadth-first Morton octree over unit-cube points."""
+    points = _points(points)
+    depth = _integer_parameter("depth", depth)
+    if not 0 <= depth <= 19:
+        raise ValueError("depth must be between 0 and 19")
+    ctx = _Context()
+    dpts = _to_device(points, ctx.device)
+    if dpts.shape[0]:
+        bad = (~torch.isfinite(dpts)).any() | (dpts < 0).any() | (dpts > 1).any()
+        if bool(bad):
+            raise ValueError("octree points must be finite and inside [0, 1]^3")
+    return _octree_out(_octree_device(ctx, dpts, depth), device_out)
+
+
+# ---- solve (core.py:196-306) ---------------------------------------------------
+
+def _splat_assemble(ctx: _Context, points: torch.Tensor, normals: torch.Tensor, depth: int, point_weight: float,
+                    confidence: bool, samples_per_node: float):
+    L = ctx.lib
+    n = (1 << depth) + 1
+    count = points.shape[0]
+    grids = {k: torch.zeros((n, n, n), dtype=torch.float64, device=ctx.device)
+             for k in ("density", "vx", "vy", "vz", "screen", "rhs")}
+    accepted = torch.zeros(1, dtype=torch.int64, device=ctx.device)
+    if count:
+        ptr, size = ctx.ws.get(L.pb_splat_workspace_size(count, n))
+        ctx.check(L.pb_splat_f64(points.data_ptr(), normals.data_ptr(), count, n, int(confidence),
+                                 grids["density"].data_ptr(), grids["vx"].data_ptr(), grids["vy"].data_ptr(),
+                                 grids["vz"].data_ptr(), grids["screen"].data_ptr(), samples_per_node,
+                                 accepted.data_ptr(), ptr, size, ctx.stream), "splat")
+        ctx.check(L.pb_divide_f64(grids["density"].data_ptr(), n ** 3, samples_per_node, ctx.stream), "divide")
+        ctx.check(L.pb_assemble_f64(grids["vx"].data_ptr(), grids["vy"].data_ptr(), grids["vz"].data_ptr(),
+                                    grids["screen"].data_ptr(), grids["rhs"].data_ptr(), n, point_weight, 0.5,
+                                    ctx.stream), "assemble")
+    for k in ("vx", "vy", "vz"):
+        del grids[k]
+    return grids, accepted
+
+
+def _iso_value(ctx: _Context, field: torch.Tensor, points: torch.Tensor, normals: torch.Tensor,
+               confidence: bool) -> torch.Tensor:
+    iso = torch.zeros(1, dtype=torch.float64, device=ctx.device)
+    count = points.shape[0]
+    if count:
+        ptr, size = ctx.ws.get(ctx.lib.pb_iso_value_workspace_size(count))
+        ctx.check(ctx.lib.pb_iso_value_f64(field.data_ptr(), points.data_ptr(), normals.data_ptr(), count,
+                                           field.shape[0], int(confidence), iso.data_ptr(), ptr, size, ctx.stream),
+                  "iso value")
+    return iso
+
+
+def _solve_device(ctx: _Context, points: torch.Tensor, normals: torch.Tensor, *, depth: int, point_weight: float,
+                  confidence: bool, cycles: int, samples_per_node: float, precision: str, tol, max_cycles: int,
+                  octree: bool):
+    tree = _octree_device(ctx, points, depth) if octree else None
+    grids, accepted = _splat_assemble(ctx, points, normals, depth, point_weight, confidence, samples_per_node)
+    count = points.shape[0]
+    if precision == "fp64":
+        field, stats = solver.solve_fp64(grids["rhs"], grids["screen"], point_weight, ctx.ws, cycles=cycles,
+                                         tol=tol, max_cycles=max_cycles, has_points=count > 0)
+    else:
+        from . import solver32
+        field, stats = solver32.solve_refined(grids["rhs"], grids["screen"], point_weight, ctx.ws,
+                                              tol=1e-8 if tol is None else tol, max_cycles=max_cycles,
+                                              has_points=count > 0)
+    iso = _iso_value(ctx, field, points, normals, confidence)
+    if count and int(accepted.item()) != count:
+        raise RuntimeError(f"splat accepted {int(accepted.item())} of {count} validated samples")
+    return field, grids, iso, stats, tree
+
+
+def solve_screened_poisson(
+    points,
+    normals,
+    *,
+    depth: int = 6,
+    point_weight: float = 4.0,
+    confidence: bool = False,
+    cycles: int = 4,
+    samples_per_node: float = 1.5,
+    precision: str = "fp64",
+    tol: float | None = None,
+    max_cycles: int = 200,
+    device_out: bool = False,
+) -> GridSolution:
+    """Build the octree, splat samples, and solve the screened Poisson system."""
+    points = _points(points)
+    normals = _points(normals)
+    if tuple(points.shape) != tuple(normals.shape):
+        raise ValueError("points and normals must have the same shape")
+    depth = _integer_parameter("depth", depth)
+    cycles = _integer_parameter("cycles", cycles)
+    max_cycles = _integer_parameter("max_cycles", max_cycles)
+    point_weight = _finite_parameter("point_weight", point_weight)
+    samples_per_node = _finite_parameter("samples_per_node", samples_per_node)
+    precision = _precision(precision)
+    tol = _tolerance(tol)
+    if not 2 <= depth <= MAX_DEPTH:
+        raise ValueError(f"depth must be between 2 and {MAX_DEPTH}")
+    if cycles < 1:
+        raise ValueError("cycles must be positive")
+    if point_weight < 0 or samples_per_node <= 0:
+        raise ValueError("point_weight must be non-negative and samples_per_node positive")
+    ctx = _Context()
+    dp = _to_device(points, ctx.device)
+    dn = _to_device(normals, ctx.device)
+    if dp.shape[0]:
+        dp, dn, count, _ = _prepare(ctx, dp, dn, 0.0)
+        if count:
+            outside = torch.zeros(1, dtype=torch.int32, device=ctx.device)
+            ctx.check(ctx.lib.pb_unit_cube_check_f64(dp.data_ptr(), count, outside.data_ptr(), ctx.stream),
+                      "unit cube check")
+            if int(outside.item()):
+                raise ValueError("solver points must be inside [0, 1]^3")
+    field, grids, iso, stats, tree = _solve_device(
+        ctx, dp, dn, depth=depth, point_weight=point_weight, confidence=confidence, cycles=cycles,
+        samples_per_node=samples_per_node, precision=precision, tol=tol, max_cycles=max_cycles, octree=True)
+    return GridSolution(
+        _host(field, device_out), _host(grids["density"], device_out), _host(grids["screen"], device_out),
+        _host(grids["rhs"], device_out), float(iso.item()), float(stats.residual_norm),
+        _octree_out(tree, device_out), stats.cycles, stats.relative_residual, precision)
+
+
+# ---- extraction (core.py:309-374) --------------------------------------------
+
+def _extract_device(ctx: _Context, field: torch.Tensor, density: torch.Tensor, iso: torch.Tensor):
+    """Two-pass dual contouring on device tensors; returns (vertices, faces, vdens)."""
+    L = ctx.lib
+    n = field.shape[0]
+    cells = n - 1
+    ptr, size = ctx.ws.get(L.pb_dual_workspace_size(n))
+    count = torch.zeros(1, dtype=torch.int64, device=ctx.device)
+    ctx.check(L.pb_dual_vertices_f64_isoptr(field.data_ptr(), density.data_ptr(), n, iso.data_ptr(), None, None,
+                                            None, 0, count.data_ptr(), ptr, size, ctx.stream), "dual count")
+    nv = int(count.item())
+    if nv < 0 or nv > cells ** 3:
+        raise RuntimeError(f"invalid dual vertex count: {nv}")
+    if nv == 0:
+        empty = torch.empty((0, 3), dtype=torch.float64, device=ctx.device)
+        return empty, torch.empty((0, 3), dtype=torch.int64, device=ctx.device), torch.empty(
+            0, dtype=torch.float64, device=ctx.device)
+    vertices = torch.empty((nv, 3), dtype=torch.float64, device=ctx.device)
+    vdens = torch.empty(nv, dtype=torch.float64, device=ctx.device)
+    cell_map = torch.empty(cells ** 3, dtype=torch.int64, device=ctx.device)
+    ctx.check(L.pb_dual_vertices_f64_isoptr(field.data_ptr(), density.data_ptr(), n, iso.data_ptr(),
+                                            cell_map.data_ptr(), vertices.data_ptr(), vdens.data_ptr(), nv,
+                                            count.data_ptr(), ptr, size, ctx.stream), "dual vertices")
+    fcount = torch.zeros(1, dtype=torch.int64, device=ctx.device)
+    ctx.check(L.pb_dual_faces_f64_isoptr(field.data_ptr(), n, iso.data_ptr(), cell_map.data_ptr(), None, 0,
+                                         fcount.data_ptr(), ptr, size, ctx.stream), "dual face count")
+    pair = torch.stack([count, fcount]).cpu()
+    if int(pair[0]) != nv:
+        raise RuntimeError("dual vertex count changed between extraction passes")
+    nf = int(pair[1])
+    if nf < 0 or nf > 6 * cells ** 3:
+        raise RuntimeError(f"invalid dual face count: {nf}")
+    faces = torch.empty((nf, 3), dtype=torch.int64, device=ctx.device)
+    if nf:
+        ctx.check(L.pb_dual_faces_f64_isoptr(field.data_ptr(), n, iso.data_ptr(), cell_map.data_ptr(),
+                                             faces.data_ptr(), nf, fcount.data_ptr(), ptr, size, ctx.stream),
+                  "dual faces")
+    del cell_map
+    return vertices, faces, vdens
+
+
+def extract_isosurface(field, *, iso_value: float = 0.0, density=None, device_out: bool = False) -> Mesh:
+    """Extract a triangle mesh from a cubic scalar grid on the dual grid."""
+    field = f64(field)
+    if field.ndim != 3 or len(set(tuple(field.shape))) != 1 or field.shape[0] < 2:
+        raise ValueError("field must be a cubic array with side length >= 2")
+    iso_value = _finite_parameter("iso_value", iso_value)
+
+    def all_finite(values) -> bool:
+        if isinstance(values, np.ndarray):
+            return bool(np.isfinite(values).all())
+        return bool(torch.isfinite(values).all())
+
+    if not all_finite(field):
+        raise ValueError("field and iso_value must be finite")
+    if density is not None:
+        density = f64(density)
+        if tuple(density.shape) != tuple(field.shape):
+            raise ValueError("density must have the same shape as field")
+        if not all_finite(density):
+            raise ValueError("density must be finite")
+    ctx = _Context()
+    dfield = _to_device(field, ctx.device)
+    ddens = torch.zeros_like(dfield) if density is None else _to_device(density, ctx.device)
+    iso = torch.full((1,), iso_value, dtype=torch.float64, device=ctx.device)
+    v, f, d = _extract_device(ctx, dfield, ddens, iso)
+    return Mesh(_host(v, device_out), _host(f, device_out), _host(d, device_out), iso_value)
+
+
+# ---- reconstruct (core.py:388-455) ----------------------------------------------
+
+def reconstruct(
+    points,
+    normals,
+    *,
+    depth: int = 6,
+    point_weight: float = 4.0,
+    confidence: bool = False,
+    cycles: int = 4,
+    scale: float = 1.1,
+    samples_per_node: float = 1.5,
+    precision: str = "fp64",
+    tol: float | None = None,
+    max_cycles: int = 200,
+    device_out: bool = False,
+) -> Mesh:
+    """Reconstruct a watertight surface from oriented points."""
+    points = _points(points)
+    normals = _points(normals)
+    if tuple(points.shape) != tuple(normals.shape):
+        raise ValueError("points and normals must have the same shape")
+    scale = _finite_parameter("scale", scale)
+    if scale <= 1.0:
+        raise ValueError("scale must be greater than 1")
+    depth = _integer_parameter("depth", depth)
+    cycles = _integer_parameter("cycles", cycles)
+    max_cycles = _integer_parameter("max_cycles", max_cycles)
+    point_weight = _finite_parameter("point_weight", point_weight)
+    samples_per_node = _finite_parameter("samples_per_node", samples_per_node)
+    precision = _precision(precision)
+    tol = _tolerance(tol)
+    if not 2 <= depth <= MAX_DEPTH:
+        raise ValueError(f"depth must be between 2 and {MAX_DEPTH}")
+    if cycles < 1:
+        raise ValueError("cycles must be positive")
+    if point_weight < 0 or samples_per_node <= 0:
+        raise ValueError("point_weight must be non-negative and samples_per_node positive")
+
+    def empty() -> Mesh:
+        if device_out:
+            dev = nat.require_cuda()
+            return Mesh(torch.empty((0, 3), dtype=torch.float64, device=dev),
+                        torch.empty((0, 3), dtype=torch.int64, device=dev),
+                        torch.empty(0, dtype=torch.float64, device=dev))
+        return Mesh(np.empty((0, 3), np.float64), np.empty((0, 3), np.int64), np.empty(0))
+
+    if points.shape[0] == 0:
+        return empty()
+    ctx = _Context()
+    dp, dn, count, fmap = _prepare(ctx, _to_device(points, ctx.device), _to_device(normals, ctx.device), scale)
+    if count == 0:
+        return empty()
+    # The reference also builds the octree here and discards it; it feeds no output.
+    field, grids, iso, stats, _ = _solve_device(
+        ctx, dp, dn, depth=depth, point_weight=point_weight, confidence=confidence, cycles=cycles,
+        samples_per_node=samples_per_node, precision=precision, tol=tol, max_cycles=max_cycles, octree=False)
+    vertices, faces, vdens = _extract_device(ctx, field, grids["density"], iso)
+    ctx.check(ctx.lib.pb_map_vertices_f64(vertices.data_ptr(), vertices.shape[0], fmap.data_ptr(), ctx.stream),
+              "map vertices")
+    return Mesh(_host(vertices, device_out), _host(faces, device_out), _host(vdens, device_out),
+                float(iso.item()), float(stats.residual_norm))
+
+
+# ---- mesh input (core.py:429-455) -------------------------------------------
+
+def oriented_points_from_mesh(vertices, faces):
+    """Return referenced vertices and area-weighted normals from a triangle mesh."""
+    vertices = np.asarray(_points(vertices.cpu() if isinstance(vertices, torch.Tensor) else vertices))
+    faces = np.asarray(i64(faces.cpu() if isinstance(faces, torch.Tensor) else faces))
+    if faces.ndim != 2 or faces.shape[1] != 3:
+        raise ValueError("faces must have shape (m, 3)")
+    if len(faces) and (faces.min() < 0 or faces.max() >= len(vertices)):
+        raise ValueError("face index out of range")
+    normals = np.zeros_like(vertices)
+    referenced = np.zeros(len(vertices), dtype=bool)
+    if len(faces):
+        a, b, c = faces[:, 0], faces[:, 1], faces[:, 2]
+        cross = np.cross(vertices[b] - vertices[a], vertices[c] - vertices[a])
+        good = np.isfinite(cross).all(axis=1) & (np.einsum("ij,ij->i", cross, cross) > 0)
+        tri = faces[good]
+        # np.add.at applies the updates one by one in index order: the same
+        # per-vertex summation order as the reference's per-face loop.
+        order = tri.reshape(-1)
+        np.add.at(normals, order, np.repeat(cross[good], 3, axis=0))
+        referenced[order] = True
+    lengths = np.linalg.norm(normals, axis=1)
+    keep = referenced & (lengths > 0) & np.isfinite(lengths)
+    normals[keep] /= lengths[keep, None]
+    return np.ascontiguousarray(vertices[keep]), np.ascontiguousarray(normals[keep])
+
+
+def reconstruct_mesh(vertices, faces, **kwargs) -> Mesh:
+    points, normals = oriented_points_from_mesh(vertices, faces)
+    return reconstruct(points, normals, **kwargs)

@@ -1,0 +1,69 @@
+// Shared helpers for the sm_100a kernels of the screened-Poisson path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/poisson_b200.h"
+
+namespace pb {
+
+// Sets the thread-local message returned by pb_last_error() and passes the code through.
+int fail(int code, const char* fmt, ...);
+
+// Maps a CUDA error (from a launch or an API call) to PB_ERR_CUDA with its text.
+int cuda_fail(cudaError_t err, const char* where);
+
+#define PB_CHECK_LAUNCH(where)                                   \
+    do {                                                         \
+        cudaError_t e_ = cudaGetLastError();                     \
+        if (e_ != cudaSuccess) return ::pb::cuda_fail(e_, where); \
+    } while (0)
+
+#define PB_CHECK_CUDA(call, where)                               \
+    do {                                                         \
+        cudaError_t e_ = (call);                                 \
+        if (e_ != cudaSuccess) return ::pb::cuda_fail(e_, where); \
+    } while (0)
+
+#define PB_TRY(expr)              \
+    do {                          \
+        int s_ = (expr);          \
+        if (s_ != PB_OK) return s_; \
+    } while (0)
+
+constexpr int kSMs = 148;  // B200: 148 SMs on two dies
+
+__host__ __device__ __forceinline__ int64_t grid_index(int64_t x, int64_t y, int64_t z, int64_t n) {
+    return (z * n + y) * n + x;
+}
+
+inline unsigned blocks_for(int64_t items, int threads) {
+    int64_t b = (items + threads - 1) / threads;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
+// A caller-provided scratch buffer carved into aligned pieces.
+struct Workspace {
+    char* base;
+    size_t size;
+    size_t used;
+    __host__ Workspace(void* p, size_t s) : base((char*)p), size(s), used(0) {}
+    template <typename T>
+    __host__ T* take(size_t count) {
+        size_t off = (used + 255) & ~size_t(255);
+        used = off + count * sizeof(T);
+        return base ? (T*)(base + off) : nullptr;
+    }
+    __host__ bool fits() const { return used <= size; }
+};
+
+// Bytes a sequence of `take` calls needs (run the same carving with base = null).
+template <typename F>
+size_t measure(F&& carve) {
+    Workspace w(nullptr, 0);
+    carve(w);
+    return w.used + 256;
+}
+
+}  // namespace pb

@@ -1,0 +1,279 @@
+// Two-pass trilinear splat, bit-identical to the serial reference.
+//
+// Reference: src/capi.mojo:104-224.  The reference adds each sample's eight
+// corner weights into the grids in point order; floating-point addition is not
+// associative, so atomics would change the last bits.  Here every (point,
+// corner) pair becomes a record keyed by its grid node; a stable radix sort
+// groups the records by node while keeping point order inside each group; one
+// thread then adds a node's contributions in that order, starting from the
+// node's current value — the same additions, in the same order, as the
+// reference.  Pass 2 reuses the sorted order (both passes address the same
+// eight nodes per sample).
+//
+// Compiled with -fmad=false: every product and sum rounds as written.
+#include "radix_sort.cuh"
+
+namespace pb {
+
+__device__ __forceinline__ double norm3(double x, double y, double z) {  // capi.mojo:51-59
+    double scale = fmax(fabs(x), fmax(fabs(y), fabs(z)));
+    if (scale == 0.0) return 0.0;
+    double sx = x / scale, sy = y / scale, sz = z / scale;
+    return scale * sqrt(sx * sx + sy * sy + sz * sz);
+}
+
+__device__ __forceinline__ double clamp01(double v) {  // min(max(v, 0), 1)
+    double m = v > 0.0 ? v : 0.0;
+    return m < 1.0 ? m : 1.0;
+}
+
+// Pass-1 base cell and fractions (capi.mojo:139-162).
+__device__ __forceinline__ void pass1_cell(double p, int64_t res, int64_t& i, double& f) {
+    double g = p * (double)res;
+    i = (int64_t)g;
+    if (i < 0) i = 0;
+    if (i >= res) {
+        i = res - 1;
+        g = (double)res;
+    }
+    f = g - (double)i;
+}
+
+// Pass-2 / iso-value base cell and fractions (capi.mojo:187-195, :771-779).
+__device__ __forceinline__ void pass2_cell(double p, int64_t res, int64_t& i, double& f) {
+    double g = p * (double)res;
+    int64_t t = (int64_t)g;
+    i = t < 0 ? 0 : (t > res - 1 ? res - 1 : t);
+    f = clamp01(g - (double)i);
+}
+
+// Records: key = grid node (or the sentinel n^3 for a rejected sample), value =
+// point*8 + corner, corner = dz*4 + dy*2 + dx; weight[record] = pass-1 weight.
+__global__ void splat_records_kernel(const double* __restrict__ points, const double* __restrict__ normals,
+                                     int64_t count, int64_t n, int confidence, uint32_t* __restrict__ keys,
+                                     uint32_t* __restrict__ vals, double* __restrict__ weight,
+                                     unsigned long long* __restrict__ accepted) {
+    __shared__ unsigned int block_accepted;
+    if (threadIdx.x == 0) block_accepted = 0;
+    __syncthreads();
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < count) {
+        const int64_t res = n - 1;
+        double nx = normals[3 * p], ny = normals[3 * p + 1], nz = normals[3 * p + 2];
+        double length = norm3(nx, ny, nz);
+        const uint32_t r0 = (uint32_t)(p * 8);
+        if (length <= 0.0) {  // capi.mojo:132-133
+            const uint32_t sentinel = (uint32_t)(n * n * n);
+            for (int c = 0; c < 8; ++c) {
+                keys[r0 + c] = sentinel;
+                vals[r0 + c] = r0 + c;
+                weight[r0 + c] = 0.0;
+            }
+        } else {
+            double sw = confidence ? length : 1.0;
+            int64_t ix, iy, iz;
+            double fx, fy, fz;
+            pass1_cell(points[3 * p], res, ix, fx);
+            pass1_cell(points[3 * p + 1], res, iy, fy);
+            pass1_cell(points[3 * p + 2], res, iz, fz);
+            for (int dz = 0; dz < 2; ++dz) {
+                double wz = dz == 1 ? fz : 1.0 - fz;
+                for (int dy = 0; dy < 2; ++dy) {
+                    double wy = dy == 1 ? fy : 1.0 - fy;
+                    for (int dx = 0; dx < 2; ++dx) {
+                        double wx = dx == 1 ? fx : 1.0 - fx;
+                        const int c = dz * 4 + dy * 2 + dx;
+                        keys[r0 + c] = (uint32_t)grid_index(ix + dx, iy + dy, iz + dz, n);
+                        vals[r0 + c] = r0 + c;
+                        weight[r0 + c] = wx * wy * wz * sw;
+                    }
+                }
+            }
+            atomicAdd(&block_accepted, 1u);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && block_accepted) atomicAdd(accepted, (unsigned long long)block_accepted);
+}
+
+// Pass 1 (capi.mojo:171-172): density += 2w, screen += w, per node in point order.
+__global__ void splat_density_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                                     int64_t records, uint32_t sentinel, const double* __restrict__ weight,
+                                     double* __restrict__ density, double* __restrict__ screen) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= records) return;
+    const uint32_t node = keys[j];
+    if (node == sentinel || (j > 0 && keys[j - 1] == node)) return;
+    double d = density[node], s = screen[node];
+    for (int64_t k = j; k < records && keys[k] == node; ++k) {
+        double w = weight[vals[k]];
+        d += 2.0 * w;
+        s += w;
+    }
+    density[node] = d;
+    screen[node] = s;
+}
+
+// Pass 2, per sample (capi.mojo:176-209): local density from the pass-1 grid,
+// the density factor, and per-record vector weights w * res / factor.
+__global__ void splat_vector_weights_kernel(const double* __restrict__ points, const double* __restrict__ normals,
+                                            int64_t count, int64_t n, int confidence, double samples_per_node,
+                                            const double* __restrict__ density, double* __restrict__ weight,
+                                            double* __restrict__ unit_normals) {
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= count) return;
+    double nx = normals[3 * p], ny = normals[3 * p + 1], nz = normals[3 * p + 2];
+    double length = norm3(nx, ny, nz);
+    if (length <= 0.0) return;  // capi.mojo:181-182
+    const int64_t res = n - 1;
+    double sw = confidence ? length : 1.0;
+    unit_normals[3 * p] = nx / length;
+    unit_normals[3 * p + 1] = ny / length;
+    unit_normals[3 * p + 2] = nz / length;
+    int64_t ix, iy, iz;
+    double fx, fy, fz;
+    pass2_cell(points[3 * p], res, ix, fx);
+    pass2_cell(points[3 * p + 1], res, iy, fy);
+    pass2_cell(points[3 * p + 2], res, iz, fz);
+    double local = 0.0;
+    for (int dz = 0; dz < 2; ++dz) {
+        double wz = dz == 1 ? fz : 1.0 - fz;
+        for (int dy = 0; dy < 2; ++dy) {
+            double wy = dy == 1 ? fy : 1.0 - fy;
+            for (int dx = 0; dx < 2; ++dx) {
+                double wx = dx == 1 ? fx : 1.0 - fx;
+                local += density[grid_index(ix + dx, iy + dy, iz + dz, n)] * wx * wy * wz;
+            }
+        }
+    }
+    double q = local / samples_per_node;
+    double factor = 1.0 > q ? 1.0 : q;
+    const int64_t r0 = p * 8;
+    for (int dz = 0; dz < 2; ++dz) {
+        double wz = dz == 1 ? fz : 1.0 - fz;
+        for (int dy = 0; dy < 2; ++dy) {
+            double wy = dy == 1 ? fy : 1.0 - fy;
+            for (int dx = 0; dx < 2; ++dx) {
+                double wx = dx == 1 ? fx : 1.0 - fx;
+                double w = wx * wy * wz * sw;
+                weight[r0 + dz * 4 + dy * 2 + dx] = w * (double)res / factor;
+            }
+        }
+    }
+}
+
+// Pass 2 (capi.mojo:221-223): V -= n_hat * vector_weight, per node in point order.
+__global__ void splat_vector_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                                    int64_t records, uint32_t sentinel, const double* __restrict__ weight,
+                                    const double* __restrict__ unit_normals, double* __restrict__ vx,
+                                    double* __restrict__ vy, double* __restrict__ vz) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= records) return;
+    const uint32_t node = keys[j];
+    if (node == sentinel || (j > 0 && keys[j - 1] == node)) return;
+    double ax = vx[node], ay = vy[node], az = vz[node];
+    for (int64_t k = j; k < records && keys[k] == node; ++k) {
+        const uint32_t r = vals[k];
+        const double vw = weight[r];
+        const double* u = unit_normals + 3 * (int64_t)(r >> 3);
+        ax -= u[0] * vw;
+        ay -= u[1] * vw;
+        az -= u[2] * vw;
+    }
+    vx[node] = ax;
+    vy[node] = ay;
+    vz[node] = az;
+}
+
+__global__ void store_count_kernel(const unsigned long long* __restrict__ src, int64_t* __restrict__ dst) {
+    *dst = (int64_t)*src;
+}
+
+struct SplatWork {
+    uint32_t *keys, *keys_alt, *vals, *vals_alt;
+    double* weight;
+    double* unit_normals;
+    unsigned long long* accepted;
+};
+
+static SplatWork splat_carve(Workspace& w, int64_t count) {
+    SplatWork o;
+    const int64_t records = count * 8;
+    o.keys = w.take<uint32_t>(records);
+    o.keys_alt = w.take<uint32_t>(records);
+    o.vals = w.take<uint32_t>(records);
+    o.vals_alt = w.take<uint32_t>(records);
+    o.weight = w.take<double>(records);
+    o.unit_normals = w.take<double>(count * 3);
+    o.accepted = w.take<unsigned long long>(1);
+    return o;
+}
+
+static size_t splat_ws_bytes(int64_t count) {
+    return measure([&](Workspace& w) {
+        splat_carve(w, count);
+        radix_carve<uint32_t>(w, count * 8);
+    });
+}
+
+static int bit_width(uint64_t v) {
+    int b = 0;
+    while (v) {
+        ++b;
+        v >>= 1;
+    }
+    return b;
+}
+
+}  // namespace pb
+
+using namespace pb;
+
+extern "C" size_t pb_splat_workspace_size(int64_t point_count, int64_t n) {
+    (void)n;
+    return splat_ws_bytes(point_count < 1 ? 1 : point_count);
+}
+
+extern "C" int pb_splat_f64(const double* points, const double* normals, int64_t point_count, int64_t n,
+                            int64_t confidence, double* density, double* vx, double* vy, double* vz, double* screen,
+                            double samples_per_node, int64_t* accepted, void* workspace, size_t workspace_bytes,
+                            void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    if (n < 2) return fail(PB_ERR_INVALID, "splat: n must be >= 2");
+    if (n * n * n >= (int64_t)0x7FFFFFFF) return fail(PB_ERR_INVALID, "splat: n^3 must be < 2^31");
+    if (point_count < 0 || point_count * 8 >= (int64_t)0xFFFFFFFFll)
+        return fail(PB_ERR_INVALID, "splat: point_count must be in [0, 2^29)");
+    if (!accepted || !density || !vx || !vy || !vz || !screen) return fail(PB_ERR_INVALID, "splat: null buffer");
+    if (point_count == 0) {
+        PB_CHECK_CUDA(cudaMemsetAsync(accepted, 0, sizeof(int64_t), s), "splat accepted");
+        return PB_OK;
+    }
+    if (!points || !normals) return fail(PB_ERR_INVALID, "splat: null points/normals");
+    const size_t need = splat_ws_bytes(point_count);
+    if (!workspace || workspace_bytes < need) return fail(PB_ERR_WORKSPACE, "splat: workspace needs %zu bytes", need);
+    Workspace w(workspace, workspace_bytes);
+    SplatWork o = splat_carve(w, point_count);
+    const int64_t records = point_count * 8;
+    const uint32_t sentinel = (uint32_t)(n * n * n);
+    PB_CHECK_CUDA(cudaMemsetAsync(o.accepted, 0, sizeof(unsigned long long), s), "splat accepted");
+    splat_records_kernel<<<blocks_for(point_count, 256), 256, 0, s>>>(points, normals, point_count, n, (int)confidence,
+                                                                      o.keys, o.vals, o.weight, o.accepted);
+    PB_CHECK_LAUNCH("splat_records_kernel");
+    bool in_alt = false;
+    PB_TRY(radix_sort_pairs<uint32_t>(o.keys, o.vals, o.keys_alt, o.vals_alt, records, bit_width(sentinel), &in_alt,
+                                      w, s));
+    const uint32_t* keys = in_alt ? o.keys_alt : o.keys;
+    const uint32_t* vals = in_alt ? o.vals_alt : o.vals;
+    splat_density_kernel<<<blocks_for(records, 256), 256, 0, s>>>(keys, vals, records, sentinel, o.weight, density,
+                                                                   screen);
+    PB_CHECK_LAUNCH("splat_density_kernel");
+    splat_vector_weights_kernel<<<blocks_for(point_count, 256), 256, 0, s>>>(
+        points, normals, point_count, n, (int)confidence, samples_per_node, density, o.weight, o.unit_normals);
+    PB_CHECK_LAUNCH("splat_vector_weights_kernel");
+    splat_vector_kernel<<<blocks_for(records, 256), 256, 0, s>>>(keys, vals, records, sentinel, o.weight,
+                                                                  o.unit_normals, vx, vy, vz);
+    PB_CHECK_LAUNCH("splat_vector_kernel");
+    store_count_kernel<<<1, 1, 0, s>>>(o.accepted, accepted);
+    PB_CHECK_LAUNCH("store_count_kernel");
+    return PB_OK;
+}

@@ -1,0 +1,166 @@
+"""The FP32-refined path: its FP32 kernels against the FP64 oracle (FP32
+tolerance, written per test), and the defect-corrected solve against the
+FP64 solve of the same system.
+
+Tolerances: a FP32 kernel's output is compared with the oracle's FP64 output
+on the same (FP32-representable) inputs within rtol 2e-6 of the largest
+magnitude; the refined solve must reach ||b - A x|| / ||b|| <= 1e-8 measured in
+FP64 and agree with the FP64 solution at equal residual within 1e-6 relative
+(max norm)."""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def L():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from mojo_poissonrecon_b200 import _native
+
+    return _native.lib()
+
+
+def _a(x):
+    return int(x.ctypes.data)
+
+
+def geometry(L, n):
+    pitch, count = ctypes.c_int64(), ctypes.c_int64()
+    assert L.pb_level_geometry(n, ctypes.byref(pitch), ctypes.byref(count)) == 0
+    return pitch.value, count.value
+
+
+def to_padded(L, a):
+    n = a.shape[0]
+    pitch, count = geometry(L, n)
+    out = np.zeros(count, np.float32)
+    view = out.reshape(n + 2, n + 2, pitch)
+    view[1:n + 1, 1:n + 1, 4:n + 4] = a
+    return torch.from_numpy(out).cuda()
+
+
+def from_padded(L, t, n):
+    pitch, _ = geometry(L, n)
+    v = t.cpu().numpy().reshape(n + 2, n + 2, pitch)
+    return v[1:n + 1, 1:n + 1, 4:n + 4].astype(np.float64)
+
+
+def ghosts_zero(L, t, n):
+    pitch, _ = geometry(L, n)
+    v = t.cpu().numpy().reshape(n + 2, n + 2, pitch).copy()
+    v[1:n + 1, 1:n + 1, 4:n + 4] = 0
+    return not v.any()
+
+
+def setup(L, n, seed):
+    rng = np.random.default_rng(seed)
+    screen = rng.random((n, n, n)) * (rng.random((n, n, n)) < 0.2)
+    rhs = rng.normal(size=(n, n, n)).astype(np.float32).astype(np.float64)
+    x = rng.normal(size=(n, n, n)).astype(np.float32).astype(np.float64)
+    D = torch.zeros(geometry(L, n)[1], dtype=torch.float32, device="cuda")
+    invD = torch.zeros_like(D)
+    s64 = torch.from_numpy(screen).cuda()
+    assert L.pb_level_setup_f32(s64.data_ptr(), n, 4.0, D.data_ptr(), invD.data_ptr(),
+                                torch.cuda.current_stream().cuda_stream) == 0
+    return screen, rhs, x, D, invD, s64
+
+
+@pytest.mark.parametrize("n,z_chunk", [(3, 32), (9, 4), (17, 5), (33, 32), (65, 7), (129, 32), (257, 64)])
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_sweep_matches_fp64_relax(L, oracle, n, z_chunk, mode):
+    screen, rhs, x, D, invD, _ = setup(L, n, n + mode)
+    cn = (n + 1) // 2
+    coarse = np.random.default_rng(1).normal(size=(cn,) * 3).astype(np.float32).astype(np.float64)
+    start = x.copy() if mode != 1 else np.zeros_like(x)
+    if mode == 2:
+        oracle.lib().mpr_prolong_add_f64(_a(coarse), _a(start), n)
+    want = start.copy()
+    oracle.lib().mpr_relax_f64(_a(want), _a(rhs), _a(screen), n, 4.0, 1)
+    e_in, rhs32, c32 = to_padded(L, x), to_padded(L, rhs.astype(np.float32)), to_padded(L, coarse)
+    e_out = torch.zeros_like(e_in)
+    s = torch.cuda.current_stream().cuda_stream
+    assert L.pb_sweep_f32(e_in.data_ptr(), e_out.data_ptr(), rhs32.data_ptr(), invD.data_ptr(), c32.data_ptr(), n,
+                          mode, z_chunk, s) == 0
+    got = from_padded(L, e_out, n)
+    scale = np.abs(want).max()
+    assert np.allclose(got, want, rtol=0, atol=2e-6 * scale)
+    assert ghosts_zero(L, e_out, n)
+
+
+@pytest.mark.parametrize("n", [5, 17, 65, 129])
+def test_residual32_restrict32_match_oracle(L, oracle, n):
+    screen, rhs, x, D, invD, _ = setup(L, n, 3 * n)
+    want = np.empty_like(x)
+    oracle.lib().mpr_residual_f64(_a(x), _a(rhs), _a(screen), _a(want), n, 4.0)
+    e32, rhs32 = to_padded(L, x), to_padded(L, rhs)
+    res = torch.zeros_like(e32)
+    s = torch.cuda.current_stream().cuda_stream
+    assert L.pb_residual_f32(e32.data_ptr(), rhs32.data_ptr(), D.data_ptr(), res.data_ptr(), n, s) == 0
+    got = from_padded(L, res, n)
+    # cancellation: compare against the size of the terms, not of the result
+    terms = ((6 + 4 * screen) * (n - 1) ** 2).max() * np.abs(x).max()
+    assert np.abs(got - want).max() <= 4e-7 * terms
+    cn = (n + 1) // 2
+    coarse = torch.zeros(geometry(L, cn)[1], dtype=torch.float32, device="cuda")
+    res_in = to_padded(L, want)
+    assert L.pb_restrict_f32(res_in.data_ptr(), coarse.data_ptr(), n, s) == 0
+    c_ref = np.empty((cn,) * 3)
+    oracle.lib().mpr_restrict_f64(_a(want.astype(np.float32).astype(np.float64)), _a(c_ref), n)
+    assert np.allclose(from_padded(L, coarse, cn), c_ref, rtol=0, atol=2e-6 * np.abs(c_ref).max())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_refined"])
+def test_tolerance_solves_reach_target(oracle, precision):
+    import mojo_poissonrecon_b200 as mpr
+    from mojo_poissonrecon_b200 import workloads
+
+    pts, nrm = workloads.torus(40_000, seed=3)
+    keep = oracle.valid_rows(pts, nrm)
+    unit, _, _ = oracle.normalize(pts[keep], 1.1)
+    ref = oracle.solve(unit, nrm[keep], depth=6, confidence=True, tol=1e-11, max_cycles=200, octree=False)
+    got = mpr.solve_screened_poisson(unit, nrm[keep], depth=6, confidence=True, tol=1e-8, precision=precision)
+    # the reported relative residual is measured in FP64 on the returned field
+    res = np.empty_like(got.field)
+    n = got.field.shape[0]
+    r = oracle.lib().mpr_residual_f64(_a(got.field), _a(got.rhs), _a(got.screen), _a(res), n, 4.0)
+    assert r / np.linalg.norm(got.rhs) <= 1e-8
+    assert got.relative_residual == pytest.approx(r / np.linalg.norm(got.rhs), rel=1e-6)
+    err = np.abs(got.field - ref.field).max() / np.abs(ref.field).max()
+    assert err <= 1e-6, err
+    assert got.iso_value == pytest.approx(ref.iso_value, rel=1e-6)
+
+
+def test_refined_cycle_count_close_to_fp64():
+    """Each refined step contracts like an FP64 V-cycle: the step counts agree."""
+    import mojo_poissonrecon_b200 as mpr
+    from mojo_poissonrecon_b200 import workloads
+
+    pts, nrm = workloads.torus(100_000, seed=8)
+    a = mpr.solve_screened_poisson(*_unit(pts, nrm), depth=7, confidence=True, tol=1e-8, precision="fp64")
+    b = mpr.solve_screened_poisson(*_unit(pts, nrm), depth=7, confidence=True, tol=1e-8, precision="fp32_refined")
+    assert b.relative_residual <= 1e-8 and a.relative_residual <= 1e-8
+    assert abs(a.cycles - b.cycles) <= 2, (a.cycles, b.cycles)
+
+
+def _unit(pts, nrm):
+    lo, hi = pts.min(0), pts.max(0)
+    w = (hi - lo).max() * 1.1
+    return (pts - (0.5 * (lo + hi) - 0.5 * w)) / w, nrm
+
+
+def test_refined_mesh_matches_fp64_mesh():
+    import mojo_poissonrecon_b200 as mpr
+    from mojo_poissonrecon_b200 import workloads
+
+    pts, nrm = workloads.torus(50_000, seed=4)
+    a = mpr.reconstruct(pts, nrm, depth=7, confidence=True, tol=1e-8, precision="fp64")
+    b = mpr.reconstruct(pts, nrm, depth=7, confidence=True, tol=1e-8, precision="fp32_refined")
+    assert abs(a.faces.shape[0] - b.faces.shape[0]) <= 0.001 * a.faces.shape[0]
+    assert b.iso_value == pytest.approx(a.iso_value, rel=1e-6)
