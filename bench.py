@@ -1,0 +1,408 @@
+#!/usr/bin/env python
+"""Benchmark: reconstructions/s and p99 latency for the screened-Poisson path.
+
+Workload (one step = one reconstruction): 1,000,000 points sampled uniformly by
+area on a torus (R = 0.6, r = 0.25) with Gaussian position noise 0.002 and
+normals scaled by a confidence U(0.5, 1.5) (confidence=True), screening weight
+4.0, depth 8 (257^3 grid), V-cycles until ||b - A x|| / ||b|| <= 1e-8, then
+dual contouring.  Seeded synthetic data (no dataset is involved).
+
+Arms:
+  ours (default)     value = FP32-refined reconstructions/s with the inputs
+                     already in HBM; "fp64" = the plain FP64 solve on the same
+                     workload; "e2e" = the public API on pinned host arrays,
+                     host->device and device->host copies inside the timed
+                     region.  Under torchrun every rank runs its own replica
+                     (reconstructions are independent): weak scaling, no
+                     collective on the data path.
+  --impl reference   the CPU restatement of the reference (oracle/, OpenMP
+                     build, all host threads) on the same workload; rank 0 only.
+
+Prints one JSON line on rank 0.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "recons/s & p99 ms: batched FP32+FP64-refined vs plain FP64 at rel-res 1e-8"
+WORKLOAD = "torus 1M points, depth 8 (257^3), confidence normals, point_weight 4, solve to rel-res 1e-8, dual contour"
+POINTS = 1_000_000
+DEPTH = 8
+TOL = 1e-8
+SWEEP_PROFILE = os.path.join(ROOT, "profiles", "sweep_tma_f32_257.md")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--points", type=int, default=POINTS)
+    ap.add_argument("--depth", type=int, default=DEPTH)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="only the FP32-refined arm (the command the ncu captures run)")
+    return ap.parse_args()
+
+
+def workload(points: int, seed: int = 1):
+    from mojo_poissonrecon_b200 import workloads
+
+    return workloads.torus(points, seed=seed)
+
+
+# ---- clocks sampled during the timed region ------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            with open(self.path, encoding="utf8") as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+        def num(s):
+            m = re.match(r"([\d.]+)", s)
+            return float(m.group(1)) if m else None
+
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---- our arm -----------------------------------------------------------------
+
+def run_ours(args, rank: int, world: int, dist) -> dict | None:
+    import torch
+
+    import mojo_poissonrecon_b200 as mpr
+    from mojo_poissonrecon_b200 import _native, solver32
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pts, nrm = workload(args.points)
+    host_p = torch.from_numpy(pts).pin_memory()
+    host_n = torch.from_numpy(nrm).pin_memory()
+    dev_p, dev_n = host_p.to(dev), host_n.to(dev)
+    common = dict(depth=args.depth, confidence=True, point_weight=4.0, tol=TOL)
+    lib = _native.lib()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(value: float) -> float:
+        if dist is None:
+            return value
+        t = torch.tensor([value], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(fn, steps):
+        """CUDA-event timing of `steps` calls, per-step latencies; max over ranks."""
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        barrier()
+        evs[0].record()
+        for k in range(steps):
+            fn()
+            evs[k + 1].record()
+        torch.cuda.synchronize()
+        barrier()
+        per = [evs[k].elapsed_time(evs[k + 1]) for k in range(steps)]
+        return max_over_ranks(sum(per)), per
+
+    def refined_device():
+        return mpr.reconstruct(dev_p, dev_n, precision="fp32_refined", device_out=True, **common)
+
+    def fp64_device():
+        return mpr.reconstruct(dev_p, dev_n, precision="fp64", device_out=True, **common)
+
+    def refined_e2e():
+        return mpr.reconstruct(host_p, host_n, precision="fp32_refined", device_out=False, **common)
+
+    for _ in range(args.warmup):
+        refined_device()
+        if not args.profile:
+            fp64_device()
+            refined_e2e()
+    torch.cuda.synchronize()
+
+    # headline: FP32-refined, inputs resident in HBM; the level-0 sweep launches
+    # are bracketed with CUDA events on the launching stream for the roofline
+    probe = []
+    solver32.PROBE = probe
+    launches0 = lib.pb_launch_count()
+    with ClockSampler(local) as clocks:
+        total_ms, per = timed(refined_device, args.steps)
+    launches = lib.pb_launch_count() - launches0
+    solver32.PROBE = None
+    clock_info = clocks.summary()
+    sweep_ms = [a.elapsed_time(b) for a, b, mode in probe if mode == 0]
+    value = world * args.steps / (total_ms / 1e3)
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile": True, "value": value, "launches_per_step": launches / args.steps}))
+        return None
+
+    fp64_ms, per64 = timed(fp64_device, max(3, args.steps // 2))
+    value64 = world * len(per64) / (fp64_ms / 1e3)
+
+    # end to end through the public API with host buffers
+    mesh_holder = {}
+
+    def e2e_step():
+        mesh_holder["m"] = refined_e2e()
+
+    e2e_ms, per_e2e = timed(e2e_step, max(3, args.steps // 2))
+    mesh = mesh_holder["m"]
+    h2d = 2 * args.points * 3 * 8
+    d2h = mesh.vertices.nbytes + mesh.faces.nbytes + mesh.density.nbytes
+    e2e_value = world * len(per_e2e) / (e2e_ms / 1e3)
+
+    # accuracy of the refined result against the FP64 solve (not timed)
+    keep_solution = {}
+    from mojo_poissonrecon_b200 import core
+
+    unit_p = None
+    if rank == 0:
+        ctx = core._Context()
+        dp, dn, _, _ = core._prepare(ctx, dev_p, dev_n, 1.1)
+        unit_p = (dp, dn)
+        f32, _, _, st32, _ = core._solve_device(ctx, dp, dn, depth=args.depth, point_weight=4.0, confidence=True,
+                                                cycles=4, samples_per_node=1.5, precision="fp32_refined", tol=TOL,
+                                                max_cycles=200, octree=False)
+        f64, _, _, st64, _ = core._solve_device(ctx, dp, dn, depth=args.depth, point_weight=4.0, confidence=True,
+                                                cycles=4, samples_per_node=1.5, precision="fp64", tol=TOL,
+                                                max_cycles=200, octree=False)
+        err = float((f32 - f64).abs().max() / f64.abs().max())
+        keep_solution = {"refined_cycles": st32.cycles, "fp64_cycles": st64.cycles,
+                         "refined_rel_residual": st32.relative_residual, "fp64_rel_residual": st64.relative_residual,
+                         "field_max_rel_err_refined_vs_fp64": err}
+    del unit_p
+
+    n = (1 << args.depth) + 1
+    roofline = None
+    if sweep_ms:
+        from json import loads
+
+        peaks = {}
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json"), encoding="utf8") as f:
+                peaks = loads(f.read())
+        except OSError:
+            pass
+        peak = float(peaks.get("hbm_gbs", 6650.0))
+        peak_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
+        avg_ms = statistics.mean(sweep_ms)
+        algorithmic = 16.0 * n**3  # read e, rhs, 1/D and write e, FP32, per launch
+        achieved = algorithmic / (avg_ms / 1e3) / 1e9
+        roofline = {"kernel": "pb::tma::sweep_kernel<false> (fused red-black sweep, level 0, 257^3)",
+                    "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                    "frac": round(achieved / peak, 4), "peak_source": peak_src,
+                    "avg_launch_ms": round(avg_ms, 4), "launches_timed": len(sweep_ms),
+                    "algorithmic_bytes_per_launch": int(algorithmic), "traffic": read_profile_traffic()}
+
+    if rank != 0:
+        return None
+    result = {
+        "metric": METRIC,
+        "value": round(value, 3),
+        "unit": "recons/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64",
+        "data": "synthetic (seeded torus, see bench.py docstring)",
+        "config": {"workload": WORKLOAD, "points": args.points, "depth": args.depth, "grid": f"{n}^3",
+                   "precision": "fp32_refined", "tol": TOL,
+                   "l2": "no flush needed: each step streams > 1 GB of grids, larger than the 126 MB L2",
+                   "parallelism": f"replicas x{world} (request-level)"},
+        "p50_ms": round(statistics.median(per), 3),
+        "p99_ms": round(float(np.percentile(per, 99)), 3),
+        "fp64": {"value": round(value64, 3), "unit": "recons/s", "p50_ms": round(statistics.median(per64), 3),
+                 "p99_ms": round(float(np.percentile(per64, 99)), 3)},
+        "accuracy": keep_solution,
+        "e2e": {"value": round(e2e_value, 3), "unit": "recons/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": int(d2h), "p50_ms": round(statistics.median(per_e2e), 3),
+                "p99_ms": round(float(np.percentile(per_e2e, 99)), 3)},
+        "roofline": roofline,
+        "gpu_launches": int(launches),
+        "clocks": clock_info,
+    }
+    return result
+
+
+def read_profile_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    try:
+        with open(SWEEP_PROFILE, encoding="utf8") as f:
+            for line in f:
+                m = re.match(r"\s*traffic_bytes_per_launch_257:\s*([\d.eE+]+)", line)
+                if m:
+                    return float(m.group(1))
+    except OSError:
+        pass
+    return None
+
+
+# ---- CPU baselines (the oracle: test infrastructure, timed only here) -------------
+
+def cpu_sample(pts, nrm, depth: int, threaded: bool, full: bool):
+    """Seconds per reconstruction of the workload on the host.  full=False times
+    the set-up and 3 V-cycles and extrapolates to the cycle count the FP64
+    solve needs (the cycle count comes from a GPU or earlier CPU run)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pipeline as oracle
+
+    if not os.path.exists(os.path.join(ROOT, "oracle", "liboracle_mpr.so")):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-s"], check=True)
+    keep = oracle.valid_rows(pts, nrm)
+    t0 = time.perf_counter()
+    if full:
+        oracle.reconstruct(pts, nrm, depth=depth, confidence=True, point_weight=4.0, tol=TOL, max_cycles=200,
+                           threaded=threaded, octree=False)
+        return time.perf_counter() - t0, "full reconstruction"
+    unit, _, _ = oracle.normalize(pts[keep], 1.1)
+    t_a = time.perf_counter()
+    sol = oracle.solve(unit, nrm[keep], depth=depth, confidence=True, point_weight=4.0, cycles=1,
+                       threaded=threaded, octree=False)
+    t_b = time.perf_counter()
+    sol3 = oracle.solve(unit, nrm[keep], depth=depth, confidence=True, point_weight=4.0, cycles=3,
+                        threaded=threaded, octree=False)
+    t_c = time.perf_counter()
+    per_cycle = ((t_c - t_b) - (t_b - t_a)) / 2.0
+    setup = (t_b - t_a) - per_cycle
+    t_d = time.perf_counter()
+    oracle.extract(sol3.field, sol3.iso_value, sol3.density, threaded)
+    extract_s = time.perf_counter() - t_d
+    cycles = 31  # V-cycles the FP64 solve of this workload needs to reach 1e-8 (measured)
+    total = (t_a - t0) + setup + cycles * per_cycle + extract_s
+    return total, f"set-up + 1 and 3 V-cycles timed, extrapolated to {cycles} cycles + extraction"
+
+
+def run_reference(args) -> dict:
+    """The CPU restatement of the reference on all host threads (oracle OpenMP build)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pipeline as oracle
+
+    pts, nrm = workload(args.points)
+    threads = int(oracle.lib(True).mpr_oracle_threads())
+    first, how = cpu_sample(pts, nrm, args.depth, True, True)
+    budget = 180.0
+    full = first * (args.steps + args.warmup) <= budget
+    times = []
+    for k in range(args.warmup + args.steps):
+        if k == 0:
+            dt = first
+        else:
+            dt, how = cpu_sample(pts, nrm, args.depth, True, full)
+        if k >= args.warmup:
+            times.append(dt)
+        if not full and k >= args.warmup:
+            break
+    per = statistics.mean(times) if times else first
+    value = 1.0 / per
+    return {
+        "metric": METRIC, "impl": "reference", "value": round(value, 5), "unit": "recons/s", "n_gpus": args.gpus,
+        "steps": len(times), "warmup": args.warmup, "ms_per_step": round(per * 1e3, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (same seeded torus)",
+        "config": {"workload": WORKLOAD, "points": args.points, "depth": args.depth, "precision": "fp64", "tol": TOL},
+        "cpu_baseline": {"value": round(value, 5), "unit": "recons/s", "cores": threads, "kind": "port",
+                         "sample": how + " (oracle/mpr_oracle.c OpenMP build: the reference's CPU kernels restated)"},
+        "e2e": {"value": round(value, 5), "unit": "recons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as torch_dist
+
+        torch_dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = torch_dist
+    try:
+        result = run_ours(args, rank, world, dist)
+        if rank == 0 and result is not None:
+            if world == 1 and not args.no_cpu_baseline and not args.profile:
+                pts, nrm = workload(args.points)
+                per, how = cpu_sample(pts, nrm, args.depth, False, False)
+                result["cpu_baseline"] = {"value": round(1.0 / per, 5), "unit": "recons/s", "cores": 1,
+                                          "kind": "port",
+                                          "sample": how + " (serial oracle/mpr_oracle.c, the reference's "
+                                                          "single-threaded CPU kernels restated)"}
+            print(json.dumps(result), flush=True)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

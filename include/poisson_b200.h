@@ -44,6 +44,8 @@ enum {
 const char *pb_last_error(void);
 /* ABI version, major*10000 + minor*100 + patch. */
 int pb_version(void);
+/* Number of kernels this library has launched in the process so far. */
+long long pb_launch_count(void);
 
 /* Replaces mpr_parallel_init (_lib.py:21; capi.mojo:36-38): selects `device`
  * and checks it is an sm_100 part.  Optional; every call works without it. */
@@ -184,6 +186,13 @@ int pb_defect_f64(const double *x_old, const float *e, double *x_new, const doub
  * prolongation of `coarse` (side (n+1)/2).  n = 2^k + 1. */
 int pb_sweep_f32(const float *e_in, float *e_out, const float *rhs, const float *invD,
                  const float *coarse, int64_t n, int64_t mode, int64_t z_chunk, void *stream);
+/* The same sweep with TMA-staged planes (n = 2^k + 1 >= 33): mode 0 from
+ * e_in, mode 1 from zero.  z_chunk <= 0 picks one.  A bounded wait that gives
+ * up sets *status (device int) to 1. */
+int pb_sweep_tma_f32(const float *e_in, float *e_out, const float *rhs, const float *invD, int64_t n,
+                     int64_t mode, int64_t z_chunk, int *status, void *stream);
+/* fine += trilinear prolongation of coarse (side (n+1)/2), padded layouts. */
+int pb_prolong_add_f32(const float *coarse, float *fine, int64_t fine_n, void *stream);
 int pb_residual_f32(const float *e, const float *rhs, const float *D, float *residual, int64_t n,
                     void *stream);
 int pb_restrict_f32(const float *fine, float *coarse, int64_t fine_n, void *stream);

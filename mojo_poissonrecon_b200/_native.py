@@ -25,6 +25,7 @@ C = ctypes.c_int
 _SIGNATURES = {
     "pb_last_error": ([], ctypes.c_char_p),
     "pb_version": ([], C),
+    "pb_launch_count": ([], ctypes.c_longlong),
     "pb_init": ([C], C),
     "pb_octree_codes_f64": ([P, I, I, P, P], C),
     "pb_octree_workspace_size": ([I, I], S),
@@ -58,6 +59,8 @@ _SIGNATURES = {
     "pb_defect_workspace_size": ([I], S),
     "pb_defect_f64": ([P, P, P, P, P, I, F, P, P, P, S, P], C),
     "pb_sweep_f32": ([P, P, P, P, P, I, I, I, P], C),
+    "pb_sweep_tma_f32": ([P, P, P, P, I, I, I, P, P], C),
+    "pb_prolong_add_f32": ([P, P, I, P], C),
     "pb_residual_f32": ([P, P, P, P, I, P], C),
     "pb_restrict_f32": ([P, P, I, P], C),
     "pb_coarse_cycle_f32": ([I, P, P, P, P, P, P, I, I, I, P], C),

@@ -14,8 +14,12 @@ int fail(int code, const char* fmt, ...);
 // Maps a CUDA error (from a launch or an API call) to PB_ERR_CUDA with its text.
 int cuda_fail(cudaError_t err, const char* where);
 
+// Counts every kernel this library launches (read by pb_launch_count()).
+void count_launch();
+
 #define PB_CHECK_LAUNCH(where)                                   \
     do {                                                         \
+        ::pb::count_launch();                                    \
         cudaError_t e_ = cudaGetLastError();                     \
         if (e_ != cudaSuccess) return ::pb::cuda_fail(e_, where); \
     } while (0)

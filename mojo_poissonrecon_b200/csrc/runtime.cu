@@ -1,4 +1,5 @@
 // Error reporting, version and device check for the C ABI.
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 
@@ -7,6 +8,9 @@
 namespace pb {
 
 static thread_local char g_last_error[512] = "";
+static std::atomic<long long> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 int fail(int code, const char* fmt, ...) {
     va_list args;
@@ -25,6 +29,8 @@ int cuda_fail(cudaError_t err, const char* where) {
 extern "C" const char* pb_last_error(void) { return pb::g_last_error; }
 
 extern "C" int pb_version(void) { return 10000; }
+
+extern "C" long long pb_launch_count(void) { return pb::g_launches.load(std::memory_order_relaxed); }
 
 extern "C" int pb_init(int device) {
     cudaError_t e = cudaSetDevice(device);

@@ -25,6 +25,11 @@ from .solver import SolveStats, level_sizes, norm
 
 COARSE_N = 17  # levels of this side or smaller: one single-block launch
 
+# When set to a list, every finest-level sweep launch appends (start, end, mode)
+# CUDA events recorded on the launching stream around it (used by bench.py to
+# time the dominant kernel inside its timed region).
+PROBE: list | None = None
+
 
 class Level32:
     def __init__(self, n: int, screen64: torch.Tensor, pw: float, device: torch.device, lib, stream):
@@ -44,7 +49,10 @@ class Level32:
 class Hierarchy32:
     """FP32 levels (padded layout) built from the FP64 screen hierarchy."""
 
-    def __init__(self, screen: torch.Tensor, point_weight: float, workspace: nat.Workspace, z_chunk: int = 32):
+    def __init__(self, screen: torch.Tensor, point_weight: float, workspace: nat.Workspace, z_chunk: int = 0,
+                 use_tma: bool = True):
+        self.use_tma = use_tma
+        self.status = torch.zeros(1, dtype=torch.int32, device=screen.device)
         self.lib = nat.lib()
         self.stream = nat.stream_handle()
         self.ws = workspace
@@ -75,9 +83,29 @@ class Hierarchy32:
         )
 
     def _sweep(self, lv: Level32, src, dst, mode: int, coarse=None) -> None:
-        nat.check(self.lib.pb_sweep_f32(None if src is None else src.data_ptr(), dst.data_ptr(), lv.rhs.data_ptr(),
-                                        lv.invD.data_ptr(), None if coarse is None else coarse.data_ptr(), lv.n,
-                                        mode, self.z_chunk, self.stream), "sweep")
+        L = self.lib
+        if self.use_tma:
+            if mode == 2:  # prolongation added in place, then a plain sweep
+                nat.check(L.pb_prolong_add_f32(coarse.data_ptr(), src.data_ptr(), lv.n, self.stream), "prolong32")
+                mode = 0
+            probe = PROBE if (PROBE is not None and lv is self.levels[0]) else None
+            if probe is not None:
+                start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                start.record()
+            nat.check(L.pb_sweep_tma_f32(None if src is None else src.data_ptr(), dst.data_ptr(), lv.rhs.data_ptr(),
+                                         lv.invD.data_ptr(), lv.n, mode, self.z_chunk, self.status.data_ptr(),
+                                         self.stream), "sweep")
+            if probe is not None:
+                end.record()
+                probe.append((start, end, mode))
+            return
+        nat.check(L.pb_sweep_f32(None if src is None else src.data_ptr(), dst.data_ptr(), lv.rhs.data_ptr(),
+                                 lv.invD.data_ptr(), None if coarse is None else coarse.data_ptr(), lv.n,
+                                 mode, self.z_chunk if self.z_chunk > 0 else 32, self.stream), "sweep")
+
+    def check_status(self) -> None:
+        if int(self.status.item()):
+            raise RuntimeError("FP32 sweep: a bounded wait on a TMA barrier gave up (status word set)")
 
     def v_cycle(self, level: int = 0, pre: int = 3, post: int = 3) -> torch.Tensor:
         """Correction for levels[level].rhs from a zero start; returns its tensor."""
@@ -110,7 +138,7 @@ class Hierarchy32:
 
 def solve_refined(rhs: torch.Tensor, screen: torch.Tensor, point_weight: float, workspace: nat.Workspace, *,
                   tol: float = 1e-8, max_cycles: int = 200, has_points: bool = True,
-                  z_chunk: int = 32) -> tuple[torch.Tensor, SolveStats]:
+                  z_chunk: int = 0, use_tma: bool = True) -> tuple[torch.Tensor, SolveStats]:
     L = nat.lib()
     s = nat.stream_handle()
     n = rhs.shape[0]
@@ -124,7 +152,7 @@ def solve_refined(rhs: torch.Tensor, screen: torch.Tensor, point_weight: float, 
         return x, stats
     nat.check(L.pb_fill_f64(x.data_ptr(), x.numel(), 0.5, s), "fill")
     x_next = torch.empty_like(rhs)
-    h = Hierarchy32(screen, point_weight, workspace, z_chunk)
+    h = Hierarchy32(screen, point_weight, workspace, z_chunk, use_tma)
     bnorm = norm(rhs, workspace, torch.empty(1, dtype=torch.float64, device=device))
     norm2 = torch.empty(1, dtype=torch.float64, device=device)
     ws = nat.Workspace(device)
@@ -144,5 +172,6 @@ def solve_refined(rhs: torch.Tensor, screen: torch.Tensor, point_weight: float, 
         stats.cycles += 1
         r = math.sqrt(float(norm2.item()))
         stats.history.append(r)
+    h.check_status()
     stats.residual_norm = r
     return x, stats

@@ -94,6 +94,32 @@ def test_sweep_matches_fp64_relax(L, oracle, n, z_chunk, mode):
     assert ghosts_zero(L, e_out, n)
 
 
+@pytest.mark.parametrize("n,z_chunk", [(33, 0), (33, 5), (65, 0), (129, 3), (257, 0), (257, 100), (513, 0)])
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_tma_sweep_matches_fp64_relax(L, oracle, n, z_chunk, mode):
+    """TMA-staged sweep (mode 2 = prolongation added in place first)."""
+    screen, rhs, x, D, invD, _ = setup(L, n, 7 * n + mode)
+    cn = (n + 1) // 2
+    coarse = np.random.default_rng(2).normal(size=(cn,) * 3).astype(np.float32).astype(np.float64)
+    start = x.copy() if mode != 1 else np.zeros_like(x)
+    if mode == 2:
+        oracle.lib().mpr_prolong_add_f64(_a(coarse), _a(start), n)
+    want = start.copy()
+    oracle.lib().mpr_relax_f64(_a(want), _a(rhs), _a(screen), n, 4.0, 1)
+    e_in, rhs32, c32 = to_padded(L, x), to_padded(L, rhs.astype(np.float32)), to_padded(L, coarse)
+    e_out = torch.zeros_like(e_in)
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    if mode == 2:
+        assert L.pb_prolong_add_f32(c32.data_ptr(), e_in.data_ptr(), n, s) == 0
+    assert L.pb_sweep_tma_f32(e_in.data_ptr(), e_out.data_ptr(), rhs32.data_ptr(), invD.data_ptr(), n,
+                              1 if mode == 1 else 0, z_chunk, status.data_ptr(), s) == 0, L.pb_last_error()
+    assert int(status.item()) == 0
+    got = from_padded(L, e_out, n)
+    assert np.allclose(got, want, rtol=0, atol=2e-6 * np.abs(want).max())
+    assert ghosts_zero(L, e_out, n)
+
+
 @pytest.mark.parametrize("n", [5, 17, 65, 129])
 def test_residual32_restrict32_match_oracle(L, oracle, n):
     screen, rhs, x, D, invD, _ = setup(L, n, 3 * n)
@@ -112,7 +138,8 @@ def test_residual32_restrict32_match_oracle(L, oracle, n):
     res_in = to_padded(L, want)
     assert L.pb_restrict_f32(res_in.data_ptr(), coarse.data_ptr(), n, s) == 0
     c_ref = np.empty((cn,) * 3)
-    oracle.lib().mpr_restrict_f64(_a(want.astype(np.float32).astype(np.float64)), _a(c_ref), n)
+    want32 = want.astype(np.float32).astype(np.float64)  # a named array: _a() takes its address
+    oracle.lib().mpr_restrict_f64(_a(want32), _a(c_ref), n)
     assert np.allclose(from_padded(L, coarse, cn), c_ref, rtol=0, atol=2e-6 * np.abs(c_ref).max())
 
 
