@@ -153,6 +153,16 @@ int pb_dual_vertices_f64_isoptr(const double *field, const double *density, int6
                                 double *vertex_density, int64_t capacity, int64_t *count,
                                 void *workspace, size_t workspace_bytes, void *stream);
 
+/* Active-cell count of pb_dual_vertices_f64's count mode, for callers that
+ * cannot allocate device memory (no workspace argument).  No counterpart in
+ * the reference: its count mode writes into the caller's scratch buffer.
+ * Scratch is a fixed 512 KiB array in the library's device memory, so
+ * n <= 513; larger grids get PB_ERR_INVALID.  The first call on a device
+ * looks the array up (make it before any stream capture); calls that overlap
+ * on the GPU share the array and race. */
+int pb_dual_vertex_count_f64_noalloc(const double *field, int64_t n, double iso, int64_t *count,
+                                     void *stream);
+
 /* mpr_dual_faces_f64 (_lib.py:31; capi.mojo:1076-1129): two triangles per
  * sign-changing interior edge (x-edges, then y-edges, then z-edges, each in
  * z,y,x order); faces are written while 2 more fit in `capacity`; *count

@@ -45,6 +45,7 @@ _SIGNATURES = {
     "pb_dual_workspace_size": ([I], S),
     "pb_dual_vertices_f64": ([P, P, I, F, P, P, P, I, P, P, S, P], C),
     "pb_dual_vertices_f64_isoptr": ([P, P, I, P, P, P, P, I, P, P, S, P], C),
+    "pb_dual_vertex_count_f64_noalloc": ([P, I, F, P, P], C),
     "pb_dual_faces_f64": ([P, I, F, P, P, I, P, P, S, P], C),
     "pb_dual_faces_f64_isoptr": ([P, I, P, P, P, I, P, P, S, P], C),
     "pb_scale_f64": ([P, I, F, P], C),
