@@ -185,12 +185,23 @@ int pb_level_geometry(int64_t n, int64_t *pitch, int64_t *padded_count);
 /* D = (degree + pw*screen)*(n-1)^2 and 1/D per node from the dense FP64 screen. */
 int pb_level_setup_f32(const double *screen, int64_t n, double point_weight, float *D, float *invD,
                        void *stream);
-/* r32 = b - A x in FP64 (dense x, b, screen; r32 padded), *norm2 = ||b - A x||^2.
- * With e != NULL the iterate is first updated: x_new = x_old + e (written). */
+/* r32 = b - A x in FP64 (dense x, b, screen; r32 padded), *norm2 = ||b - A x||^2,
+ * and the FP64 residual into r64 when it is not NULL.  With e != NULL the
+ * iterate is first updated: x_new = x_old + e (written). */
 size_t pb_defect_workspace_size(int64_t n);
 int pb_defect_f64(const double *x_old, const float *e, double *x_new, const double *rhs,
-                  const double *screen, int64_t n, double point_weight, float *r32, double *norm2,
-                  void *workspace, size_t workspace_bytes, void *stream);
+                  const double *screen, int64_t n, double point_weight, float *r32, double *r64,
+                  double *norm2, void *workspace, size_t workspace_bytes, void *stream);
+/* One step of FP64 flexible conjugate gradients, FCG(1), preconditioned by the
+ * FP32 V-cycle: from z = M(r) (padded FP32) form p = z - beta p_prev,
+ * q = A p, alpha = (p, r)/(p, q), x += alpha p, r -= alpha q, r32 = (float) r,
+ * with the scalars kept in scal[0..4] on the device (scal[4] = ||r||^2).
+ * first != 0 on the first step (p_prev unused).  No counterpart in the
+ * reference, which repeats V-cycles (core.py:274-285). */
+size_t pb_fcg_workspace_size(int64_t n);
+int pb_fcg_step_f64(const float *z, const double *p_prev, double *p, double *q, double *x, double *r,
+                    float *r32, const double *screen, int64_t n, double point_weight, double *scal,
+                    int64_t first, void *workspace, size_t workspace_bytes, void *stream);
 /* One red-black Gauss-Seidel sweep (colour 0 then colour 1), out of place.
  * mode 0: from e_in; 1: from zero (e_in unused); 2: from e_in + trilinear
  * prolongation of `coarse` (side (n+1)/2).  n = 2^k + 1. */

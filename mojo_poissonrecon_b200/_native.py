@@ -58,7 +58,9 @@ _SIGNATURES = {
     "pb_level_geometry": ([I, P, P], C),
     "pb_level_setup_f32": ([P, I, F, P, P, P], C),
     "pb_defect_workspace_size": ([I], S),
-    "pb_defect_f64": ([P, P, P, P, P, I, F, P, P, P, S, P], C),
+    "pb_defect_f64": ([P, P, P, P, P, I, F, P, P, P, P, S, P], C),
+    "pb_fcg_workspace_size": ([I], S),
+    "pb_fcg_step_f64": ([P, P, P, P, P, P, P, P, I, F, P, I, P, S, P], C),
     "pb_sweep_f32": ([P, P, P, P, P, I, I, I, P], C),
     "pb_sweep_tma_f32": ([P, P, P, P, I, I, I, P, P], C),
     "pb_prolong_add_f32": ([P, P, I, P], C),

@@ -7,7 +7,7 @@ written against the reference runs unchanged.  Inputs may be NumPy arrays
 NumPy arrays, or CUDA tensors with ``device_out=True``.
 
 Extensions (keyword-only, defaults keep the reference's behaviour):
-``precision`` ("fp64" | "fp32_refined"), ``tol`` (stop on the relative
+``precision`` ("fp64" | "fp32_refined" | "fp32_defect"), ``tol`` (stop on the relative
 residual instead of a fixed cycle count), ``max_cycles``, ``device_out``.
 The depth cap is lifted from 8 to 10.
 """
@@ -24,7 +24,9 @@ from . import solver
 from ._convert import f64, i64
 
 MAX_DEPTH = 10
-PRECISIONS = ("fp64", "fp32_refined")
+# fp32_refined: FP64 FCG(1) preconditioned by FP32 V-cycles; fp32_defect: plain
+# FP64 defect correction x += V(r) with FP32 V-cycles.
+PRECISIONS = ("fp64", "fp32_refined", "fp32_defect")
 
 
 @dataclass(frozen=True)
@@ -232,7 +234,7 @@ def _iso_value(ctx: _Context, field: torch.Tensor, points: torch.Tensor, normals
 
 def _solve_device(ctx: _Context, points: torch.Tensor, normals: torch.Tensor, *, depth: int, point_weight: float,
                   confidence: bool, cycles: int, samples_per_node: float, precision: str, tol, max_cycles: int,
-                  octree: bool):
+                  octree: bool, refine_method: str = "fcg"):
     tree = _octree_device(ctx, points, depth) if octree else None
     grids, accepted = _splat_assemble(ctx, points, normals, depth, point_weight, confidence, samples_per_node)
     count = points.shape[0]
@@ -243,7 +245,8 @@ def _solve_device(ctx: _Context, points: torch.Tensor, normals: torch.Tensor, *,
         from . import solver32
         field, stats = solver32.solve_refined(grids["rhs"], grids["screen"], point_weight, ctx.ws,
                                               tol=1e-8 if tol is None else tol, max_cycles=max_cycles,
-                                              has_points=count > 0)
+                                              has_points=count > 0,
+                                              method="defect" if precision == "fp32_defect" else refine_method)
     iso = _iso_value(ctx, field, points, normals, confidence)
     if count and int(accepted.item()) != count:
         raise RuntimeError(f"splat accepted {int(accepted.item())} of {count} validated samples")

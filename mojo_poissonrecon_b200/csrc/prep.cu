@@ -84,15 +84,34 @@ __global__ void bbox_partial_kernel(const double* __restrict__ points, const uin
     }
 }
 
-// map[0..2] = origin, map[3] = width (core.py:377-385).
+// map[0..2] = origin, map[3] = width (core.py:377-385).  Min and max are exact
+// in any order, so the block-parallel reduction gives the serial result.
 __global__ void bbox_finish_kernel(const double* __restrict__ partial, int blocks, double scale,
                                    double* __restrict__ map) {
-    if (threadIdx.x || blockIdx.x) return;
+    __shared__ double lo[3][32], hi[3][32];
     double l[3] = {INFINITY, INFINITY, INFINITY}, h[3] = {-INFINITY, -INFINITY, -INFINITY};
-    for (int b = 0; b < blocks; ++b)
+    for (int b = threadIdx.x; b < blocks; b += blockDim.x)
         for (int k = 0; k < 3; ++k) {
             l[k] = fmin(l[k], partial[6 * b + k]);
             h[k] = fmax(h[k], partial[6 * b + 3 + k]);
+        }
+    for (int k = 0; k < 3; ++k)
+        for (int o = 16; o > 0; o >>= 1) {
+            l[k] = fmin(l[k], __shfl_down_sync(0xffffffffu, l[k], o));
+            h[k] = fmax(h[k], __shfl_down_sync(0xffffffffu, h[k], o));
+        }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int k = 0; k < 3; ++k) {
+            lo[k][warp] = l[k];
+            hi[k][warp] = h[k];
+        }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+        for (int k = 0; k < 3; ++k) {
+            l[k] = fmin(l[k], lo[k][w]);
+            h[k] = fmax(h[k], hi[k][w]);
         }
     double extent = fmax(h[0] - l[0], fmax(h[1] - l[1], h[2] - l[2]));
     double width = extent * scale;
@@ -179,7 +198,7 @@ extern "C" int pb_prepare_points_f64(const double* points, const double* normals
     if (scale > 0.0) {
         bbox_partial_kernel<<<pb_blocks, 256, 0, s>>>(out_points, total, partial);
         PB_CHECK_LAUNCH("bbox_partial_kernel");
-        bbox_finish_kernel<<<1, 32, 0, s>>>(partial, (int)pb_blocks, scale, map);
+        bbox_finish_kernel<<<1, 256, 0, s>>>(partial, (int)pb_blocks, scale, map);
         PB_CHECK_LAUNCH("bbox_finish_kernel");
         normalize_kernel<<<capped_blocks(3 * point_count), 256, 0, s>>>(out_points, total, map);
         PB_CHECK_LAUNCH("normalize_kernel");

@@ -47,59 +47,72 @@ __global__ void level_setup_kernel(const double* __restrict__ screen, Geom g, do
 
 // ---- FP64 defect with the fused update x_new = x_old + e ------------------------
 // r32 = (float)(b - A x_new) into the padded level-0 rhs, ||b - A x_new||^2 per block.
-constexpr int kDefThreads = 256;
-
+// Block-wide sum (valid in linear thread 0) for 1-D, 2-D or 3-D blocks.
 __device__ __forceinline__ double warp_block_sum(double v, double* shared) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int warps = (blockDim.x * blockDim.y * blockDim.z) >> 5;
     if (lane == 0) shared[warp] = v;
     __syncthreads();
     double r = 0.0;
     if (warp == 0) {
-        r = lane < (int)(blockDim.x >> 5) ? shared[lane] : 0.0;
+        r = lane < warps ? shared[lane] : 0.0;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
     }
     return r;
 }
 
+// Tiled variant: a block owns a 64 x 4 (x, y) tile and a z range; coordinates
+// come from the launch shape (no 64-bit division per node), rows are read
+// coalesced, and the z-neighbours of consecutive planes stay in L1/L2.
+constexpr int kDefTX = 64, kDefTY = 4, kDefZ = 16;
+
 template <bool UPDATE>
-__global__ void __launch_bounds__(kDefThreads) defect_kernel(const double* __restrict__ x_old,
-                                                             const float* __restrict__ e, double* __restrict__ x_new,
-                                                             const double* __restrict__ b,
-                                                             const double* __restrict__ screen, Geom g, double pw,
-                                                             float* __restrict__ r32, double* __restrict__ partial) {
+__global__ void __launch_bounds__(kDefTX* kDefTY) defect_tile_kernel(
+    const double* __restrict__ x_old, const float* __restrict__ e, double* __restrict__ x_new,
+    const double* __restrict__ b, const double* __restrict__ screen, Geom g, double pw, float* __restrict__ r32,
+    double* __restrict__ r64, double* __restrict__ partial) {
     __shared__ double shared[32];
     const int n = g.n;
-    const int64_t nn = (int64_t)n * n, total = nn * n;
+    const int x = blockIdx.x * kDefTX + threadIdx.x;
+    const int y = blockIdx.y * kDefTY + threadIdx.y;
+    const int z0 = blockIdx.z * kDefZ, z1 = min(n, z0 + kDefZ);
     const double h = (double)(n - 1), h2 = h * h;
+    const int64_t nn = (int64_t)n * n;
     double sq = 0.0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % n), y = (int)((i / n) % n), z = (int)(i / nn);
-        const int64_t p = g.at(x, y, z);
-        auto val = [&](int64_t di, int64_t dp) -> double {
-            double v = x_old[i + di];
-            if (UPDATE) v += (double)e[p + dp];
-            return v;
-        };
-        double s = 0.0;
-        int deg = 0;
-        if (x > 0) { s += val(-1, -1); ++deg; }
-        if (x + 1 < n) { s += val(1, 1); ++deg; }
-        if (y > 0) { s += val(-n, -g.P); ++deg; }
-        if (y + 1 < n) { s += val(n, g.P); ++deg; }
-        if (z > 0) { s += val(-nn, -g.plane); ++deg; }
-        if (z + 1 < n) { s += val(nn, g.plane); ++deg; }
-        const double xc = val(0, 0);
-        if (UPDATE) x_new[i] = xc;
-        const double applied = ((double)deg * h2 + pw * screen[i] * h2) * xc - s * h2;
-        const double r = b[i] - applied;
-        r32[p] = (float)r;
-        sq += r * r;
+    if (x < n && y < n) {
+        const int degxy = (x > 0) + (x + 1 < n) + (y > 0) + (y + 1 < n);
+        for (int z = z0; z < z1; ++z) {
+            const int64_t i = (int64_t)z * nn + (int64_t)y * n + x;
+            const int64_t p = g.at(x, y, z);
+            auto val = [&](int64_t di, int64_t dp) -> double {
+                double v = x_old[i + di];
+                if (UPDATE) v += (double)e[p + dp];
+                return v;
+            };
+            double s = 0.0;
+            if (x > 0) s += val(-1, -1);
+            if (x + 1 < n) s += val(1, 1);
+            if (y > 0) s += val(-n, -g.P);
+            if (y + 1 < n) s += val(n, g.P);
+            if (z > 0) s += val(-nn, -g.plane);
+            if (z + 1 < n) s += val(nn, g.plane);
+            const int deg = degxy + (z > 0) + (z + 1 < n);
+            const double xc = val(0, 0);
+            if (UPDATE) x_new[i] = xc;
+            const double applied = ((double)deg * h2 + pw * screen[i] * h2) * xc - s * h2;
+            const double r = b[i] - applied;
+            r32[p] = (float)r;
+            if (r64) r64[i] = r;
+            sq += r * r;
+        }
     }
     const double t = warp_block_sum(sq, shared);
-    if (threadIdx.x == 0) partial[blockIdx.x] = t;
+    if (threadIdx.x == 0 && threadIdx.y == 0)
+        partial[(blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = t;
 }
 
 __global__ void sum_partials_kernel(const double* __restrict__ partial, int count, double* __restrict__ out) {
@@ -398,7 +411,14 @@ static unsigned stride_grid(int64_t items, int threads, int per_sm = 16) {
     return (unsigned)(b < 1 ? 1 : b);
 }
 
-unsigned defect_blocks(int n) { return stride_grid((int64_t)n * n * n, kDefThreads); }
+static dim3 defect_grid(int n) {
+    return dim3((n + kDefTX - 1) / kDefTX, (n + kDefTY - 1) / kDefTY, (n + kDefZ - 1) / kDefZ);
+}
+
+unsigned defect_blocks(int n) {
+    const dim3 g = defect_grid(n);
+    return g.x * g.y * g.z;
+}
 
 }  // namespace pb
 
@@ -423,8 +443,8 @@ extern "C" int pb_level_setup_f32(const double* screen, int64_t n, double point_
 extern "C" size_t pb_defect_workspace_size(int64_t n) { return (size_t)defect_blocks((int)(n < 2 ? 2 : n)) * 8 + 256; }
 
 extern "C" int pb_defect_f64(const double* x_old, const float* e, double* x_new, const double* rhs,
-                             const double* screen, int64_t n, double point_weight, float* r32, double* norm2,
-                             void* workspace, size_t workspace_bytes, void* stream) {
+                             const double* screen, int64_t n, double point_weight, float* r32, double* r64,
+                             double* norm2, void* workspace, size_t workspace_bytes, void* stream) {
     if (n < 2 || n > 4097 || !x_old || !rhs || !screen || !r32 || !norm2) return fail(PB_ERR_INVALID, "defect: bad args");
     if (e && !x_new) return fail(PB_ERR_INVALID, "defect: update needs x_new");
     if (e && x_new == x_old) return fail(PB_ERR_INVALID, "defect: x_new must not alias x_old");
@@ -432,14 +452,15 @@ extern "C" int pb_defect_f64(const double* x_old, const float* e, double* x_new,
     if (!workspace || workspace_bytes < (size_t)blocks * 8) return fail(PB_ERR_WORKSPACE, "defect: workspace too small");
     cudaStream_t s = (cudaStream_t)stream;
     double* partial = (double*)workspace;
+    const dim3 grid = defect_grid((int)n), block(kDefTX, kDefTY);
     if (e)
-        defect_kernel<true><<<blocks, kDefThreads, 0, s>>>(x_old, e, x_new, rhs, screen, geom((int)n), point_weight,
-                                                           r32, partial);
+        defect_tile_kernel<true><<<grid, block, 0, s>>>(x_old, e, x_new, rhs, screen, geom((int)n), point_weight, r32,
+                                                        r64, partial);
     else
-        defect_kernel<false><<<blocks, kDefThreads, 0, s>>>(x_old, nullptr, nullptr, rhs, screen, geom((int)n),
-                                                            point_weight, r32, partial);
-    PB_CHECK_LAUNCH("defect_kernel");
-    sum_partials_kernel<<<1, 256, 0, s>>>(partial, (int)blocks, norm2);
+        defect_tile_kernel<false><<<grid, block, 0, s>>>(x_old, nullptr, nullptr, rhs, screen, geom((int)n),
+                                                         point_weight, r32, r64, partial);
+    PB_CHECK_LAUNCH("defect_tile_kernel");
+    sum_partials_kernel<<<1, 1024, 0, s>>>(partial, (int)blocks, norm2);
     PB_CHECK_LAUNCH("sum_partials_kernel");
     return PB_OK;
 }

@@ -213,6 +213,168 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
 }
 
+// ---- version 2: in-place colour-0 updates on float4 column groups -------------
+// The state ring holds e for planes t-2 .. t+3.  Colour 0 of plane t is
+// updated in place (float4 groups of 4 columns, 18 groups per 72-column box
+// row); colour 1 of plane t-1 is computed into registers and written out with
+// the colour-0 values of the same group as one float4 store.  A colour-0
+// update reads only colour-1 nodes and vice versa, so in-place stores never
+// change a value another thread of the same phase reads.  For a group at box
+// row br on plane t (colour 0) or t-1 (colour 1), the updated columns are
+// j = s and s + 2 with s = (br + t) & 1, because x0 and y0 are even.
+constexpr int kGroups = kBoxX / 4;  // 18
+
+// Geometry of one v2 configuration: tile height TY (the last y tile holds
+// TY + 1 rows), SLOTS planes in the ring (SLOTS - 4 planes of prefetch).
+template <int TY, int SLOTS>
+struct Geo2 {
+    static constexpr int kBoxRows = TY + 1 + 4;
+    static constexpr int kBox = kBoxX * kBoxRows;
+    static constexpr int kStride = (kBox + 31) / 32 * 32;  // 128-byte aligned slot arrays
+    struct Smem {
+        float slot[SLOTS][3][kStride];
+        unsigned long long bar[SLOTS];
+    };
+};
+
+__device__ __forceinline__ float4 lds4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+
+template <bool ZERO_IN, int TY, int SLOTS>
+__global__ void __launch_bounds__(kThreads, 2)
+    sweep_v2_kernel(const __grid_constant__ CUtensorMap map_e, const __grid_constant__ CUtensorMap map_rhs,
+                    const __grid_constant__ CUtensorMap map_invD, Params p) {
+    using G = Geo2<TY, SLOTS>;
+    constexpr int kSlots2 = SLOTS;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const uint32_t raw = saddr(smem_raw);
+    typename G::Smem& S = *reinterpret_cast<typename G::Smem*>(smem_raw + (((raw + 127u) & ~127u) - raw));
+    const int n = p.n;
+    const int bx = blockIdx.x, by = blockIdx.y;
+    const int x0 = bx * kTX, y0 = by * TY;
+    const int W = (bx == p.ntx - 1 ? n : x0 + kTX) - x0;
+    const int H = (by == p.nty - 1 ? n : y0 + TY) - y0;
+    const int zb = blockIdx.z * p.z_chunk;
+    const int ze = min(n, zb + p.z_chunk);
+    const int zfirst = zb - 2, zlast = ze + 1;
+    const int tid = threadIdx.x;
+    const uint32_t bytes = (ZERO_IN ? 2u : 3u) * G::kBox * 4u;
+    const float h2 = p.h2;
+
+    if (tid == 0) {
+        for (int s = 0; s < kSlots2; ++s) bar_init(&S.bar[s]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    auto slot_of = [&](int z) { return (z - zfirst) % kSlots2; };
+    auto parity_of = [&](int z) { return (uint32_t)(((z - zfirst) / kSlots2) & 1); };
+    auto issue = [&](int z) {
+        const int s = slot_of(z);
+        bar_expect(&S.bar[s], bytes);
+        if (!ZERO_IN) load_box(S.slot[s][0], &map_e, x0, y0 - 1, z + 1, &S.bar[s]);
+        load_box(S.slot[s][1], &map_rhs, x0, y0 - 1, z + 1, &S.bar[s]);
+        load_box(S.slot[s][2], &map_invD, x0, y0 - 1, z + 1, &S.bar[s]);
+    };
+    int issued = zfirst;
+    if (tid == 0)
+        for (; issued <= zlast && issued < zfirst + kSlots2; ++issued) issue(issued);
+
+    bool ok = bar_wait(&S.bar[slot_of(zfirst)], parity_of(zfirst));
+    ok = bar_wait(&S.bar[slot_of(zfirst + 1)], parity_of(zfirst + 1)) && ok;
+    ok = __syncthreads_and(ok);
+
+    const int itemsA = (H + 2) * kGroups;
+    const int groupsB = (W + 3) / 4;  // groups 1 .. groupsB cover box columns 4 .. W+3
+    const int itemsB = H * groupsB;
+    for (int t = zb - 1; t <= ze && ok; ++t) {
+        const bool arrived = bar_wait(&S.bar[slot_of(t + 1)], parity_of(t + 1));
+        {  // colour 0 of plane t on box rows 1 .. H+2, columns 3 .. W+4
+            float* e = S.slot[slot_of(t)][0];
+            const float* em = S.slot[slot_of(t - 1)][0];
+            const float* ep = S.slot[slot_of(t + 1)][0];
+            const float* rhs = S.slot[slot_of(t)][1];
+            const float* inv = S.slot[slot_of(t)][2];
+            for (int i = tid; i < itemsA; i += kThreads) {
+                const int br = 1 + i / kGroups, g = i - (br - 1) * kGroups;
+                const int base = br * kBoxX + 4 * g;
+                const int s = (br + t) & 1;
+                const float4 r4 = lds4(rhs + base), i4 = lds4(inv + base);
+                float4 c = lds4(e + base);
+                float v[4];
+                if (ZERO_IN) {
+                    v[0] = r4.x * i4.x; v[1] = r4.y * i4.y; v[2] = r4.z * i4.z; v[3] = r4.w * i4.w;
+                } else {
+                    const float4 u = lds4(e + base - kBoxX), d = lds4(e + base + kBoxX);
+                    const float4 zm = lds4(em + base), zp = lds4(ep + base);
+                    const float L = g > 0 ? e[base - 1] : 0.0f;
+                    const float R = g < kGroups - 1 ? e[base + 4] : 0.0f;
+                    v[0] = (r4.x + (L + c.y + u.x + d.x + zm.x + zp.x) * h2) * i4.x;
+                    v[1] = (r4.y + (c.x + c.z + u.y + d.y + zm.y + zp.y) * h2) * i4.y;
+                    v[2] = (r4.z + (c.y + c.w + u.z + d.z + zm.z + zp.z) * h2) * i4.z;
+                    v[3] = (r4.w + (c.z + R + u.w + d.w + zm.w + zp.w) * h2) * i4.w;
+                }
+                const int b0 = 4 * g;
+                float cc[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const bool upd = ((j & 1) == s) && (b0 + j >= 3) && (b0 + j < W + 5);
+                    cc[j] = upd ? v[j] : cc[j];
+                }
+                *reinterpret_cast<float4*>(e + base) = make_float4(cc[0], cc[1], cc[2], cc[3]);
+            }
+        }
+        ok = __syncthreads_and(arrived);
+        if (!ok) break;
+        if (t - 1 >= zb) {  // colour 1 of plane t-1 on the tile, written with colour 0
+            const int z = t - 1;
+            const float* e = S.slot[slot_of(z)][0];
+            const float* em = S.slot[slot_of(z - 1)][0];
+            const float* ep = S.slot[slot_of(z + 1)][0];
+            const float* rhs = S.slot[slot_of(z)][1];
+            const float* inv = S.slot[slot_of(z)][2];
+            for (int i = tid; i < itemsB; i += kThreads) {
+                const int r = i / groupsB;
+                const int g = 1 + (i - r * groupsB);
+                const int br = r + 2;
+                const int base = br * kBoxX + 4 * g;
+                const int s = (br + t) & 1;
+                const float4 c = lds4(e + base), u = lds4(e + base - kBoxX), d = lds4(e + base + kBoxX);
+                const float4 zm = lds4(em + base), zp = lds4(ep + base);
+                const float4 r4 = lds4(rhs + base), i4 = lds4(inv + base);
+                const float L = e[base - 1];
+                const float R = g < kGroups - 1 ? e[base + 4] : 0.0f;
+                float v[4];
+                v[0] = (r4.x + (L + c.y + u.x + d.x + zm.x + zp.x) * h2) * i4.x;
+                v[1] = (r4.y + (c.x + c.z + u.y + d.y + zm.y + zp.y) * h2) * i4.y;
+                v[2] = (r4.z + (c.y + c.w + u.z + d.z + zm.z + zp.z) * h2) * i4.z;
+                v[3] = (r4.w + (c.z + R + u.w + d.w + zm.w + zp.w) * h2) * i4.w;
+                float o[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j) o[j] = ((j & 1) == s) ? v[j] : o[j];
+                float* dst = p.e_out + ((int64_t)(z + 1) * (n + 2) + (y0 - 1 + br)) * p.P + (x0 + 4 * g);
+                const int valid = W + 4 - 4 * g;  // columns of this group inside the tile
+                if (valid >= 4) {
+                    *reinterpret_cast<float4*>(dst) = make_float4(o[0], o[1], o[2], o[3]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 3; ++j)
+                        if (j < valid) dst[j] = o[j];
+                }
+            }
+        }
+        __syncthreads();  // plane t-2 is no longer read
+        if (tid == 0 && t - 2 >= zfirst && issued <= zlast) issue(issued++);
+    }
+    if (!ok) {
+        if (tid == 0) {
+            atomicExch(p.status, 1);
+            for (int z = max(zfirst, issued - kSlots2); z < issued; ++z)
+                (void)bar_wait(&S.bar[slot_of(z)], parity_of(z));
+        }
+        __syncthreads();
+    }
+}
+
 typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -229,14 +391,14 @@ static EncodeTiled encoder() {
     return fn;
 }
 
-// 3D map over a padded level: dims (P, n+2, n+2) floats, box (72, 21, 1).
-static int make_map(CUtensorMap* map, const float* base, int n, int P) {
+// 3D map over a padded level: dims (P, n+2, n+2) floats, box (72, rows, 1).
+static int make_map(CUtensorMap* map, const float* base, int n, int P, int rows) {
     EncodeTiled enc = encoder();
     if (!enc) return fail(PB_ERR_CUDA, "sweep: cuTensorMapEncodeTiled is unavailable");
     if (reinterpret_cast<uintptr_t>(base) & 15) return fail(PB_ERR_INVALID, "sweep: arrays must be 16-byte aligned");
     const cuuint64_t dims[3] = {(cuuint64_t)P, (cuuint64_t)(n + 2), (cuuint64_t)(n + 2)};
     const cuuint64_t strides[2] = {(cuuint64_t)P * 4, (cuuint64_t)P * (n + 2) * 4};
-    const cuuint32_t box[3] = {kBoxX, kBoxY, 1};
+    const cuuint32_t box[3] = {kBoxX, (cuuint32_t)rows, 1};
     const cuuint32_t estride[3] = {1, 1, 1};
     CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, estride,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -276,57 +438,84 @@ static int pitch_for(int n) { return ((n + 5) + 7) & ~7; }
 // single-block coarse kernel).  mode 0: from e_in; mode 1: from zero.
 // z_chunk <= 0 picks one that fills the 148 SMs with two blocks each.
 // *status (device int) is set to 1 if a bounded wait gave up.
+template <typename K>
+static int launch_sweep(K kernel, size_t smem, int ty, int n, int z_chunk, cudaStream_t s, const float* e_in,
+                        const float* rhs, const float* invD, pb::tma::Params prm) {
+    using namespace pb::tma;
+    const int P = prm.P;
+    prm.nty = (n - 1) / ty > 0 ? (n - 1) / ty : 1;
+    const int tiles = prm.ntx * prm.nty;
+    int per_sm = (int)((228 * 1024) / (smem + 1024));
+    if (per_sm < 1) per_sm = 1;
+    if (per_sm > 2) per_sm = 2 + (per_sm > 2);  // register file: at most 3 blocks of 256 threads
+    if (z_chunk <= 0) {
+        const int want = per_sm * kSMs;
+        int chunks = want / tiles > 1 ? want / tiles : 1;
+        z_chunk = (n + chunks - 1) / chunks;
+        if (z_chunk < 4) z_chunk = 4;
+    }
+    prm.z_chunk = z_chunk;
+    CUtensorMap me, mr, mi;
+    const int rows = ty + 5;
+    PB_TRY(make_map(&mr, rhs, n, P, rows));
+    PB_TRY(make_map(&mi, invD, n, P, rows));
+    PB_TRY(make_map(&me, e_in ? e_in : rhs, n, P, rows));
+    const dim3 grid(prm.ntx, prm.nty, (n + z_chunk - 1) / z_chunk);
+    PB_CHECK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                  "sweep_tma smem");
+    kernel<<<grid, kThreads, smem, s>>>(me, mr, mi, prm);
+    PB_CHECK_LAUNCH("sweep_tma kernel");
+    return PB_OK;
+}
+
+template <int TY, int SLOTS>
+static int launch_v2(bool zero_in, int n, int z_chunk, cudaStream_t s, const float* e_in, const float* rhs,
+                     const float* invD, const pb::tma::Params& prm) {
+    using namespace pb::tma;
+    const size_t smem = sizeof(typename Geo2<TY, SLOTS>::Smem) + 128;
+    return zero_in ? launch_sweep(sweep_v2_kernel<true, TY, SLOTS>, smem, TY, n, z_chunk, s, nullptr, rhs, invD, prm)
+                   : launch_sweep(sweep_v2_kernel<false, TY, SLOTS>, smem, TY, n, z_chunk, s, e_in, rhs, invD, prm);
+}
+
+// Bits 8..15 of `mode` select a tile-height / ring-depth configuration of the
+// kernel (0: 16 rows, 6 slots — the default); bit 2 selects the first TMA
+// version.  Both are there for tuning runs.
 extern "C" int pb_sweep_tma_f32(const float* e_in, float* e_out, const float* rhs, const float* invD, int64_t n,
                                 int64_t mode, int64_t z_chunk, int* status, void* stream) {
     using namespace pb::tma;
+    const bool legacy = (mode & 4) != 0;
+    const int variant = (int)((mode >> 8) & 0xff);
+    mode &= 3;
     if (n < 33 || n > 4097 || ((n - 1) & (n - 2)) || !e_out || !rhs || !invD || !status || (mode == 0 && !e_in) ||
-        mode < 0 || mode > 1)
+        mode > 1 || variant > 5)
         return fail(PB_ERR_INVALID, "sweep_tma: bad args (n must be 2^k + 1 >= 33)");
     if (e_in == e_out) return fail(PB_ERR_INVALID, "sweep_tma: out of place only");
-    const int N = (int)n, P = pitch_for(N);
+    const int N = (int)n;
     Params prm;
     prm.n = N;
-    prm.P = P;
-    prm.plane = (int64_t)(N + 2) * P;
+    prm.P = pitch_for(N);
+    prm.plane = (int64_t)(N + 2) * prm.P;
     prm.ntx = (N - 1) / kTX > 0 ? (N - 1) / kTX : 1;
-    prm.nty = (N - 1) / kTY > 0 ? (N - 1) / kTY : 1;
-    const int tiles = prm.ntx * prm.nty;
-    if (z_chunk <= 0) {
-        const int want = 2 * kSMs;
-        int chunks = want / tiles > 1 ? want / tiles : 1;
-        z_chunk = (N + chunks - 1) / chunks;
-        if (z_chunk < 4) z_chunk = 4;
-    }
-    prm.z_chunk = (int)z_chunk;
+    prm.nty = 1;
+    prm.z_chunk = 0;
     prm.h2 = (float)((N - 1) * (N - 1));
     prm.e_out = e_out;
     prm.status = status;
-    CUtensorMap me, mr, mi;
-    PB_TRY(make_map(&mr, rhs, N, P));
-    PB_TRY(make_map(&mi, invD, N, P));
-    PB_TRY(make_map(&me, mode == 1 ? rhs : e_in, N, P));
-    const dim3 grid(prm.ntx, prm.nty, (N + prm.z_chunk - 1) / prm.z_chunk);
-    const size_t smem = sizeof(Smem) + 128;
     cudaStream_t s = (cudaStream_t)stream;
-    if (mode == 1) {
-        static bool attr1 = false;
-        if (!attr1) {
-            PB_CHECK_CUDA(cudaFuncSetAttribute(sweep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                          "sweep_tma smem");
-            attr1 = true;
-        }
-        sweep_kernel<true><<<grid, kThreads, smem, s>>>(me, mr, mi, prm);
-    } else {
-        static bool attr0 = false;
-        if (!attr0) {
-            PB_CHECK_CUDA(cudaFuncSetAttribute(sweep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                          "sweep_tma smem");
-            attr0 = true;
-        }
-        sweep_kernel<false><<<grid, kThreads, smem, s>>>(me, mr, mi, prm);
+    const bool zero = mode == 1;
+    if (legacy) {
+        const size_t smem = sizeof(Smem) + 128;
+        return zero ? launch_sweep(sweep_kernel<true>, smem, kTY, N, (int)z_chunk, s, nullptr, rhs, invD, prm)
+                    : launch_sweep(sweep_kernel<false>, smem, kTY, N, (int)z_chunk, s, e_in, rhs, invD, prm);
     }
-    PB_CHECK_LAUNCH("sweep_tma kernel");
-    return PB_OK;
+    switch (variant) {
+        case 1: return launch_v2<16, 8>(zero, N, (int)z_chunk, s, e_in, rhs, invD, prm);
+        case 2: return launch_v2<8, 6>(zero, N, (int)z_chunk, s, e_in, rhs, invD, prm);
+        case 3: return launch_v2<8, 8>(zero, N, (int)z_chunk, s, e_in, rhs, invD, prm);
+        case 4: return launch_v2<8, 10>(zero, N, (int)z_chunk, s, e_in, rhs, invD, prm);
+        case 5: return launch_v2<16, 7>(zero, N, (int)z_chunk, s, e_in, rhs, invD, prm);
+        default: return launch_v2<16, 6>(zero, N, (int)z_chunk, s, e_in, rhs, invD, prm);
+    }
 }
 
 // fine += trilinear prolongation of coarse (side (n+1)/2), padded layouts.

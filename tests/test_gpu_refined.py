@@ -143,7 +143,7 @@ def test_residual32_restrict32_match_oracle(L, oracle, n):
     assert np.allclose(from_padded(L, coarse, cn), c_ref, rtol=0, atol=2e-6 * np.abs(c_ref).max())
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32_refined"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32_refined", "fp32_defect"])
 def test_tolerance_solves_reach_target(oracle, precision):
     import mojo_poissonrecon_b200 as mpr
     from mojo_poissonrecon_b200 import workloads
@@ -164,16 +164,23 @@ def test_tolerance_solves_reach_target(oracle, precision):
     assert got.iso_value == pytest.approx(ref.iso_value, rel=1e-6)
 
 
-def test_refined_cycle_count_close_to_fp64():
-    """Each refined step contracts like an FP64 V-cycle: the step counts agree."""
+def test_refined_cycle_counts():
+    """Defect correction contracts like an FP64 V-cycle per step (the counts
+    agree); FCG(1) with the same FP32 V-cycle needs far fewer cycles."""
     import mojo_poissonrecon_b200 as mpr
     from mojo_poissonrecon_b200 import workloads
 
     pts, nrm = workloads.torus(100_000, seed=8)
     a = mpr.solve_screened_poisson(*_unit(pts, nrm), depth=7, confidence=True, tol=1e-8, precision="fp64")
-    b = mpr.solve_screened_poisson(*_unit(pts, nrm), depth=7, confidence=True, tol=1e-8, precision="fp32_refined")
-    assert b.relative_residual <= 1e-8 and a.relative_residual <= 1e-8
+    b = mpr.solve_screened_poisson(*_unit(pts, nrm), depth=7, confidence=True, tol=1e-8, precision="fp32_defect")
+    c = mpr.solve_screened_poisson(*_unit(pts, nrm), depth=7, confidence=True, tol=1e-8, precision="fp32_refined")
+    for sol in (a, b, c):
+        assert sol.relative_residual <= 1e-8
     assert abs(a.cycles - b.cycles) <= 2, (a.cycles, b.cycles)
+    assert c.cycles <= 0.6 * a.cycles, (a.cycles, c.cycles)
+    # Field accuracy is asserted against a tightly converged oracle solve in
+    # test_tolerance_solves_reach_target: two solves that each stop at a 1e-8
+    # residual can differ by more than that in the field (about 1.4e-6 here).
 
 
 def _unit(pts, nrm):
