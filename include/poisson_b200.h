@@ -202,21 +202,18 @@ size_t pb_fcg_workspace_size(int64_t n);
 int pb_fcg_step_f64(const float *z, const double *p_prev, double *p, double *q, double *x, double *r,
                     float *r32, const double *screen, int64_t n, double point_weight, double *scal,
                     int64_t first, void *workspace, size_t workspace_bytes, void *stream);
-/* One red-black Gauss-Seidel sweep (colour 0 then colour 1), out of place.
- * mode 0: from e_in; 1: from zero (e_in unused); 2: from e_in + trilinear
- * prolongation of `coarse` (side (n+1)/2).  n = 2^k + 1. */
-int pb_sweep_f32(const float *e_in, float *e_out, const float *rhs, const float *invD,
-                 const float *coarse, int64_t n, int64_t mode, int64_t z_chunk, void *stream);
-/* The same sweep with TMA-staged planes (n = 2^k + 1 >= 33): mode 0 from
- * e_in, mode 1 from zero.  z_chunk <= 0 picks one.  A bounded wait that gives
- * up sets *status (device int) to 1. */
+/* One red-black Gauss-Seidel sweep (colour 0 then colour 1), out of place,
+ * with TMA-staged planes (n = 2^k + 1 >= 33): mode 0 from e_in, mode 1 from
+ * zero (e_in unused).  z_chunk <= 0 picks one.  A bounded wait that gives up
+ * sets *status (device int) to 1. */
 int pb_sweep_tma_f32(const float *e_in, float *e_out, const float *rhs, const float *invD, int64_t n,
                      int64_t mode, int64_t z_chunk, int *status, void *stream);
 /* fine += trilinear prolongation of coarse (side (n+1)/2), padded layouts. */
 int pb_prolong_add_f32(const float *coarse, float *fine, int64_t fine_n, void *stream);
-int pb_residual_f32(const float *e, const float *rhs, const float *D, float *residual, int64_t n,
-                    void *stream);
-int pb_restrict_f32(const float *fine, float *coarse, int64_t fine_n, void *stream);
+/* coarse_rhs (side (n+1)/2) = full-weighting restriction of rhs - A e (side
+ * n), in FP32 on the padded layout, without writing the fine residual. */
+int pb_residual_restrict_f32(const float *e, const float *rhs, const float *D, float *coarse_rhs,
+                             int64_t n, void *stream);
 /* The V-cycle below a level of side <= 17 in one block: count levels, finest
  * first (host arrays of device pointers); rhs[0] holds the right-hand side,
  * e[0] receives the correction. */

@@ -61,11 +61,9 @@ _SIGNATURES = {
     "pb_defect_f64": ([P, P, P, P, P, I, F, P, P, P, P, S, P], C),
     "pb_fcg_workspace_size": ([I], S),
     "pb_fcg_step_f64": ([P, P, P, P, P, P, P, P, I, F, P, I, P, S, P], C),
-    "pb_sweep_f32": ([P, P, P, P, P, I, I, I, P], C),
     "pb_sweep_tma_f32": ([P, P, P, P, I, I, I, P, P], C),
     "pb_prolong_add_f32": ([P, P, I, P], C),
-    "pb_residual_f32": ([P, P, P, P, I, P], C),
-    "pb_restrict_f32": ([P, P, I, P], C),
+    "pb_residual_restrict_f32": ([P, P, P, P, I, P], C),
     "pb_coarse_cycle_f32": ([I, P, P, P, P, P, P, I, I, I, P], C),
 }
 

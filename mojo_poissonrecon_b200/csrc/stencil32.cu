@@ -123,36 +123,8 @@ __global__ void sum_partials_kernel(const double* __restrict__ partial, int coun
     if (threadIdx.x == 0) *out = t;
 }
 
-// ---- fused red-black sweep, out of place -------------------------------------
-// Colour 0 = (x+y+z) even, updated first (capi.mojo:403-405).  A block owns an
-// (x, y) tile and a z range and marches z with a three-plane ring of input
-// values (halo 2) and of updated colour-0 values (halo 1): at step t it loads
-// input plane t+1, updates colour 0 on plane t, then colour 1 on plane t-1 and
-// writes plane t-1.  Input modes: ZERO_IN (e = 0), PROLONG (e_in + trilinear
-// prolongation of the coarse correction, capi.mojo:677-742, fused into the load).
-constexpr int kTX = 64;          // tile width (the last x tile may hold kTX + 1 columns)
-constexpr int kTY = 8;           // tile height (the last y tile may hold kTY + 1 rows)
-constexpr int kSX = kTX + 1 + 4; // shared row length for the input ring (halo 2)
-constexpr int kSY = kTY + 1 + 4;
-constexpr int kRX = kTX + 1 + 2; // colour-0 ring (halo 1)
-constexpr int kRY = kTY + 1 + 2;
-constexpr int kSweepThreads = 256;
-
-struct Tile {
-    int x0, x1, y0, y1;  // interior [x0, x1) x [y0, y1)
-};
-
-__device__ __forceinline__ Tile tile_of(int n, int bx, int by) {
-    const int ntx = (n - 1) / kTX > 0 ? (n - 1) / kTX : 1;
-    const int nty = (n - 1) / kTY > 0 ? (n - 1) / kTY : 1;
-    Tile t;
-    t.x0 = bx * kTX;
-    t.x1 = bx == ntx - 1 ? n : t.x0 + kTX;
-    t.y0 = by * kTY;
-    t.y1 = by == nty - 1 ? n : t.y0 + kTY;
-    return t;
-}
-
+// Trilinear prolongation of the coarse correction at fine node (x, y, z)
+// (capi.mojo:677-742 in FP32).
 __device__ __forceinline__ float prolong_at(const float* __restrict__ c, const Geom& gc, int x, int y, int z) {
     const int x0 = x >> 1, y0 = y >> 1, z0 = z >> 1;
     const int x1 = min(x0 + 1, gc.n - 1), y1 = min(y0 + 1, gc.n - 1), z1 = min(z0 + 1, gc.n - 1);
@@ -166,141 +138,75 @@ __device__ __forceinline__ float prolong_at(const float* __restrict__ c, const G
     return c0 * (1.f - tz) + c1 * tz;
 }
 
-template <int MODE>  // 0 = plain input, 1 = zero input, 2 = input + prolongation
-__global__ void __launch_bounds__(kSweepThreads) rb_sweep_kernel(const float* __restrict__ e_in,
-                                                                 float* __restrict__ e_out,
-                                                                 const float* __restrict__ rhs,
-                                                                 const float* __restrict__ invD,
-                                                                 const float* __restrict__ coarse, Geom g, Geom gc,
-                                                                 float h2, int z_chunk) {
-    __shared__ float in_ring[3][kSY][kSX];
-    __shared__ float red_ring[3][kRY][kRX];
-    const int n = g.n;
-    const Tile T = tile_of(n, blockIdx.x, blockIdx.y);
-    const int zb = blockIdx.z * z_chunk;
-    const int ze = min(n, zb + z_chunk);
-    const int W = T.x1 - T.x0, H = T.y1 - T.y0;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = kSweepThreads / 32;
+// ---- FP32 residual fused with full-weighting restriction -----------------------
+// coarse_rhs = restrict(rhs - A e) (capi.mojo:413-470 then :557-673, in FP32)
+// without writing the fine residual.  A block owns a 32 x 4 tile of coarse
+// (x, y) and marches coarse z; fine residual planes of the tile plus a halo of
+// one (65 x 9 nodes) are computed into a three-plane ring in shared memory,
+// plane 2zc+1 being reused as plane 2(zc+1)-1 of the next coarse plane.  The
+// restriction weights (1,2,1)^3 over in-grid fine nodes, normalised by their
+// sum, as in the reference.
+constexpr int kRrCX = 32, kRrCY = 4, kRrCZ = 8;
+constexpr int kRrFX = 2 * kRrCX + 1, kRrFY = 2 * kRrCY + 1;  // 65 x 9 fine nodes
+constexpr int kRrThreads = 256;
 
-    auto load_plane = [&](int z) {
-        float(*dst)[kSX] = in_ring[(z + 3) % 3];
-        for (int ly = warp; ly < H + 4; ly += warps) {
-            const int y = T.y0 - 2 + ly;
-            for (int lx = lane; lx < W + 4; lx += 32) {
-                const int x = T.x0 - 2 + lx;
-                float v = 0.0f;
-                if (MODE != 1 && z >= 0 && z < n && x >= 0 && x < n && y >= 0 && y < n) {
-                    v = e_in[g.at(x, y, z)];
-                    if (MODE == 2) v += prolong_at(coarse, gc, x, y, z);
-                }
-                dst[ly][lx] = v;
+__global__ void __launch_bounds__(kRrThreads) residual_restrict32_kernel(const float* __restrict__ e,
+                                                                          const float* __restrict__ rhs,
+                                                                          const float* __restrict__ D, Geom gf,
+                                                                          float h2, float* __restrict__ coarse,
+                                                                          Geom gc) {
+    __shared__ float ring[3][kRrFY][kRrFX + 3];
+    const int fn = gf.n, cn = gc.n;
+    const int xc0 = blockIdx.x * kRrCX, yc0 = blockIdx.y * kRrCY;
+    const int zc0 = blockIdx.z * kRrCZ, zc1 = min(cn, zc0 + kRrCZ);
+    const int fx0 = 2 * xc0 - 1, fy0 = 2 * yc0 - 1;
+    const int tid = threadIdx.x;
+    auto fine_plane = [&](int f) {  // residual of fine plane f over the tile region
+        float(*dst)[kRrFX + 3] = ring[(f + 3) % 3];
+        for (int i = tid; i < kRrFY * kRrFX; i += kRrThreads) {
+            const int ly = i / kRrFX, lx = i - ly * kRrFX;
+            const int x = fx0 + lx, y = fy0 + ly;
+            float r = 0.0f;
+            if (f >= 0 && f < fn && x >= 0 && x < fn && y >= 0 && y < fn) {
+                const int64_t p = gf.at(x, y, f);
+                const float sum = e[p - 1] + e[p + 1] + e[p - gf.P] + e[p + gf.P] + e[p - gf.plane] + e[p + gf.plane];
+                r = rhs[p] - (D[p] * e[p] - sum * h2);
             }
+            dst[ly][lx] = r;
         }
     };
-    // colour-0 nodes of plane z on the halo-1 region
-    auto red_plane = [&](int z) {
-        float(*dst)[kRX] = red_ring[(z + 3) % 3];
-        const float(*cm)[kSX] = in_ring[(z + 2) % 3];
-        const float(*cc)[kSX] = in_ring[(z + 3) % 3];
-        const float(*cp)[kSX] = in_ring[(z + 4) % 3];
-        for (int ly = warp; ly < H + 2; ly += warps) {
-            const int y = T.y0 - 1 + ly;
-            for (int lx = lane; lx < W + 2; lx += 32) {
-                const int x = T.x0 - 1 + lx;
-                float v = 0.0f;
-                if (z >= 0 && z < n && x >= 0 && x < n && y >= 0 && y < n && ((x + y + z) & 1) == 0) {
-                    const int sy = ly + 1, sx = lx + 1;
-                    const float s = cc[sy][sx - 1] + cc[sy][sx + 1] + cc[sy - 1][sx] + cc[sy + 1][sx] + cm[sy][sx] +
-                                    cp[sy][sx];
-                    const int64_t p = g.at(x, y, z);
-                    v = (rhs[p] + s * h2) * invD[p];
-                }
-                dst[ly][lx] = v;
-            }
-        }
-    };
-    // colour-1 nodes of plane z on the interior, and the output plane
-    auto black_plane = [&](int z) {
-        const float(*rm)[kRX] = red_ring[(z + 2) % 3];
-        const float(*rc)[kRX] = red_ring[(z + 3) % 3];
-        const float(*rp)[kRX] = red_ring[(z + 4) % 3];
-        for (int ly = warp; ly < H; ly += warps) {
-            const int y = T.y0 + ly;
-            for (int lx = lane; lx < W; lx += 32) {
-                const int x = T.x0 + lx;
-                const int sy = ly + 1, sx = lx + 1;
-                const int64_t p = g.at(x, y, z);
-                float v;
-                if (((x + y + z) & 1) == 0) {
-                    v = rc[sy][sx];
-                } else {
-                    const float s = rc[sy][sx - 1] + rc[sy][sx + 1] + rc[sy - 1][sx] + rc[sy + 1][sx] + rm[sy][sx] +
-                                    rp[sy][sx];
-                    v = (rhs[p] + s * h2) * invD[p];
-                }
-                e_out[p] = v;
-            }
-        }
-    };
-
-    // Ring discipline: load(t+1) overwrites plane t-2, last read by red(t-1);
-    // red(t) overwrites colour-0 plane t-3, last read by black(t-2).  The two
-    // barriers per step separate exactly those pairs.
-    load_plane(zb - 2);
-    load_plane(zb - 1);
-    load_plane(zb);
-    __syncthreads();
-    red_plane(zb - 1);  // zero outside the grid
-    __syncthreads();
-    for (int t = zb; t <= ze; ++t) {
-        load_plane(t + 1);
+    fine_plane(2 * zc0 - 1);
+    for (int zc = zc0; zc < zc1; ++zc) {
+        fine_plane(2 * zc);
+        fine_plane(2 * zc + 1);
         __syncthreads();
-        red_plane(t);
-        __syncthreads();
-        if (t - 1 >= zb) black_plane(t - 1);
-    }
-}
-
-// ---- FP32 residual (padded) and full-weighting restriction -------------------
-__global__ void residual32_kernel(const float* __restrict__ e, const float* __restrict__ rhs,
-                                  const float* __restrict__ D, Geom g, float h2, float* __restrict__ res) {
-    const int n = g.n;
-    const int64_t total = (int64_t)n * n * n;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % n), y = (int)((i / n) % n), z = (int)(i / ((int64_t)n * n));
-        const int64_t p = g.at(x, y, z);
-        const float s = e[p - 1] + e[p + 1] + e[p - g.P] + e[p + g.P] + e[p - g.plane] + e[p + g.plane];
-        res[p] = rhs[p] - (D[p] * e[p] - s * h2);
-    }
-}
-
-// capi.mojo:557-673 in FP32 on the padded layout: weights (1,2,1)^3 over the
-// in-grid fine nodes, normalised by their sum.
-__global__ void restrict32_kernel(const float* __restrict__ fine, Geom gf, float* __restrict__ coarse, Geom gc) {
-    const int cn = gc.n, fn = gf.n;
-    const int64_t total = (int64_t)cn * cn * cn;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % cn), y = (int)((i / cn) % cn), z = (int)(i / ((int64_t)cn * cn));
-        float sum = 0.0f, wsum = 0.0f;
-        for (int oz = -1; oz <= 1; ++oz) {
-            const int zz = 2 * z + oz;
-            if (zz < 0 || zz >= fn) continue;
-            const float wz = oz == 0 ? 2.f : 1.f;
-            for (int oy = -1; oy <= 1; ++oy) {
-                const int yy = 2 * y + oy;
-                if (yy < 0 || yy >= fn) continue;
-                const float wy = oy == 0 ? 2.f : 1.f;
-                const float* row = fine + gf.at(0, yy, zz);
-                for (int ox = -1; ox <= 1; ++ox) {
-                    const int xx = 2 * x + ox;
-                    if (xx < 0 || xx >= fn) continue;
-                    const float w = (ox == 0 ? 2.f : 1.f) * wy * wz;
-                    sum += row[xx] * w;
-                    wsum += w;
+        if (tid < kRrCX * kRrCY) {
+            const int cy = tid / kRrCX, cx = tid - cy * kRrCX;
+            const int xc = xc0 + cx, yc = yc0 + cy;
+            if (xc < cn && yc < cn) {
+                float sum = 0.0f, wsum = 0.0f;
+                for (int oz = -1; oz <= 1; ++oz) {
+                    const int zz = 2 * zc + oz;
+                    if (zz < 0 || zz >= fn) continue;
+                    const float wz = oz == 0 ? 2.f : 1.f;
+                    for (int oy = -1; oy <= 1; ++oy) {
+                        const int yy = 2 * yc + oy;
+                        if (yy < 0 || yy >= fn) continue;
+                        const float wy = oy == 0 ? 2.f : 1.f;
+                        const float* row = ring[(zz + 3) % 3][2 * cy + 1 + oy];
+                        for (int ox = -1; ox <= 1; ++ox) {
+                            const int xx = 2 * xc + ox;
+                            if (xx < 0 || xx >= fn) continue;
+                            const float w = (ox == 0 ? 2.f : 1.f) * wy * wz;
+                            sum += row[2 * cx + 1 + ox] * w;
+                            wsum += w;
+                        }
+                    }
                 }
+                coarse[gc.at(xc, yc, zc)] = sum / wsum;
             }
         }
-        coarse[gc.at(x, y, z)] = sum / wsum;
+        __syncthreads();  // the ring slots of planes 2zc-1 and 2zc are rewritten next
     }
 }
 
@@ -465,55 +371,16 @@ extern "C" int pb_defect_f64(const double* x_old, const float* e, double* x_new,
     return PB_OK;
 }
 
-static dim3 sweep_grid(int n, int z_chunk) {
-    const int ntx = (n - 1) / kTX > 0 ? (n - 1) / kTX : 1;
-    const int nty = (n - 1) / kTY > 0 ? (n - 1) / kTY : 1;
-    return dim3(ntx, nty, (n + z_chunk - 1) / z_chunk);
-}
-
-// One fused red-black sweep e_out <- sweep(e_in).  mode 0: e_in as is; 1: e_in
-// taken as zero (e_in may be NULL); 2: e_in + prolongation of `coarse` (side
-// (n+1)/2).  The grid side must satisfy n = 2^k + 1 or n <= kTX + 1.
-extern "C" int pb_sweep_f32(const float* e_in, float* e_out, const float* rhs, const float* invD, const float* coarse,
-                            int64_t n, int64_t mode, int64_t z_chunk, void* stream) {
-    if (n < 2 || n > 4097 || !e_out || !rhs || !invD || (mode != 1 && !e_in) || (mode == 2 && !coarse) || mode < 0 ||
-        mode > 2)
-        return fail(PB_ERR_INVALID, "sweep: bad args");
-    if (e_in == e_out) return fail(PB_ERR_INVALID, "sweep: out of place only");
-    const int ntx = (int)((n - 1) / kTX > 0 ? (n - 1) / kTX : 1);
-    const int nty = (int)((n - 1) / kTY > 0 ? (n - 1) / kTY : 1);
-    if (n - (int64_t)(ntx - 1) * kTX > kTX + 1 || n - (int64_t)(nty - 1) * kTY > kTY + 1)
-        return fail(PB_ERR_INVALID, "sweep: n = %lld does not tile (needs n = 2^k + 1)", (long long)n);
-    if (z_chunk < 1) z_chunk = 32;
-    const Geom g = geom((int)n);
-    const Geom gc = geom((int)((n + 1) / 2));
+// coarse_rhs (side (n+1)/2) = full-weighting restriction of rhs - A e on side n.
+extern "C" int pb_residual_restrict_f32(const float* e, const float* rhs, const float* D, float* coarse_rhs,
+                                        int64_t n, void* stream) {
+    if (n < 3 || n > 4097 || !e || !rhs || !D || !coarse_rhs) return fail(PB_ERR_INVALID, "residual_restrict: bad args");
+    const int cn = (int)((n + 1) / 2);
     const float h2 = (float)((n - 1) * (n - 1));
-    const dim3 grid = sweep_grid((int)n, (int)z_chunk);
-    cudaStream_t s = (cudaStream_t)stream;
-    if (mode == 0)
-        rb_sweep_kernel<0><<<grid, kSweepThreads, 0, s>>>(e_in, e_out, rhs, invD, nullptr, g, gc, h2, (int)z_chunk);
-    else if (mode == 1)
-        rb_sweep_kernel<1><<<grid, kSweepThreads, 0, s>>>(nullptr, e_out, rhs, invD, nullptr, g, gc, h2, (int)z_chunk);
-    else
-        rb_sweep_kernel<2><<<grid, kSweepThreads, 0, s>>>(e_in, e_out, rhs, invD, coarse, g, gc, h2, (int)z_chunk);
-    PB_CHECK_LAUNCH("rb_sweep_kernel");
-    return PB_OK;
-}
-
-extern "C" int pb_residual_f32(const float* e, const float* rhs, const float* D, float* res, int64_t n, void* stream) {
-    if (n < 2 || n > 4097 || !e || !rhs || !D || !res) return fail(PB_ERR_INVALID, "residual32: bad args");
-    const float h2 = (float)((n - 1) * (n - 1));
-    residual32_kernel<<<stride_grid(n * n * n, 256), 256, 0, (cudaStream_t)stream>>>(e, rhs, D, geom((int)n), h2, res);
-    PB_CHECK_LAUNCH("residual32_kernel");
-    return PB_OK;
-}
-
-extern "C" int pb_restrict_f32(const float* fine, float* coarse, int64_t fine_n, void* stream) {
-    if (fine_n < 3 || fine_n > 4097 || !fine || !coarse) return fail(PB_ERR_INVALID, "restrict32: bad args");
-    const int cn = (int)((fine_n + 1) / 2);
-    restrict32_kernel<<<stride_grid((int64_t)cn * cn * cn, 256), 256, 0, (cudaStream_t)stream>>>(
-        fine, geom((int)fine_n), coarse, geom(cn));
-    PB_CHECK_LAUNCH("restrict32_kernel");
+    const dim3 grid((cn + kRrCX - 1) / kRrCX, (cn + kRrCY - 1) / kRrCY, (cn + kRrCZ - 1) / kRrCZ);
+    residual_restrict32_kernel<<<grid, kRrThreads, 0, (cudaStream_t)stream>>>(e, rhs, D, geom((int)n), h2,
+                                                                              coarse_rhs, geom(cn));
+    PB_CHECK_LAUNCH("residual_restrict32_kernel");
     return PB_OK;
 }
 

@@ -2,13 +2,15 @@
 //
 // Same update as capi.mojo:310-410 for one iteration (colour 0 then colour 1)
 // in FP32, out of place.  A block owns an (x, y) tile of up to 65 x 17 nodes
-// and a z range.  One thread issues cp.async.bulk.tensor loads of whole plane
-// boxes (72 x 21 floats: the tile plus a halo of 2, x origin aligned to 16
-// bytes) of e_in, rhs and 1/D into a ring of kSlots slots, each guarded by an
-// mbarrier, kSlots-1 planes ahead of the plane being updated; all threads then
-// compute out of shared memory.  Out-of-grid nodes read as zero (ghost layer
-// or TMA zero fill) and 1/D is zero there, so colour-0 values at halo nodes
-// outside the grid come out zero without branches.
+// and a z range, and marches z.  One thread issues cp.async.bulk.tensor loads
+// of whole plane boxes (72 x 21 floats: the tile plus a halo of 2, x origin
+// aligned to 16 bytes) of e_in, rhs and 1/D into a ring of kSlots slots, each
+// guarded by an mbarrier, three planes ahead of the plane being updated.
+// Each thread owns one float4 column group of the box for the whole march and
+// keeps its planes in registers (see sweep_kernel); shared memory serves only
+// the in-plane neighbours.  Out-of-grid nodes read as zero (ghost layer or TMA
+// zero fill) and 1/D is zero there, so colour-0 values at halo nodes outside
+// the grid come out zero without branches.
 //
 // Waits are bounded: a barrier that does not complete within ~1 s of SM clock
 // sets *status = 1 and the block stops issuing work, after draining its own
@@ -25,19 +27,8 @@ constexpr int kTX = 64;                 // interior tile width (last x tile: 65)
 constexpr int kTY = 16;                 // interior tile height (last y tile: 17)
 constexpr int kBoxX = 72;               // kTX + 1 + halo 2 + 2, rounded to 16 B; x origin = x0 - 4
 constexpr int kBoxY = kTY + 1 + 4;      // 21
-constexpr int kRedX = 68;               // colour-0 ring row stride (>= kTX + 1 + 2)
-constexpr int kRedY = kTY + 1 + 2;      // 19
-constexpr int kSlots = 5;
-constexpr int kThreads = 256;
-constexpr int kBoxFloats = kBoxX * kBoxY;  // 1512 floats = 6048 bytes land per box
-constexpr int kPlane = 1536;               // slot stride: 6144 bytes keeps every box 128-byte aligned
+constexpr int kSlots = 5;               // planes t-1 .. t+3
 constexpr long long kWaitCycles = 2000000000ll;
-
-struct Smem {
-    float slot[kSlots][3][kPlane];      // [slot][e, rhs, invD][row * kBoxX + col]
-    float red[3][kRedY][kRedX];
-    unsigned long long bar[kSlots];
-};
 
 __device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -84,148 +75,9 @@ struct Params {
     int* status;
 };
 
-template <bool ZERO_IN>
-__global__ void __launch_bounds__(kThreads, 2)
-    sweep_kernel(const __grid_constant__ CUtensorMap map_e, const __grid_constant__ CUtensorMap map_rhs,
-                 const __grid_constant__ CUtensorMap map_invD, Params p) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    // TMA destinations must be 128-byte aligned: align the carve-out base.
-    const uint32_t raw = saddr(smem_raw);
-    Smem& S = *reinterpret_cast<Smem*>(smem_raw + (((raw + 127u) & ~127u) - raw));
-    const int n = p.n;
-    const int bx = blockIdx.x, by = blockIdx.y;
-    const int x0 = bx * kTX, y0 = by * kTY;
-    const int W = (bx == p.ntx - 1 ? n : x0 + kTX) - x0;
-    const int H = (by == p.nty - 1 ? n : y0 + kTY) - y0;
-    const int zb = blockIdx.z * p.z_chunk;
-    const int ze = min(n, zb + p.z_chunk);
-    const int zfirst = zb - 2, zlast = ze + 1;  // planes read by this block
-    const int tid = threadIdx.x;
-    const uint32_t bytes = (ZERO_IN ? 2u : 3u) * kBoxFloats * 4u;
+constexpr int kGroups = kBoxX / 4;  // 18 float4 column groups per box row
 
-    if (tid == 0) {
-        for (int s = 0; s < kSlots; ++s) bar_init(&S.bar[s]);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-
-    auto issue = [&](int z) {  // thread 0 only
-        const int k = z - zfirst, s = k % kSlots;
-        bar_expect(&S.bar[s], bytes);
-        // box origin in storage coordinates: x = x0 - 4 + 4, y = (y0 - 2) + 1, z = z + 1
-        if (!ZERO_IN) load_box(S.slot[s][0], &map_e, x0, y0 - 1, z + 1, &S.bar[s]);
-        load_box(S.slot[s][1], &map_rhs, x0, y0 - 1, z + 1, &S.bar[s]);
-        load_box(S.slot[s][2], &map_invD, x0, y0 - 1, z + 1, &S.bar[s]);
-    };
-    auto slot_of = [&](int z) { return (z - zfirst) % kSlots; };
-    auto parity_of = [&](int z) { return (uint32_t)(((z - zfirst) / kSlots) & 1); };
-
-    int issued = zfirst;  // next plane to issue
-    if (tid == 0)
-        for (; issued <= zlast && issued < zfirst + kSlots; ++issued) issue(issued);
-
-    // Planes zfirst and zfirst + 1 must be resident before the first colour-0
-    // step.  Every give-up decision is made block-wide (__syncthreads_and) so
-    // that no thread leaves the loop while others wait at a barrier.
-    bool ok = bar_wait(&S.bar[slot_of(zfirst)], parity_of(zfirst));
-    ok = bar_wait(&S.bar[slot_of(zfirst + 1)], parity_of(zfirst + 1)) && ok;
-    ok = __syncthreads_and(ok);
-
-    for (int t = zb - 1; t <= ze && ok; ++t) {
-        const bool arrived = bar_wait(&S.bar[slot_of(t + 1)], parity_of(t + 1));
-        // colour 0 on plane t over the tile plus a halo of 1 (all reads stay
-        // inside the ring, so a late plane only gives unused values)
-        {
-            const float* em = S.slot[slot_of(t - 1)][0];
-            const float* ec = S.slot[slot_of(t)][0];
-            const float* ep = S.slot[slot_of(t + 1)][0];
-            const float* rhs = S.slot[slot_of(t)][1];
-            const float* inv = S.slot[slot_of(t)][2];
-            float(*red)[kRedX] = S.red[(t + 3) % 3];
-            const int rows = H + 2, pairs = (W + 3) / 2;
-            for (int i = tid; i < rows * 34; i += kThreads) {
-                const int ly = i / 34, k = i - ly * 34;
-                if (k >= pairs) continue;
-                const int y = y0 - 1 + ly;
-                const int lx = 2 * k + ((1 + y + t) & 1);  // x = x0 - 1 + lx has x + y + t even
-                if (lx >= W + 2) continue;
-                const int c = (ly + 1) * kBoxX + lx + 3;
-                float v = 0.0f;
-                if (!ZERO_IN) {
-                    const float s = ec[c - 1] + ec[c + 1] + ec[c - kBoxX] + ec[c + kBoxX] + em[c] + ep[c];
-                    v = (rhs[c] + s * p.h2) * inv[c];
-                } else {
-                    v = rhs[c] * inv[c];
-                }
-                red[ly][lx] = v;
-            }
-        }
-        ok = __syncthreads_and(arrived);
-        if (!ok) break;
-        // colour 1 on plane t - 1 over the tile, and its output rows
-        if (t - 1 >= zb) {
-            const int z = t - 1;
-            const float* rhs = S.slot[slot_of(z)][1];
-            const float* inv = S.slot[slot_of(z)][2];
-            const float(*rm)[kRedX] = S.red[(z + 2) % 3];
-            const float(*rc)[kRedX] = S.red[(z + 3) % 3];
-            const float(*rp)[kRedX] = S.red[(z + 4) % 3];
-            const int pairs = (W + 1) / 2;
-            for (int i = tid; i < H * 33; i += kThreads) {
-                const int ly = i / 33, k = i - ly * 33;
-                if (k >= pairs) continue;
-                const int y = y0 + ly;
-                const int lx = 2 * k;
-                float out[2];
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    const int x = x0 + lx + j;
-                    const int ry = ly + 1, rx = lx + j + 1;
-                    if (((x + y + z) & 1) == 0) {
-                        out[j] = rc[ry][rx];
-                    } else {
-                        const float s = rc[ry][rx - 1] + rc[ry][rx + 1] + rc[ry - 1][rx] + rc[ry + 1][rx] +
-                                        rm[ry][rx] + rp[ry][rx];
-                        const int c = (ly + 2) * kBoxX + lx + j + 4;
-                        out[j] = (rhs[c] + s * p.h2) * inv[c];
-                    }
-                }
-                float* dst = p.e_out + ((int64_t)(z + 1) * (n + 2) + (y + 1)) * p.P + (x0 + lx + 4);
-                if (lx + 1 < W) {
-                    *reinterpret_cast<float2*>(dst) = make_float2(out[0], out[1]);
-                } else {
-                    dst[0] = out[0];
-                }
-            }
-        }
-        __syncthreads();  // slot of plane t - 1 and colour-0 plane t - 2 are free now
-        if (tid == 0 && issued <= zlast) issue(issued++);
-    }
-    if (!ok) {
-        if (tid == 0) {
-            atomicExch(p.status, 1);
-            // drain: the copies still in flight (at most the last kSlots issued)
-            // must land before the block exits; each wait is bounded too
-            for (int z = max(zfirst, issued - kSlots); z < issued; ++z)
-                (void)bar_wait(&S.bar[slot_of(z)], parity_of(z));
-        }
-        __syncthreads();
-    }
-}
-
-// ---- version 2: in-place colour-0 updates on float4 column groups -------------
-// The state ring holds e for planes t-2 .. t+3.  Colour 0 of plane t is
-// updated in place (float4 groups of 4 columns, 18 groups per 72-column box
-// row); colour 1 of plane t-1 is computed into registers and written out with
-// the colour-0 values of the same group as one float4 store.  A colour-0
-// update reads only colour-1 nodes and vice versa, so in-place stores never
-// change a value another thread of the same phase reads.  For a group at box
-// row br on plane t (colour 0) or t-1 (colour 1), the updated columns are
-// j = s and s + 2 with s = (br + t) & 1, because x0 and y0 are even.
-constexpr int kGroups = kBoxX / 4;  // 18
-
-// Geometry of one v2 configuration: tile height TY (the last y tile holds
-// TY + 1 rows), SLOTS planes in the ring (SLOTS - 4 planes of prefetch).
+// Shared-memory ring of SLOTS planes: box of e, rhs and 1/D per plane.
 template <int TY, int SLOTS>
 struct Geo2 {
     static constexpr int kBoxRows = TY + 1 + 4;
@@ -239,12 +91,25 @@ struct Geo2 {
 
 __device__ __forceinline__ float4 lds4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 
-template <bool ZERO_IN, int TY, int SLOTS>
+// Each thread owns one float4 column group (box row br, group g: box columns
+// 4g .. 4g+3) for the whole z range and keeps in registers the input of planes
+// t-1, t and t+1, the colour-0-updated values of planes t-2 and t-1, and rhs
+// and 1/D of planes t-1 and t.  At step t it updates colour 0 of plane t in
+// place (float4 store back into the slot, read by the neighbours' colour-1
+// updates), then colour 1 of plane t-1, written out together with that
+// plane's colour-0 values as one float4.  A colour-0 update reads only
+// colour-1 nodes and vice versa, so concurrent in-place stores never change a
+// value another thread of the same phase uses.  Because x0 and y0 are even,
+// the updated columns of a group on box row br are j = s and s + 2 with
+// s = (br + t) & 1 in both phases.
+constexpr int kThreads = 352;  // 19 box rows x 18 groups = 342 work items, one per thread
+
+template <bool ZERO_IN, int SLOTS>
 __global__ void __launch_bounds__(kThreads, 2)
-    sweep_v2_kernel(const __grid_constant__ CUtensorMap map_e, const __grid_constant__ CUtensorMap map_rhs,
+    sweep_kernel(const __grid_constant__ CUtensorMap map_e, const __grid_constant__ CUtensorMap map_rhs,
                     const __grid_constant__ CUtensorMap map_invD, Params p) {
+    constexpr int TY = kTY;
     using G = Geo2<TY, SLOTS>;
-    constexpr int kSlots2 = SLOTS;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const uint32_t raw = saddr(smem_raw);
     typename G::Smem& S = *reinterpret_cast<typename G::Smem*>(smem_raw + (((raw + 127u) & ~127u) - raw));
@@ -261,13 +126,12 @@ __global__ void __launch_bounds__(kThreads, 2)
     const float h2 = p.h2;
 
     if (tid == 0) {
-        for (int s = 0; s < kSlots2; ++s) bar_init(&S.bar[s]);
+        for (int s = 0; s < SLOTS; ++s) bar_init(&S.bar[s]);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-
-    auto slot_of = [&](int z) { return (z - zfirst) % kSlots2; };
-    auto parity_of = [&](int z) { return (uint32_t)(((z - zfirst) / kSlots2) & 1); };
+    auto slot_of = [&](int z) { return (z - zfirst) % SLOTS; };
+    auto parity_of = [&](int z) { return (uint32_t)(((z - zfirst) / SLOTS) & 1); };
     auto issue = [&](int z) {
         const int s = slot_of(z);
         bar_expect(&S.bar[s], bytes);
@@ -277,98 +141,100 @@ __global__ void __launch_bounds__(kThreads, 2)
     };
     int issued = zfirst;
     if (tid == 0)
-        for (; issued <= zlast && issued < zfirst + kSlots2; ++issued) issue(issued);
+        for (; issued <= zlast && issued < zfirst + SLOTS; ++issued) issue(issued);
+
+    // this thread's work item
+    const int br = 1 + tid / kGroups, g = tid - (br - 1) * kGroups;
+    const bool has_a = br <= H + 2;                                       // colour-0 region rows 1 .. H+2
+    const bool has_b = br >= 2 && br <= H + 1 && g >= 1 && g <= (W + 3) / 4;  // output rows and groups
+    const int base = br * kBoxX + 4 * g;
+    const int b0 = 4 * g;
+    bool upd_ok[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) upd_ok[j] = (b0 + j >= 3) && (b0 + j < W + 5);
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
 
     bool ok = bar_wait(&S.bar[slot_of(zfirst)], parity_of(zfirst));
     ok = bar_wait(&S.bar[slot_of(zfirst + 1)], parity_of(zfirst + 1)) && ok;
     ok = __syncthreads_and(ok);
 
-    const int itemsA = (H + 2) * kGroups;
-    const int groupsB = (W + 3) / 4;  // groups 1 .. groupsB cover box columns 4 .. W+3
-    const int itemsB = H * groupsB;
+    // registers: e at t-1 (input), e at t (input); updated colour-0 planes t-2, t-1
+    float4 e_prev = zero4, e_cur = zero4;
+    if (!ZERO_IN && has_a && ok) {
+        e_prev = lds4(S.slot[slot_of(zb - 2)][0] + base);
+        e_cur = lds4(S.slot[slot_of(zb - 1)][0] + base);
+    }
+    float4 r_prev = zero4, i_prev = zero4, red_prev2 = zero4, red_prev = zero4;
+
     for (int t = zb - 1; t <= ze && ok; ++t) {
         const bool arrived = bar_wait(&S.bar[slot_of(t + 1)], parity_of(t + 1));
-        {  // colour 0 of plane t on box rows 1 .. H+2, columns 3 .. W+4
-            float* e = S.slot[slot_of(t)][0];
-            const float* em = S.slot[slot_of(t - 1)][0];
-            const float* ep = S.slot[slot_of(t + 1)][0];
-            const float* rhs = S.slot[slot_of(t)][1];
-            const float* inv = S.slot[slot_of(t)][2];
-            for (int i = tid; i < itemsA; i += kThreads) {
-                const int br = 1 + i / kGroups, g = i - (br - 1) * kGroups;
-                const int base = br * kBoxX + 4 * g;
-                const int s = (br + t) & 1;
-                const float4 r4 = lds4(rhs + base), i4 = lds4(inv + base);
-                float4 c = lds4(e + base);
-                float v[4];
-                if (ZERO_IN) {
-                    v[0] = r4.x * i4.x; v[1] = r4.y * i4.y; v[2] = r4.z * i4.z; v[3] = r4.w * i4.w;
-                } else {
-                    const float4 u = lds4(e + base - kBoxX), d = lds4(e + base + kBoxX);
-                    const float4 zm = lds4(em + base), zp = lds4(ep + base);
-                    const float L = g > 0 ? e[base - 1] : 0.0f;
-                    const float R = g < kGroups - 1 ? e[base + 4] : 0.0f;
-                    v[0] = (r4.x + (L + c.y + u.x + d.x + zm.x + zp.x) * h2) * i4.x;
-                    v[1] = (r4.y + (c.x + c.z + u.y + d.y + zm.y + zp.y) * h2) * i4.y;
-                    v[2] = (r4.z + (c.y + c.w + u.z + d.z + zm.z + zp.z) * h2) * i4.z;
-                    v[3] = (r4.w + (c.z + R + u.w + d.w + zm.w + zp.w) * h2) * i4.w;
-                }
-                const int b0 = 4 * g;
-                float cc[4] = {c.x, c.y, c.z, c.w};
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const bool upd = ((j & 1) == s) && (b0 + j >= 3) && (b0 + j < W + 5);
-                    cc[j] = upd ? v[j] : cc[j];
-                }
-                *reinterpret_cast<float4*>(e + base) = make_float4(cc[0], cc[1], cc[2], cc[3]);
+        float4 red_cur = zero4, r_cur = zero4, i_cur = zero4, e_next = zero4;
+        if (has_a) {  // colour 0 of plane t
+            const float* e = S.slot[slot_of(t)][0];
+            r_cur = lds4(S.slot[slot_of(t)][1] + base);
+            i_cur = lds4(S.slot[slot_of(t)][2] + base);
+            const int s = (br + t) & 1;
+            float v[4];
+            if (ZERO_IN) {
+                v[0] = r_cur.x * i_cur.x; v[1] = r_cur.y * i_cur.y; v[2] = r_cur.z * i_cur.z; v[3] = r_cur.w * i_cur.w;
+            } else {
+                e_next = lds4(S.slot[slot_of(t + 1)][0] + base);
+                const float4 u = lds4(e + base - kBoxX), d = lds4(e + base + kBoxX);
+                const float L = g > 0 ? e[base - 1] : 0.0f;
+                const float R = g < kGroups - 1 ? e[base + 4] : 0.0f;
+                const float4 c = e_cur, zm = e_prev, zp = e_next;
+                v[0] = (r_cur.x + (L + c.y + u.x + d.x + zm.x + zp.x) * h2) * i_cur.x;
+                v[1] = (r_cur.y + (c.x + c.z + u.y + d.y + zm.y + zp.y) * h2) * i_cur.y;
+                v[2] = (r_cur.z + (c.y + c.w + u.z + d.z + zm.z + zp.z) * h2) * i_cur.z;
+                v[3] = (r_cur.w + (c.z + R + u.w + d.w + zm.w + zp.w) * h2) * i_cur.w;
             }
+            float cc[4] = {e_cur.x, e_cur.y, e_cur.z, e_cur.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) cc[j] = ((j & 1) == s && upd_ok[j]) ? v[j] : cc[j];
+            red_cur = make_float4(cc[0], cc[1], cc[2], cc[3]);
+            *reinterpret_cast<float4*>(S.slot[slot_of(t)][0] + base) = red_cur;
         }
         ok = __syncthreads_and(arrived);
         if (!ok) break;
-        if (t - 1 >= zb) {  // colour 1 of plane t-1 on the tile, written with colour 0
+        if (has_b && t - 1 >= zb) {  // colour 1 of plane t-1, written out with its colour 0
             const int z = t - 1;
             const float* e = S.slot[slot_of(z)][0];
-            const float* em = S.slot[slot_of(z - 1)][0];
-            const float* ep = S.slot[slot_of(z + 1)][0];
-            const float* rhs = S.slot[slot_of(z)][1];
-            const float* inv = S.slot[slot_of(z)][2];
-            for (int i = tid; i < itemsB; i += kThreads) {
-                const int r = i / groupsB;
-                const int g = 1 + (i - r * groupsB);
-                const int br = r + 2;
-                const int base = br * kBoxX + 4 * g;
-                const int s = (br + t) & 1;
-                const float4 c = lds4(e + base), u = lds4(e + base - kBoxX), d = lds4(e + base + kBoxX);
-                const float4 zm = lds4(em + base), zp = lds4(ep + base);
-                const float4 r4 = lds4(rhs + base), i4 = lds4(inv + base);
-                const float L = e[base - 1];
-                const float R = g < kGroups - 1 ? e[base + 4] : 0.0f;
-                float v[4];
-                v[0] = (r4.x + (L + c.y + u.x + d.x + zm.x + zp.x) * h2) * i4.x;
-                v[1] = (r4.y + (c.x + c.z + u.y + d.y + zm.y + zp.y) * h2) * i4.y;
-                v[2] = (r4.z + (c.y + c.w + u.z + d.z + zm.z + zp.z) * h2) * i4.z;
-                v[3] = (r4.w + (c.z + R + u.w + d.w + zm.w + zp.w) * h2) * i4.w;
-                float o[4] = {c.x, c.y, c.z, c.w};
+            const float4 u = lds4(e + base - kBoxX), d = lds4(e + base + kBoxX);
+            const float L = e[base - 1];
+            const float R = g < kGroups - 1 ? e[base + 4] : 0.0f;
+            const float4 c = red_prev, zm = red_prev2, zp = red_cur;
+            const int s = (br + t) & 1;
+            float v[4];
+            v[0] = (r_prev.x + (L + c.y + u.x + d.x + zm.x + zp.x) * h2) * i_prev.x;
+            v[1] = (r_prev.y + (c.x + c.z + u.y + d.y + zm.y + zp.y) * h2) * i_prev.y;
+            v[2] = (r_prev.z + (c.y + c.w + u.z + d.z + zm.z + zp.z) * h2) * i_prev.z;
+            v[3] = (r_prev.w + (c.z + R + u.w + d.w + zm.w + zp.w) * h2) * i_prev.w;
+            float o[4] = {c.x, c.y, c.z, c.w};
 #pragma unroll
-                for (int j = 0; j < 4; ++j) o[j] = ((j & 1) == s) ? v[j] : o[j];
-                float* dst = p.e_out + ((int64_t)(z + 1) * (n + 2) + (y0 - 1 + br)) * p.P + (x0 + 4 * g);
-                const int valid = W + 4 - 4 * g;  // columns of this group inside the tile
-                if (valid >= 4) {
-                    *reinterpret_cast<float4*>(dst) = make_float4(o[0], o[1], o[2], o[3]);
-                } else {
+            for (int j = 0; j < 4; ++j) o[j] = ((j & 1) == s) ? v[j] : o[j];
+            float* dst = p.e_out + ((int64_t)(z + 1) * (n + 2) + (y0 - 1 + br)) * p.P + (x0 + 4 * g);
+            const int valid = W + 4 - 4 * g;
+            if (valid >= 4) {
+                *reinterpret_cast<float4*>(dst) = make_float4(o[0], o[1], o[2], o[3]);
+            } else {
 #pragma unroll
-                    for (int j = 0; j < 3; ++j)
-                        if (j < valid) dst[j] = o[j];
-                }
+                for (int j = 0; j < 3; ++j)
+                    if (j < valid) dst[j] = o[j];
             }
         }
-        __syncthreads();  // plane t-2 is no longer read
-        if (tid == 0 && t - 2 >= zfirst && issued <= zlast) issue(issued++);
+        red_prev2 = red_prev;
+        red_prev = red_cur;
+        r_prev = r_cur;
+        i_prev = i_cur;
+        e_prev = e_cur;
+        e_cur = e_next;
+        __syncthreads();  // plane t-1 is no longer read
+        if (tid == 0 && t - 1 >= zfirst && issued <= zlast) issue(issued++);
     }
     if (!ok) {
         if (tid == 0) {
             atomicExch(p.status, 1);
-            for (int z = max(zfirst, issued - kSlots2); z < issued; ++z)
+            for (int z = max(zfirst, issued - SLOTS); z < issued; ++z)
                 (void)bar_wait(&S.bar[slot_of(z)], parity_of(z));
         }
         __syncthreads();
@@ -410,19 +276,33 @@ static int make_map(CUtensorMap* map, const float* base, int n, int P, int rows)
 }  // namespace tma
 
 // ---- prolongation add on the padded layout (capi.mojo:677-742 in FP32) -------
-__global__ void prolong_add32_kernel(const float* __restrict__ c, float* __restrict__ f, int n, int P, int cn,
-                                     int cP) {
-    const int64_t total = (int64_t)n * n * n;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % n), y = (int)((i / n) % n), z = (int)(i / ((int64_t)n * n));
-        const int x0 = x >> 1, y0 = y >> 1, z0 = z >> 1;
-        const int x1 = min(x0 + 1, cn - 1), y1 = min(y0 + 1, cn - 1), z1 = min(z0 + 1, cn - 1);
-        const float tx = (x & 1) ? 0.5f : 0.f, ty = (y & 1) ? 0.5f : 0.f, tz = (z & 1) ? 0.5f : 0.f;
-        auto C = [&](int a, int b, int d) { return c[((int64_t)(d + 1) * (cn + 2) + (b + 1)) * cP + (a + 4)]; };
-        const float c00 = C(x0, y0, z0) * (1.f - tx) + C(x1, y0, z0) * tx;
-        const float c10 = C(x0, y1, z0) * (1.f - tx) + C(x1, y1, z0) * tx;
-        const float c01 = C(x0, y0, z1) * (1.f - tx) + C(x1, y0, z1) * tx;
-        const float c11 = C(x0, y1, z1) * (1.f - tx) + C(x1, y1, z1) * tx;
+// Tiled: a block owns a 64 x 4 (x, y) fine tile and 16 fine planes; the fine
+// coordinates come from the launch shape, rows are read and written
+// coalesced, and the coarse values (one coarse node per 2 x 2 x 2 fine nodes)
+// stay in L1/L2 across the fine planes that share them.
+constexpr int kProTX = 64, kProTY = 4, kProTZ = 16;
+
+__global__ void __launch_bounds__(kProTX* kProTY) prolong_add32_kernel(const float* __restrict__ c,
+                                                                       float* __restrict__ f, int n, int P, int cn,
+                                                                       int cP) {
+    const int x = blockIdx.x * kProTX + threadIdx.x, y = blockIdx.y * kProTY + threadIdx.y;
+    if (x >= n || y >= n) return;
+    const int z0 = blockIdx.z * kProTZ, z1 = min(n, z0 + kProTZ);
+    const int xa = x >> 1, ya = y >> 1;
+    const int xb = min(xa + 1, cn - 1), yb = min(ya + 1, cn - 1);
+    const float tx = (x & 1) ? 0.5f : 0.f, ty = (y & 1) ? 0.5f : 0.f;
+    const int64_t cplane = (int64_t)(cn + 2) * cP;
+    const float* ca = c + (int64_t)(ya + 1) * cP + (xa + 4);  // coarse row ya at plane -1 + 1
+    const int64_t dx = xb - xa, dy = (int64_t)(yb - ya) * cP;
+    for (int z = z0; z < z1; ++z) {
+        const int za = z >> 1, zb = min(za + 1, cn - 1);
+        const float tz = (z & 1) ? 0.5f : 0.f;
+        const float* c0 = ca + (int64_t)(za + 1) * cplane;
+        const float* c1 = ca + (int64_t)(zb + 1) * cplane;
+        const float c00 = c0[0] * (1.f - tx) + c0[dx] * tx;
+        const float c10 = c0[dy] * (1.f - tx) + c0[dy + dx] * tx;
+        const float c01 = c1[0] * (1.f - tx) + c1[dx] * tx;
+        const float c11 = c1[dy] * (1.f - tx) + c1[dy + dx] * tx;
         const float v = (c00 * (1.f - ty) + c10 * ty) * (1.f - tz) + (c01 * (1.f - ty) + c11 * ty) * tz;
         f[((int64_t)(z + 1) * (n + 2) + (y + 1)) * P + (x + 4)] += v;
     }
@@ -438,56 +318,15 @@ static int pitch_for(int n) { return ((n + 5) + 7) & ~7; }
 // single-block coarse kernel).  mode 0: from e_in; mode 1: from zero.
 // z_chunk <= 0 picks one that fills the 148 SMs with two blocks each.
 // *status (device int) is set to 1 if a bounded wait gave up.
-template <typename K>
-static int launch_sweep(K kernel, size_t smem, int ty, int n, int z_chunk, cudaStream_t s, const float* e_in,
-                        const float* rhs, const float* invD, pb::tma::Params prm) {
-    using namespace pb::tma;
-    const int P = prm.P;
-    prm.nty = (n - 1) / ty > 0 ? (n - 1) / ty : 1;
-    const int tiles = prm.ntx * prm.nty;
-    int per_sm = (int)((228 * 1024) / (smem + 1024));
-    if (per_sm < 1) per_sm = 1;
-    if (per_sm > 2) per_sm = 2 + (per_sm > 2);  // register file: at most 3 blocks of 256 threads
-    if (z_chunk <= 0) {
-        const int want = per_sm * kSMs;
-        int chunks = want / tiles > 1 ? want / tiles : 1;
-        z_chunk = (n + chunks - 1) / chunks;
-        if (z_chunk < 4) z_chunk = 4;
-    }
-    prm.z_chunk = z_chunk;
-    CUtensorMap me, mr, mi;
-    const int rows = ty + 5;
-    PB_TRY(make_map(&mr, rhs, n, P, rows));
-    PB_TRY(make_map(&mi, invD, n, P, rows));
-    PB_TRY(make_map(&me, e_in ? e_in : rhs, n, P, rows));
-    const dim3 grid(prm.ntx, prm.nty, (n + z_chunk - 1) / z_chunk);
-    PB_CHECK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                  "sweep_tma smem");
-    kernel<<<grid, kThreads, smem, s>>>(me, mr, mi, prm);
-    PB_CHECK_LAUNCH("sweep_tma kernel");
-    return PB_OK;
-}
-
-template <int TY, int SLOTS>
-static int launch_v2(bool zero_in, int n, int z_chunk, cudaStream_t s, const float* e_in, const float* rhs,
-                     const float* invD, const pb::tma::Params& prm) {
-    using namespace pb::tma;
-    const size_t smem = sizeof(typename Geo2<TY, SLOTS>::Smem) + 128;
-    return zero_in ? launch_sweep(sweep_v2_kernel<true, TY, SLOTS>, smem, TY, n, z_chunk, s, nullptr, rhs, invD, prm)
-                   : launch_sweep(sweep_v2_kernel<false, TY, SLOTS>, smem, TY, n, z_chunk, s, e_in, rhs, invD, prm);
-}
-
-// Bits 8..15 of `mode` select a tile-height / ring-depth configuration of the
-// kernel (0: 16 rows, 6 slots — the default); bit 2 selects the first TMA
-// version.  Both are there for tuning runs.
+// One TMA-staged fused sweep.  n = 2^k + 1 >= 33 (smaller levels use the
+// single-block coarse kernel).  mode 0: from e_in; mode 1: from zero.
+// z_chunk <= 0 picks one that puts two blocks on each of the 148 SMs.
+// *status (device int) is set to 1 if a bounded wait gave up.
 extern "C" int pb_sweep_tma_f32(const float* e_in, float* e_out, const float* rhs, const float* invD, int64_t n,
                                 int64_t mode, int64_t z_chunk, int* status, void* stream) {
     using namespace pb::tma;
-    const bool legacy = (mode & 4) != 0;
-    const int variant = (int)((mode >> 8) & 0xff);
-    mode &= 3;
     if (n < 33 || n > 4097 || ((n - 1) & (n - 2)) || !e_out || !rhs || !invD || !status || (mode == 0 && !e_in) ||
-        mode > 1 || variant > 5)
+        mode < 0 || mode > 1)
         return fail(PB_ERR_INVALID, "sweep_tma: bad args (n must be 2^k + 1 >= 33)");
     if (e_in == e_out) return fail(PB_ERR_INVALID, "sweep_tma: out of place only");
     const int N = (int)n;
@@ -496,36 +335,42 @@ extern "C" int pb_sweep_tma_f32(const float* e_in, float* e_out, const float* rh
     prm.P = pitch_for(N);
     prm.plane = (int64_t)(N + 2) * prm.P;
     prm.ntx = (N - 1) / kTX > 0 ? (N - 1) / kTX : 1;
-    prm.nty = 1;
-    prm.z_chunk = 0;
+    prm.nty = (N - 1) / kTY > 0 ? (N - 1) / kTY : 1;
+    const int tiles = prm.ntx * prm.nty;
+    if (z_chunk <= 0) {
+        const int want = 2 * kSMs;
+        int chunks = want / tiles > 1 ? want / tiles : 1;
+        z_chunk = (N + chunks - 1) / chunks;
+        if (z_chunk < 4) z_chunk = 4;
+    }
+    prm.z_chunk = (int)z_chunk;
     prm.h2 = (float)((N - 1) * (N - 1));
     prm.e_out = e_out;
     prm.status = status;
+    CUtensorMap me, mr, mi;
+    PB_TRY(make_map(&mr, rhs, N, prm.P, kBoxY));
+    PB_TRY(make_map(&mi, invD, N, prm.P, kBoxY));
+    PB_TRY(make_map(&me, mode == 1 ? rhs : e_in, N, prm.P, kBoxY));
+    const dim3 grid(prm.ntx, prm.nty, (N + prm.z_chunk - 1) / prm.z_chunk);
+    const size_t smem = sizeof(Geo2<kTY, kSlots>::Smem) + 128;
     cudaStream_t s = (cudaStream_t)stream;
-    const bool zero = mode == 1;
-    if (legacy) {
-        const size_t smem = sizeof(Smem) + 128;
-        return zero ? launch_sweep(sweep_kernel<true>, smem, kTY, N, (int)z_chunk, s, nullptr, rhs, invD, prm)
-                    : launch_sweep(sweep_kernel<false>, smem, kTY, N, (int)z_chunk, s, e_in, rhs, invD, prm);
-    }
-    switch (variant) {
-        case 1: return launch_v2<16, 8>(zero, N, (int)z_chunk, s, e_in, rhs, invD, prm);
-        case 2: return launch_v2<8, 6>(zero, N, (int)z_chunk, s, e_in, rhs, invD, prm);
-        case 3: return launch_v2<8, 8>(zero, N, (int)z_chunk, s, e_in, rhs, invD, prm);
-        case 4: return launch_v2<8, 10>(zero, N, (int)z_chunk, s, e_in, rhs, invD, prm);
-        case 5: return launch_v2<16, 7>(zero, N, (int)z_chunk, s, e_in, rhs, invD, prm);
-        default: return launch_v2<16, 6>(zero, N, (int)z_chunk, s, e_in, rhs, invD, prm);
-    }
+    auto launch = [&](auto kernel) -> int {
+        PB_CHECK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                      "sweep_tma smem");
+        kernel<<<grid, kThreads, smem, s>>>(me, mr, mi, prm);
+        PB_CHECK_LAUNCH("sweep_tma kernel");
+        return PB_OK;
+    };
+    return mode == 1 ? launch(sweep_kernel<true, kSlots>) : launch(sweep_kernel<false, kSlots>);
 }
 
 // fine += trilinear prolongation of coarse (side (n+1)/2), padded layouts.
 extern "C" int pb_prolong_add_f32(const float* coarse, float* fine, int64_t fine_n, void* stream) {
     if (fine_n < 3 || fine_n > 4097 || !coarse || !fine) return fail(PB_ERR_INVALID, "prolong32: bad args");
     const int n = (int)fine_n, cn = (n + 1) / 2;
-    int64_t blocks = ((int64_t)n * n * n + 255) / 256;
-    if (blocks > kSMs * 16) blocks = kSMs * 16;
-    prolong_add32_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(coarse, fine, n, pitch_for(n), cn,
-                                                                             pitch_for(cn));
+    const dim3 grid((n + kProTX - 1) / kProTX, (n + kProTY - 1) / kProTY, (n + kProTZ - 1) / kProTZ);
+    prolong_add32_kernel<<<grid, dim3(kProTX, kProTY), 0, (cudaStream_t)stream>>>(coarse, fine, n, pitch_for(n), cn,
+                                                                                   pitch_for(cn));
     PB_CHECK_LAUNCH("prolong_add32_kernel");
     return PB_OK;
 }

@@ -55,9 +55,7 @@ class Level32:
 class Hierarchy32:
     """FP32 levels (padded layout) built from the FP64 screen hierarchy."""
 
-    def __init__(self, screen: torch.Tensor, point_weight: float, workspace: nat.Workspace, z_chunk: int = 0,
-                 use_tma: bool = True):
-        self.use_tma = use_tma
+    def __init__(self, screen: torch.Tensor, point_weight: float, workspace: nat.Workspace, z_chunk: int = 0):
         self.status = torch.zeros(1, dtype=torch.int32, device=screen.device)
         self.lib = nat.lib()
         self.stream = nat.stream_handle()
@@ -89,25 +87,22 @@ class Hierarchy32:
         )
 
     def _sweep(self, lv: Level32, src, dst, mode: int, coarse=None) -> None:
+        """One red-black sweep dst <- S(src); mode 1 starts from zero, mode 2
+        first adds the prolongated coarse correction to src in place."""
         L = self.lib
-        if self.use_tma:
-            if mode == 2:  # prolongation added in place, then a plain sweep
-                nat.check(L.pb_prolong_add_f32(coarse.data_ptr(), src.data_ptr(), lv.n, self.stream), "prolong32")
-                mode = 0
-            probe = PROBE if (PROBE is not None and lv is self.levels[0]) else None
-            if probe is not None:
-                start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                start.record()
-            nat.check(L.pb_sweep_tma_f32(None if src is None else src.data_ptr(), dst.data_ptr(), lv.rhs.data_ptr(),
-                                         lv.invD.data_ptr(), lv.n, mode, self.z_chunk, self.status.data_ptr(),
-                                         self.stream), "sweep")
-            if probe is not None:
-                end.record()
-                probe.append((start, end, mode))
-            return
-        nat.check(L.pb_sweep_f32(None if src is None else src.data_ptr(), dst.data_ptr(), lv.rhs.data_ptr(),
-                                 lv.invD.data_ptr(), None if coarse is None else coarse.data_ptr(), lv.n,
-                                 mode, self.z_chunk if self.z_chunk > 0 else 32, self.stream), "sweep")
+        if mode == 2:
+            nat.check(L.pb_prolong_add_f32(coarse.data_ptr(), src.data_ptr(), lv.n, self.stream), "prolong32")
+            mode = 0
+        probe = PROBE if (PROBE is not None and lv is self.levels[0]) else None
+        if probe is not None:
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+        nat.check(L.pb_sweep_tma_f32(None if src is None else src.data_ptr(), dst.data_ptr(), lv.rhs.data_ptr(),
+                                     lv.invD.data_ptr(), lv.n, mode, self.z_chunk, self.status.data_ptr(),
+                                     self.stream), "sweep")
+        if probe is not None:
+            end.record()
+            probe.append((start, end, mode))
 
     def check_status(self) -> None:
         if int(self.status.item()):
@@ -128,10 +123,9 @@ class Hierarchy32:
         for _ in range(pre - 1):
             self._sweep(lv, src, dst, 0)
             src, dst = dst, src
-        nat.check(L.pb_residual_f32(src.data_ptr(), lv.rhs.data_ptr(), lv.D.data_ptr(), lv.res.data_ptr(), lv.n, s),
-                  "residual32")
         nxt = self.levels[level + 1]
-        nat.check(L.pb_restrict_f32(lv.res.data_ptr(), nxt.rhs.data_ptr(), lv.n, s), "restrict32")
+        nat.check(L.pb_residual_restrict_f32(src.data_ptr(), lv.rhs.data_ptr(), lv.D.data_ptr(), nxt.rhs.data_ptr(),
+                                             lv.n, s), "residual_restrict32")
         coarse = self.v_cycle(level + 1, pre, post)
         # post-smoothing: the first sweep adds the prolongated correction on load
         self._sweep(lv, src, dst, 2, coarse)
@@ -144,7 +138,7 @@ class Hierarchy32:
 
 def solve_refined(rhs: torch.Tensor, screen: torch.Tensor, point_weight: float, workspace: nat.Workspace, *,
                   tol: float = 1e-8, max_cycles: int = 200, has_points: bool = True,
-                  z_chunk: int = 0, use_tma: bool = True, method: str = "fcg") -> tuple[torch.Tensor, SolveStats]:
+                  z_chunk: int = 0, method: str = "fcg") -> tuple[torch.Tensor, SolveStats]:
     """FP64-accurate solve with FP32 V-cycles.
 
     method="fcg": flexible conjugate gradients FCG(1) in FP64 with the FP32
@@ -165,7 +159,7 @@ def solve_refined(rhs: torch.Tensor, screen: torch.Tensor, point_weight: float, 
         stats.rhs_norm = 0.0
         return x, stats
     nat.check(L.pb_fill_f64(x.data_ptr(), x.numel(), 0.5, s), "fill")  # core.py:270
-    h = Hierarchy32(screen, point_weight, workspace, z_chunk, use_tma)
+    h = Hierarchy32(screen, point_weight, workspace, z_chunk)
     bnorm = norm(rhs, workspace, torch.empty(1, dtype=torch.float64, device=device))
     norm2 = torch.empty(1, dtype=torch.float64, device=device)
     ws = nat.Workspace(device)
