@@ -182,18 +182,28 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
             refined_e2e()
     torch.cuda.synchronize()
 
-    # headline: FP32-refined, inputs resident in HBM; the level-0 sweep launches
-    # are bracketed with CUDA events on the launching stream for the roofline
-    probe = []
-    solver32.PROBE = probe
+    # headline: FP32-refined, inputs resident in HBM
     launches0 = lib.pb_launch_count()
     with ClockSampler(local) as clocks:
         total_ms, per = timed(refined_device, args.steps)
     launches = lib.pb_launch_count() - launches0
-    solver32.PROBE = None
     clock_info = clocks.summary()
-    sweep_ms = [a.elapsed_time(b) for a, b, mode in probe if mode == 0]
     value = world * args.steps / (total_ms / 1e3)
+
+    # dominant kernel: inside the timed solves it runs in graph replays, where
+    # host events cannot bracket it; time it right after the timed region on
+    # the same cached engine (same buffers and launch shapes) with CUDA events
+    # on the engine's stream around each finest-level sweep of eager V-cycles
+    n_side = (1 << args.depth) + 1
+    eng = solver32.engine_for(n_side, 4.0, dev)
+    probe = []
+    solver32.PROBE = probe
+    with torch.cuda.stream(eng.stream):
+        for _ in range(5):
+            eng.h.v_cycle(0)
+    torch.cuda.synchronize()
+    solver32.PROBE = None
+    sweep_ms = [a.elapsed_time(b) for a, b, mode in probe if mode == 0]
     if args.profile:
         if rank == 0:
             print(json.dumps({"profile": True, "value": value, "launches_per_step": launches / args.steps}))
@@ -262,6 +272,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
                     "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                     "frac": round(achieved / peak, 4), "peak_source": peak_src,
                     "avg_launch_ms": round(avg_ms, 4), "launches_timed": len(sweep_ms),
+                    "timing": "CUDA events on the launching stream around each finest-level sweep of 5 eager "
+                              "V-cycles on the timed solves' engine, right after the timed region",
                     "algorithmic_bytes_per_launch": int(algorithmic), "traffic": read_profile_traffic()}
 
     if rank != 0:

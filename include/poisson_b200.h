@@ -210,6 +210,32 @@ int pb_sweep_tma_f32(const float *e_in, float *e_out, const float *rhs, const fl
                      int64_t mode, int64_t z_chunk, int *status, void *stream);
 /* fine += trilinear prolongation of coarse (side (n+1)/2), padded layouts. */
 int pb_prolong_add_f32(const float *coarse, float *fine, int64_t fine_n, void *stream);
+/* Graph-friendly FCG(1) step: p = z - beta p in place (p = z while flags[0]
+ * != 0), q = A p, alpha, x += alpha p, r -= alpha q, r32 = (float) r;
+ * scal[0..4] as for pb_fcg_step_f64.  Touches the same buffers every call, so
+ * an iteration can be captured once and replayed. */
+int pb_fcg_step_inplace_f64(const float *z, double *p, double *q, double *x, double *r, float *r32,
+                            const double *screen, int64_t n, double point_weight, double *scal,
+                            const int *flags, void *workspace, size_t workspace_bytes, void *stream);
+
+/* Device-driven iteration (no counterpart in the reference).  Begin: a graph
+ * with one WHILE conditional node; `stream` is captured into its body until
+ * pb_loop_capture_end, which instantiates it.  The body's last launch must be
+ * pb_loop_condition(handle, ...): it counts the iteration (flags[1]), clears
+ * flags[0], records scal[4] in history[iteration-1] (if not NULL) and keeps
+ * looping while scal[4] > ctrl[0] and fewer than min(max_iter, ctrl[1])
+ * iterations ran (max_iter also bounds history).
+ * handle = 0 runs the same bookkeeping eagerly.  Every pb_graph_launch runs
+ * the loop to completion on the device. */
+int pb_loop_capture_begin(void *stream, void **graph, unsigned long long *handle);
+int pb_loop_condition(unsigned long long handle, const double *scal, const double *ctrl, int *flags,
+                      int64_t max_iter, double *history, void *stream);
+int pb_loop_capture_end(void *stream, void *graph, void **exec);
+int pb_graph_launch(void *exec, void *stream);
+int pb_graph_destroy(void *exec, void *graph);
+/* Adds launches that ran inside graphs to pb_launch_count(). */
+int pb_note_launches(long long count);
+
 /* coarse_rhs (side (n+1)/2) = full-weighting restriction of rhs - A e (side
  * n), in FP32 on the padded layout, without writing the fine residual. */
 int pb_residual_restrict_f32(const float *e, const float *rhs, const float *D, float *coarse_rhs,

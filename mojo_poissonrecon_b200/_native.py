@@ -61,6 +61,13 @@ _SIGNATURES = {
     "pb_defect_f64": ([P, P, P, P, P, I, F, P, P, P, P, S, P], C),
     "pb_fcg_workspace_size": ([I], S),
     "pb_fcg_step_f64": ([P, P, P, P, P, P, P, P, I, F, P, I, P, S, P], C),
+    "pb_fcg_step_inplace_f64": ([P, P, P, P, P, P, P, I, F, P, P, P, S, P], C),
+    "pb_loop_capture_begin": ([P, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_ulonglong)], C),
+    "pb_loop_condition": ([ctypes.c_ulonglong, P, P, P, I, P, P], C),
+    "pb_loop_capture_end": ([P, P, ctypes.POINTER(ctypes.c_void_p)], C),
+    "pb_graph_launch": ([P, P], C),
+    "pb_graph_destroy": ([P, P], C),
+    "pb_note_launches": ([ctypes.c_longlong], C),
     "pb_sweep_tma_f32": ([P, P, P, P, I, I, I, P, P], C),
     "pb_prolong_add_f32": ([P, P, I, P], C),
     "pb_residual_restrict_f32": ([P, P, P, P, I, P], C),

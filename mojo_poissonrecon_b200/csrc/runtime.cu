@@ -32,6 +32,11 @@ extern "C" int pb_version(void) { return 10000; }
 
 extern "C" long long pb_launch_count(void) { return pb::g_launches.load(std::memory_order_relaxed); }
 
+extern "C" int pb_note_launches(long long count) {
+    if (count > 0) pb::g_launches.fetch_add(count, std::memory_order_relaxed);
+    return 0;
+}
+
 extern "C" int pb_init(int device) {
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return pb::cuda_fail(e, "pb_init: cudaSetDevice");

@@ -1,26 +1,31 @@
 """FP64-accurate solves driven by FP32 V-cycles (``precision="fp32_refined"``).
 
-Defect correction (method="defect"):
+FCG(1) (the default, ``RefinedEngine``): the FP32 V-cycle preconditions FP64
+flexible conjugate gradients:
 
-    x = 0.5                                    (the reference's initial guess, core.py:270)
-    r = b - A x,  ||r||                        FP64 (pb_defect_f64)
-    while ||r|| > tol * ||b||:
-        e = V(3,3)-cycle on A e = r from e = 0 FP32 (the reference's cycle shape)
-        x = x + e;  r = b - A x                FP64, fused in one kernel
+    x = 0.5                                  (the reference's initial guess, core.py:270)
+    r = b - A x                              FP64 (pb_defect_f64)
+    while ||r|| > tol * ||b||:               evaluated on the device
+        z = V(3,3)-cycle on A e = r, e = 0   FP32 (the reference's operator and cycle shape)
+        p = z - beta p;  q = A p;  x += alpha p;  r -= alpha q      FP64 (pb_fcg_step_inplace_f64)
 
-FCG(1) (method="fcg", the default): the same FP32 V-cycle preconditions FP64
-flexible conjugate gradients (pb_fcg_step_f64), which needs about 2.5x fewer
-V-cycles to reach the same FP64 residual.
+One iteration touches the same buffers every time, so the engine captures it
+once as the body of a CUDA graph WHILE node whose condition a device kernel
+sets from ||r||^2 (pb_loop_condition); a solve is then one graph launch with
+no host synchronisation per iteration.  Engines (hierarchy, vectors, graph)
+are cached per device, grid side and point weight and reused across solves.
+
+Defect correction (``precision="fp32_defect"``): x += V(r), one FP32 V-cycle
+per FP64 residual, eager launches; about 2.5x more V-cycles than FCG(1).
 
 The FP32 cycle reuses the reference's operator, red-black smoother, boundary-
 normalised full weighting, trilinear prolongation and 40 sweeps on the 3^3
-grid (core.py:141-193); levels of side <= 17 run in a single launch.  Each
-outer step contracts the error like one FP64 V-cycle while the FP64 residual
-keeps the fixed point exact, so the iterate converges to the FP64 solution.
+grid (core.py:141-193); levels of side <= 17 run in a single launch.
 """
 
 from __future__ import annotations
 
+import collections
 import ctypes
 import math
 
@@ -30,15 +35,17 @@ from . import _native as nat
 from .solver import SolveStats, level_sizes, norm
 
 COARSE_N = 17  # levels of this side or smaller: one single-block launch
+MAX_ITER = 512  # capacity of the device iteration history (and hard cap)
 
-# When set to a list, every finest-level sweep launch appends (start, end, mode)
-# CUDA events recorded on the launching stream around it (used by bench.py to
-# time the dominant kernel inside its timed region).
+# When set to a list, every finest-level sweep launched eagerly appends
+# (start, end, mode) CUDA events recorded on the launching stream around it.
 PROBE: list | None = None
 
 
 class Level32:
-    def __init__(self, n: int, screen64: torch.Tensor, pw: float, device: torch.device, lib, stream):
+    """Padded FP32 arrays of one level (zero-filled so the ghosts stay zero)."""
+
+    def __init__(self, n: int, device: torch.device, lib):
         self.n = n
         pitch, count = ctypes.c_int64(), ctypes.c_int64()
         nat.check(lib.pb_level_geometry(n, ctypes.byref(pitch), ctypes.byref(count)), "level geometry")
@@ -48,31 +55,20 @@ class Level32:
             return torch.zeros(self.count, dtype=torch.float32, device=device)
 
         self.D, self.invD, self.rhs, self.res, self.ea, self.eb = (zeros() for _ in range(6))
-        nat.check(lib.pb_level_setup_f32(screen64.data_ptr(), n, pw, self.D.data_ptr(), self.invD.data_ptr(),
-                                         stream), "level setup")
 
 
 class Hierarchy32:
-    """FP32 levels (padded layout) built from the FP64 screen hierarchy."""
+    """FP32 levels (padded layout); `setup` fills D and 1/D from an FP64 screen."""
 
-    def __init__(self, screen: torch.Tensor, point_weight: float, workspace: nat.Workspace, z_chunk: int = 0):
-        self.status = torch.zeros(1, dtype=torch.int32, device=screen.device)
+    def __init__(self, n: int, device: torch.device, z_chunk: int = 0):
+        self.status = torch.zeros(1, dtype=torch.int32, device=device)
         self.lib = nat.lib()
-        self.stream = nat.stream_handle()
-        self.ws = workspace
-        self.pw = float(point_weight)
+        self.device = device
         self.z_chunk = int(z_chunk)
-        L, s = self.lib, self.stream
-        self.sizes = level_sizes(screen.shape[0])
-        screens = [screen]
-        for n in self.sizes[1:]:
-            coarse = torch.empty((n, n, n), dtype=torch.float64, device=screen.device)
-            nat.check(L.pb_restrict_f64(screens[-1].data_ptr(), coarse.data_ptr(), screens[-1].shape[0], s),
-                      "restrict")
-            nat.check(L.pb_scale_f64(coarse.data_ptr(), coarse.numel(), 4.0, s), "scale")
-            screens.append(coarse)
-        self.levels = [Level32(n, scr, self.pw, screen.device, L, s) for n, scr in zip(self.sizes, screens)]
-        self.first_coarse = next(i for i, n in enumerate(self.sizes) if n <= COARSE_N)
+        self.sizes = level_sizes(n)
+        self.levels = [Level32(m, device, self.lib) for m in self.sizes]
+        self.coarse_screens = [torch.empty((m, m, m), dtype=torch.float64, device=device) for m in self.sizes[1:]]
+        self.first_coarse = next(i for i, m in enumerate(self.sizes) if m <= COARSE_N)
         tail = self.levels[self.first_coarse:]
         k = len(tail)
         ptrs = lambda ts: (ctypes.c_void_p * k)(*[t.data_ptr() for t in ts])
@@ -85,21 +81,38 @@ class Hierarchy32:
             ptrs([lv.D for lv in tail]),
             ptrs([lv.invD for lv in tail]),
         )
+        self.pw = None
+
+    @property
+    def stream(self) -> int:
+        return nat.stream_handle()
+
+    def setup(self, screen: torch.Tensor, point_weight: float) -> None:
+        """core.py:267-269 screening hierarchy (FP64), then D and 1/D per level."""
+        L, s = self.lib, self.stream
+        self.pw = float(point_weight)
+        screens = [screen] + self.coarse_screens
+        for fine, coarse in zip(screens[:-1], screens[1:]):
+            nat.check(L.pb_restrict_f64(fine.data_ptr(), coarse.data_ptr(), fine.shape[0], s), "restrict")
+            nat.check(L.pb_scale_f64(coarse.data_ptr(), coarse.numel(), 4.0, s), "scale")
+        for lv, scr in zip(self.levels, screens):
+            nat.check(L.pb_level_setup_f32(scr.data_ptr(), lv.n, self.pw, lv.D.data_ptr(), lv.invD.data_ptr(), s),
+                      "level setup")
 
     def _sweep(self, lv: Level32, src, dst, mode: int, coarse=None) -> None:
         """One red-black sweep dst <- S(src); mode 1 starts from zero, mode 2
         first adds the prolongated coarse correction to src in place."""
-        L = self.lib
+        L, s = self.lib, self.stream
         if mode == 2:
-            nat.check(L.pb_prolong_add_f32(coarse.data_ptr(), src.data_ptr(), lv.n, self.stream), "prolong32")
+            nat.check(L.pb_prolong_add_f32(coarse.data_ptr(), src.data_ptr(), lv.n, s), "prolong32")
             mode = 0
         probe = PROBE if (PROBE is not None and lv is self.levels[0]) else None
         if probe is not None:
             start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             start.record()
         nat.check(L.pb_sweep_tma_f32(None if src is None else src.data_ptr(), dst.data_ptr(), lv.rhs.data_ptr(),
-                                     lv.invD.data_ptr(), lv.n, mode, self.z_chunk, self.status.data_ptr(),
-                                     self.stream), "sweep")
+                                     lv.invD.data_ptr(), lv.n, mode, self.z_chunk, self.status.data_ptr(), s),
+                  "sweep")
         if probe is not None:
             end.record()
             probe.append((start, end, mode))
@@ -117,8 +130,7 @@ class Hierarchy32:
             return self.levels[level].ea
         lv = self.levels[level]
         a, b = lv.ea, lv.eb
-        # pre-smoothing from zero: a <- S(0), then alternate
-        self._sweep(lv, None, a, 1)
+        self._sweep(lv, None, a, 1)  # pre-smoothing from zero
         src, dst = a, b
         for _ in range(pre - 1):
             self._sweep(lv, src, dst, 0)
@@ -127,8 +139,7 @@ class Hierarchy32:
         nat.check(L.pb_residual_restrict_f32(src.data_ptr(), lv.rhs.data_ptr(), lv.D.data_ptr(), nxt.rhs.data_ptr(),
                                              lv.n, s), "residual_restrict32")
         coarse = self.v_cycle(level + 1, pre, post)
-        # post-smoothing: the first sweep adds the prolongated correction on load
-        self._sweep(lv, src, dst, 2, coarse)
+        self._sweep(lv, src, dst, 2, coarse)  # post-smoothing; the first adds the correction
         src, dst = dst, src
         for _ in range(post - 1):
             self._sweep(lv, src, dst, 0)
@@ -136,69 +147,211 @@ class Hierarchy32:
         return src
 
 
+class RefinedEngine:
+    """FCG(1) state for one grid side and point weight, reused across solves.
+
+    Not thread-safe: one engine serves one stream at a time (the batch and
+    serving paths create one engine per concurrent slot)."""
+
+    def __init__(self, n: int, point_weight: float, device: torch.device):
+        self.n = n
+        self.pw = float(point_weight)
+        self.device = device
+        self.lib = nat.lib()
+        # Graph capture needs a stream other than the legacy default stream;
+        # the engine's buffers are allocated on it and it runs every solve.
+        self.stream = torch.cuda.Stream(device=device)
+        with torch.cuda.stream(self.stream):
+            self._allocate(n, device)
+
+    def _allocate(self, n: int, device: torch.device) -> None:
+        self.h = Hierarchy32(n, device)
+        f64 = lambda: torch.empty((n, n, n), dtype=torch.float64, device=device)
+        self.screen, self.x, self.r, self.p, self.q = f64(), f64(), f64(), f64(), f64()
+        self.scal = torch.zeros(8, dtype=torch.float64, device=device)
+        self.ctrl = torch.zeros(2, dtype=torch.float64, device=device)
+        self.flags = torch.zeros(4, dtype=torch.int32, device=device)
+        self.history = torch.zeros(MAX_ITER, dtype=torch.float64, device=device)
+        self.norm2 = torch.empty(1, dtype=torch.float64, device=device)
+        self.bnorm = torch.empty(1, dtype=torch.float64, device=device)
+        self.ws = nat.Workspace(device)
+        self.ws_ptr, self.ws_size = self.ws.get(max(self.lib.pb_defect_workspace_size(n),
+                                                    self.lib.pb_fcg_workspace_size(n)))
+        self.norm_ws = nat.Workspace(device)
+        self.norm_ws.get(1 << 16)
+        self.graph = ctypes.c_void_p()
+        self.exec = ctypes.c_void_p()
+        self.body_launches = 0
+
+    def __del__(self):
+        try:
+            if self.exec.value or self.graph.value:
+                self.lib.pb_graph_destroy(self.exec, self.graph)
+        except Exception:
+            pass
+
+    def nbytes(self) -> int:
+        return sum(t.numel() * t.element_size() for t in
+                   (self.screen, self.x, self.r, self.p, self.q)) + sum(
+            6 * lv.count * 4 for lv in self.h.levels)
+
+    def _iteration(self, handle: int) -> None:
+        L, s = self.lib, nat.stream_handle()
+        z = self.h.v_cycle(0)
+        nat.check(L.pb_fcg_step_inplace_f64(z.data_ptr(), self.p.data_ptr(), self.q.data_ptr(), self.x.data_ptr(),
+                                            self.r.data_ptr(), self.h.levels[0].rhs.data_ptr(),
+                                            self.screen.data_ptr(), self.n, self.pw, self.scal.data_ptr(),
+                                            self.flags.data_ptr(), self.ws_ptr, self.ws_size, s), "fcg step")
+        nat.check(L.pb_loop_condition(handle, self.scal.data_ptr(), self.ctrl.data_ptr(), self.flags.data_ptr(),
+                                      MAX_ITER, self.history.data_ptr(), s), "loop condition")
+
+    def _capture(self) -> None:
+        """Capture one iteration as the body of a device-evaluated WHILE loop."""
+        L = self.lib
+        s = nat.stream_handle()
+        handle = ctypes.c_ulonglong()
+        before = L.pb_launch_count()
+        nat.check(L.pb_loop_capture_begin(s, ctypes.byref(self.graph), ctypes.byref(handle)), "loop capture")
+        try:
+            self._iteration(handle.value)
+        except Exception:
+            end = ctypes.c_void_p()
+            L.pb_loop_capture_end(s, self.graph, ctypes.byref(end))
+            self.graph = ctypes.c_void_p()
+            raise
+        nat.check(L.pb_loop_capture_end(s, self.graph, ctypes.byref(self.exec)), "loop capture end")
+        self.body_launches = L.pb_launch_count() - before
+
+    def _start(self, rhs: torch.Tensor) -> None:
+        """x = 0.5, r = b - A x (FP64 and its FP32 copy), ||r||^2."""
+        L, s = self.lib, nat.stream_handle()
+        nat.check(L.pb_fill_f64(self.x.data_ptr(), self.x.numel(), 0.5, s), "fill")  # core.py:270
+        nat.check(L.pb_defect_f64(self.x.data_ptr(), None, None, rhs.data_ptr(), self.screen.data_ptr(), self.n,
+                                  self.pw, self.h.levels[0].rhs.data_ptr(), self.r.data_ptr(),
+                                  self.norm2.data_ptr(), self.ws_ptr, self.ws_size, s), "defect")
+
+    def solve(self, rhs: torch.Tensor, screen: torch.Tensor, tol: float,
+              max_cycles: int) -> tuple[torch.Tensor, SolveStats]:
+        """Solve on the engine's stream, ordered after the caller's stream's
+        work (rhs, screen) and before its later work (the returned field)."""
+        caller = torch.cuda.current_stream(self.device)
+        self.stream.wait_stream(caller)
+        with torch.cuda.stream(self.stream):
+            stats = self._solve(rhs, screen, tol, max_cycles)
+        caller.wait_stream(self.stream)
+        return self.x.clone(), stats
+
+    def _solve(self, rhs: torch.Tensor, screen: torch.Tensor, tol: float, max_cycles: int) -> SolveStats:
+        L, s = self.lib, nat.stream_handle()
+        stats = SolveStats()
+        self.screen.copy_(screen)
+        self.h.setup(self.screen, self.pw)
+        self._start(rhs)
+        norm(rhs, self.norm_ws, self.bnorm)
+        both = torch.cat([self.norm2, self.bnorm]).cpu()
+        stats.rhs_norm = float(both[1])
+        r = math.sqrt(max(float(both[0]), 0.0))
+        stats.history.append(r)
+        target = tol * stats.rhs_norm
+        if r > target and max_cycles > 0:
+            self.ctrl.copy_(torch.tensor([target * target, float(max_cycles)], dtype=torch.float64))
+            if not self.exec.value:
+                # one eager iteration first sets kernel attributes outside the
+                # capture; its effect is discarded by restarting below
+                self.flags.zero_()
+                self.flags[0] = 1
+                self._iteration(0)
+                self._start(rhs)
+                self._capture()
+            self.flags.zero_()
+            self.flags[0] = 1
+            nat.check(L.pb_graph_launch(self.exec, s), "graph launch")
+            it = int(self.flags[1].item())
+            L.pb_note_launches(it * self.body_launches)
+            stats.cycles = it
+            stats.history.extend(math.sqrt(max(v, 0.0)) for v in self.history[:it].cpu().tolist())
+        # the recurrence r -= alpha q drifts from b - A x by rounding; report the true residual
+        nat.check(L.pb_defect_f64(self.x.data_ptr(), None, None, rhs.data_ptr(), self.screen.data_ptr(), self.n,
+                                  self.pw, self.h.levels[0].rhs.data_ptr(), None, self.norm2.data_ptr(),
+                                  self.ws_ptr, self.ws_size, s), "defect")
+        stats.residual_norm = math.sqrt(max(float(self.norm2.item()), 0.0))
+        self.h.check_status()
+        return stats
+
+
+_ENGINES: "collections.OrderedDict[tuple, RefinedEngine]" = collections.OrderedDict()
+ENGINE_CACHE_SIZE = 3
+
+
+def engine_for(n: int, point_weight: float, device: torch.device, slot: int = 0) -> RefinedEngine:
+    """A cached engine for (device, n, point_weight, slot); least recently used
+    engines are dropped beyond ENGINE_CACHE_SIZE (or when memory runs short)."""
+    key = (device.index, n, float(point_weight), slot)
+    eng = _ENGINES.pop(key, None)
+    if eng is None:
+        while len(_ENGINES) >= ENGINE_CACHE_SIZE:
+            _ENGINES.popitem(last=False)
+        try:
+            eng = RefinedEngine(n, point_weight, device)
+        except torch.cuda.OutOfMemoryError:
+            _ENGINES.clear()
+            torch.cuda.empty_cache()
+            eng = RefinedEngine(n, point_weight, device)
+    _ENGINES[key] = eng
+    return eng
+
+
+def clear_engines() -> None:
+    _ENGINES.clear()
+
+
 def solve_refined(rhs: torch.Tensor, screen: torch.Tensor, point_weight: float, workspace: nat.Workspace, *,
                   tol: float = 1e-8, max_cycles: int = 200, has_points: bool = True,
-                  z_chunk: int = 0, method: str = "fcg") -> tuple[torch.Tensor, SolveStats]:
-    """FP64-accurate solve with FP32 V-cycles.
+                  method: str = "fcg", slot: int = 0) -> tuple[torch.Tensor, SolveStats]:
+    """FP64-accurate solve with FP32 V-cycles; stats.cycles counts V-cycles.
 
-    method="fcg": flexible conjugate gradients FCG(1) in FP64 with the FP32
-    V-cycle as preconditioner (default; about 2.5x fewer V-cycles).
-    method="defect": plain defect correction, x += V(r), one V-cycle per step.
-    stats.cycles counts V-cycles either way."""
+    method="fcg": FCG(1) on a cached RefinedEngine (graph-driven loop).
+    method="defect": plain defect correction, x += V(r), eager launches."""
     if method not in ("fcg", "defect"):
         raise ValueError("method must be 'fcg' or 'defect'")
     L = nat.lib()
     s = nat.stream_handle()
     n = rhs.shape[0]
     device = rhs.device
-    stats = SolveStats()
-    x = torch.empty_like(rhs)
     if not has_points:
+        x = torch.empty_like(rhs)
         nat.check(L.pb_fill_f64(x.data_ptr(), x.numel(), 0.0, s), "fill")
+        stats = SolveStats()
         stats.residual_norm = 0.0
         stats.rhs_norm = 0.0
         return x, stats
-    nat.check(L.pb_fill_f64(x.data_ptr(), x.numel(), 0.5, s), "fill")  # core.py:270
-    h = Hierarchy32(screen, point_weight, workspace, z_chunk)
+    if method == "fcg":
+        return engine_for(n, point_weight, device, slot).solve(rhs, screen, tol, max_cycles)
+    stats = SolveStats()
+    x = torch.empty_like(rhs)
+    nat.check(L.pb_fill_f64(x.data_ptr(), x.numel(), 0.5, s), "fill")
+    h = Hierarchy32(n, device)
+    h.setup(screen, point_weight)
     bnorm = norm(rhs, workspace, torch.empty(1, dtype=torch.float64, device=device))
     norm2 = torch.empty(1, dtype=torch.float64, device=device)
     ws = nat.Workspace(device)
-    ptr, size = ws.get(max(L.pb_defect_workspace_size(n), L.pb_fcg_workspace_size(n)))
+    ptr, size = ws.get(L.pb_defect_workspace_size(n))
     r32 = h.levels[0].rhs
-    r64 = torch.empty_like(rhs) if method == "fcg" else None
     nat.check(L.pb_defect_f64(x.data_ptr(), None, None, rhs.data_ptr(), screen.data_ptr(), n, h.pw, r32.data_ptr(),
-                              None if r64 is None else r64.data_ptr(), norm2.data_ptr(), ptr, size, s), "defect")
+                              None, norm2.data_ptr(), ptr, size, s), "defect")
     stats.rhs_norm = float(bnorm.item())
     target = tol * stats.rhs_norm
     r = math.sqrt(float(norm2.item()))
     stats.history.append(r)
-    if method == "defect":
-        x_next = torch.empty_like(rhs)
-        while r > target and stats.cycles < max_cycles:
-            e = h.v_cycle(0)
-            nat.check(L.pb_defect_f64(x.data_ptr(), e.data_ptr(), x_next.data_ptr(), rhs.data_ptr(),
-                                      screen.data_ptr(), n, h.pw, r32.data_ptr(), None, norm2.data_ptr(), ptr, size,
-                                      s), "defect")
-            x, x_next = x_next, x
-            stats.cycles += 1
-            r = math.sqrt(float(norm2.item()))
-            stats.history.append(r)
-    else:
-        p_prev, p, q = torch.empty_like(rhs), torch.empty_like(rhs), torch.empty_like(rhs)
-        scal = torch.zeros(8, dtype=torch.float64, device=device)
-        while r > target and stats.cycles < max_cycles:
-            z = h.v_cycle(0)
-            nat.check(L.pb_fcg_step_f64(z.data_ptr(), p_prev.data_ptr(), p.data_ptr(), q.data_ptr(), x.data_ptr(),
-                                        r64.data_ptr(), r32.data_ptr(), screen.data_ptr(), n, h.pw,
-                                        scal.data_ptr(), int(stats.cycles == 0), ptr, size, s), "fcg step")
-            p_prev, p = p, p_prev
-            stats.cycles += 1
-            r = math.sqrt(max(float(scal[4].item()), 0.0))
-            stats.history.append(r)
-        # the recurrence r -= alpha q drifts from b - A x by rounding; report the true residual
-        nat.check(L.pb_defect_f64(x.data_ptr(), None, None, rhs.data_ptr(), screen.data_ptr(), n, h.pw,
-                                  r32.data_ptr(), None, norm2.data_ptr(), ptr, size, s), "defect")
+    x_next = torch.empty_like(rhs)
+    while r > target and stats.cycles < max_cycles:
+        e = h.v_cycle(0)
+        nat.check(L.pb_defect_f64(x.data_ptr(), e.data_ptr(), x_next.data_ptr(), rhs.data_ptr(), screen.data_ptr(),
+                                  n, h.pw, r32.data_ptr(), None, norm2.data_ptr(), ptr, size, s), "defect")
+        x, x_next = x_next, x
+        stats.cycles += 1
         r = math.sqrt(float(norm2.item()))
+        stats.history.append(r)
     h.check_status()
     stats.residual_norm = r
     return x, stats
