@@ -57,6 +57,12 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="only the FP32-refined arm (the command the ncu captures run)")
+    ap.add_argument("--workload", choices=("torus", "batch", "serving", "deep"), default="torus",
+                    help="torus: the default line; batch: 256 uneven clouds; serving: Poisson arrivals; "
+                         "deep: depth 10")
+    ap.add_argument("--lanes", type=int, default=4)
+    ap.add_argument("--duration", type=float, default=10.0, help="serving: seconds of arrivals")
+    ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
     return ap.parse_args()
 
 
@@ -391,8 +397,114 @@ def run_reference(args) -> dict:
     }
 
 
+# ---- the other workloads (one JSON line each; not the default line) ---------------
+
+def run_batch(args) -> dict:
+    """256 clouds, sizes log-uniform 1k-200k, depths uniform in {5,6,7,8},
+    random ellipsoids and tori; all submitted at once to a Server."""
+    import torch
+
+    from mojo_poissonrecon_b200 import serve, workloads
+
+    clouds = workloads.batch_clouds(256, seed=3)
+    total_points = sum(len(p) for p, _, _ in clouds)
+    serve.reconstruct_batch(clouds[:8], lanes=args.lanes)  # warm the engines and graphs
+    serve.reconstruct_batch(clouds[:8], lanes=1)
+    results = {}
+    for lanes in (1, args.lanes):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with serve.Server(lanes=lanes) as server:
+            futures = [server.submit(p, n, depth=d) for p, n, d in clouds]
+            out = [f.result() for f in futures]
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        service = [t.service_ms for _, t in out]
+        results[lanes] = {"recons_per_s": round(len(clouds) / wall, 2), "wall_s": round(wall, 3),
+                          "service_p50_ms": round(statistics.median(service), 3),
+                          "service_p99_ms": round(float(np.percentile(service, 99)), 3)}
+    best = results[args.lanes]
+    return {"metric": METRIC, "workload": "batch: 256 uneven clouds (1k-200k points, depths 5-8, ellipsoids/tori)",
+            "value": best["recons_per_s"], "unit": "recons/s", "n_gpus": 1, "precision": "fp32_refined",
+            "tol": TOL, "points_total": total_points, "lanes": args.lanes, "by_lanes": results,
+            "data": "synthetic (workloads.batch_clouds, seed 3)"}
+
+
+def run_serving(args) -> dict:
+    """Poisson arrivals (rate, duration) of requests with log-normal sizes
+    (median 50k, sigma 1, clipped to [1k, 2M]) and depths in {6,7,8,9}.  The
+    clouds of the first 48 requests are generated before the clock starts and
+    request k reuses cloud k mod 48 (with its own depth), so point generation
+    does not stall the arrivals."""
+    import torch
+
+    from mojo_poissonrecon_b200 import serve, workloads
+
+    stream = workloads.serving_stream(rate=args.rate, duration=args.duration, seed=4)
+    pool = [workloads.request_cloud(size, shape, seed) for _, size, _, shape, seed in stream[:48]]
+    with serve.Server(lanes=args.lanes) as server:  # warm-up: one request per depth
+        for d in (6, 7, 8, 9):
+            server.submit(*pool[0], depth=d).result()
+    torch.cuda.synchronize()
+    with serve.Server(lanes=args.lanes) as server:
+        t0 = time.perf_counter()
+        futures = []
+        for k, (arrival, _, depth, _, _) in enumerate(stream):
+            delay = t0 + arrival - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            p, n = pool[k % len(pool)]
+            futures.append((depth, server.submit(p, n, depth=depth)))
+        done = [(d, f.result()) for d, f in futures]
+        wall = time.perf_counter() - t0
+    lat = [t.latency_ms for _, (_, t) in done]
+    by_depth = {}
+    for d in (6, 7, 8, 9):
+        ls = [t.service_ms for dd, (_, t) in done if dd == d]
+        if ls:
+            by_depth[d] = {"count": len(ls), "service_p50_ms": round(statistics.median(ls), 2)}
+    return {"metric": METRIC, "workload": f"serving: Poisson arrivals {args.rate}/s for {args.duration} s, "
+                                          "log-normal sizes (median 50k), depths 6-9",
+            "value": round(len(done) / wall, 2), "unit": "recons/s", "n_gpus": 1, "requests": len(done),
+            "p50_ms": round(statistics.median(lat), 2), "p99_ms": round(float(np.percentile(lat, 99)), 2),
+            "offered_rate": args.rate, "wall_s": round(wall, 2), "lanes": args.lanes, "service_by_depth": by_depth,
+            "precision": "fp32_refined", "tol": TOL, "data": "synthetic (workloads.serving_stream, seed 4)"}
+
+
+def run_deep(args) -> dict:
+    """20,000,000 points on a union of 64 spheres, depth 10 (1025^3)."""
+    import torch
+
+    import mojo_poissonrecon_b200 as mpr
+    from mojo_poissonrecon_b200 import workloads
+
+    pts, nrm = workloads.sphere_union(20_000_000, spheres=64, seed=2)
+    dp, dn = torch.from_numpy(pts).cuda(), torch.from_numpy(nrm).cuda()
+    out = {}
+    for prec in ("fp32_refined", "fp64"):
+        mpr.reconstruct(dp[:200_000], dn[:200_000], depth=10, precision=prec, tol=TOL, device_out=True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        mesh = mpr.reconstruct(dp, dn, depth=10, precision=prec, tol=TOL, device_out=True)
+        e1.record()
+        torch.cuda.synchronize()
+        out[prec] = {"ms": round(e0.elapsed_time(e1), 1), "vertices": int(mesh.vertices.shape[0]),
+                     "faces": int(mesh.faces.shape[0]), "residual_norm": mesh.residual_norm}
+    return {"metric": METRIC, "workload": "deep: 20M points on 64 spheres, depth 10 (1025^3), solve to 1e-8, "
+                                          "dual contour", "value": round(1e3 / out["fp32_refined"]["ms"], 4),
+            "unit": "recons/s", "n_gpus": 1, "fp32_refined": out["fp32_refined"], "fp64": out["fp64"],
+            "peak_memory_gib": round(torch.cuda.max_memory_allocated() / 2**30, 1),
+            "data": "synthetic (workloads.sphere_union, seed 2)"}
+
+
 def main():
     args = parse_args()
+    if args.workload != "torus" and args.impl == "ours":
+        runner = {"batch": run_batch, "serving": run_serving, "deep": run_deep}[args.workload]
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps(runner(args)), flush=True)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":

@@ -28,6 +28,7 @@ from __future__ import annotations
 import collections
 import ctypes
 import math
+import threading
 
 import torch
 
@@ -280,25 +281,48 @@ class RefinedEngine:
 
 
 _ENGINES: "collections.OrderedDict[tuple, RefinedEngine]" = collections.OrderedDict()
-ENGINE_CACHE_SIZE = 3
+_ENGINE_LOCK = threading.Lock()
+ENGINE_CACHE_SIZE = 32
+ENGINE_CACHE_FRACTION = 0.3  # of the device's memory kept in cached engines at most
+_LOCAL = threading.local()
 
 
-def engine_for(n: int, point_weight: float, device: torch.device, slot: int = 0) -> RefinedEngine:
+def current_slot() -> int:
+    """Engine slot of the calling thread (serving lanes set their own)."""
+    return getattr(_LOCAL, "slot", 0)
+
+
+def set_slot(slot: int) -> None:
+    _LOCAL.slot = int(slot)
+
+
+def _cached_bytes() -> int:
+    return sum(e.nbytes() for e in _ENGINES.values())
+
+
+def engine_for(n: int, point_weight: float, device: torch.device, slot: int | None = None) -> RefinedEngine:
     """A cached engine for (device, n, point_weight, slot); least recently used
-    engines are dropped beyond ENGINE_CACHE_SIZE (or when memory runs short)."""
+    engines are dropped beyond ENGINE_CACHE_SIZE entries or ENGINE_CACHE_FRACTION
+    of device memory (and all of them when an allocation runs out of memory).
+    The caller owns the returned engine until its solve returns: one slot per
+    concurrent thread."""
+    slot = current_slot() if slot is None else slot
     key = (device.index, n, float(point_weight), slot)
-    eng = _ENGINES.pop(key, None)
-    if eng is None:
-        while len(_ENGINES) >= ENGINE_CACHE_SIZE:
-            _ENGINES.popitem(last=False)
-        try:
-            eng = RefinedEngine(n, point_weight, device)
-        except torch.cuda.OutOfMemoryError:
-            _ENGINES.clear()
-            torch.cuda.empty_cache()
-            eng = RefinedEngine(n, point_weight, device)
-    _ENGINES[key] = eng
-    return eng
+    with _ENGINE_LOCK:
+        eng = _ENGINES.pop(key, None)
+        if eng is None:
+            budget = ENGINE_CACHE_FRACTION * torch.cuda.get_device_properties(device).total_memory
+            estimate = 96 * n**3
+            while _ENGINES and (len(_ENGINES) >= ENGINE_CACHE_SIZE or _cached_bytes() + estimate > budget):
+                _ENGINES.popitem(last=False)
+            try:
+                eng = RefinedEngine(n, point_weight, device)
+            except torch.cuda.OutOfMemoryError:
+                _ENGINES.clear()
+                torch.cuda.empty_cache()
+                eng = RefinedEngine(n, point_weight, device)
+        _ENGINES[key] = eng
+        return eng
 
 
 def clear_engines() -> None:
@@ -307,7 +331,7 @@ def clear_engines() -> None:
 
 def solve_refined(rhs: torch.Tensor, screen: torch.Tensor, point_weight: float, workspace: nat.Workspace, *,
                   tol: float = 1e-8, max_cycles: int = 200, has_points: bool = True,
-                  method: str = "fcg", slot: int = 0) -> tuple[torch.Tensor, SolveStats]:
+                  method: str = "fcg", slot: int | None = None) -> tuple[torch.Tensor, SolveStats]:
     """FP64-accurate solve with FP32 V-cycles; stats.cycles counts V-cycles.
 
     method="fcg": FCG(1) on a cached RefinedEngine (graph-driven loop).
