@@ -182,9 +182,11 @@ int pb_dual_faces_f64_isoptr(const double *field, int64_t n, const double *iso,
  *   index(x, y, z) = ((z+1)*(n+2) + (y+1))*P + (x+4),   x, y, z in [-1, n].
  * Callers allocate them zero-filled; kernels write interior nodes only. */
 int pb_level_geometry(int64_t n, int64_t *pitch, int64_t *padded_count);
-/* D = (degree + pw*screen)*(n-1)^2 and 1/D per node from the dense FP64 screen. */
+/* D = (degree + pw*screen)*(n-1)^2 and 1/D per node from the dense FP64 screen;
+ * weights (may be NULL): the prolongation weights s of the FP32 cycle, 1 on
+ * nodes of the coarse grid, else degree*(n-1)^2 / D. */
 int pb_level_setup_f32(const double *screen, int64_t n, double point_weight, float *D, float *invD,
-                       void *stream);
+                       float *weights, void *stream);
 /* r32 = b - A x in FP64 (dense x, b, screen; r32 padded), *norm2 = ||b - A x||^2,
  * and the FP64 residual into r64 when it is not NULL.  With e != NULL the
  * iterate is first updated: x_new = x_old + e (written). */
@@ -208,8 +210,11 @@ int pb_fcg_step_f64(const float *z, const double *p_prev, double *p, double *q, 
  * sets *status (device int) to 1. */
 int pb_sweep_tma_f32(const float *e_in, float *e_out, const float *rhs, const float *invD, int64_t n,
                      int64_t mode, int64_t z_chunk, int *status, void *stream);
-/* fine += trilinear prolongation of coarse (side (n+1)/2), padded layouts. */
-int pb_prolong_add_f32(const float *coarse, float *fine, int64_t fine_n, void *stream);
+/* fine += s * trilinear(coarse) (coarse side (n+1)/2), padded layouts, s the
+ * prolongation weights of the fine level (pb_level_setup_f32 for level 0,
+ * pb_level27_finish_f32 below).  Replaces mpr_prolong_add_f64
+ * (capi.mojo:677-742) inside the FP32 cycle. */
+int pb_prolong_fac_f32(const float *coarse, float *fine, const float *weights, int64_t fine_n, void *stream);
 /* Graph-friendly FCG(1) step: p = z - beta p in place (p = z while flags[0]
  * != 0), q = A p, alpha, x += alpha p, r -= alpha q, r32 = (float) r;
  * scal[0..4] as for pb_fcg_step_f64.  Touches the same buffers every call, so
@@ -236,16 +241,45 @@ int pb_graph_destroy(void *exec, void *graph);
 /* Adds launches that ran inside graphs to pb_launch_count(). */
 int pb_note_launches(long long count);
 
-/* coarse_rhs (side (n+1)/2) = full-weighting restriction of rhs - A e (side
- * n), in FP32 on the padded layout, without writing the fine residual. */
-int pb_residual_restrict_f32(const float *e, const float *rhs, const float *D, float *coarse_rhs,
-                             int64_t n, void *stream);
-/* The V-cycle below a level of side <= 17 in one block: count levels, finest
- * first (host arrays of device pointers); rhs[0] holds the right-hand side,
- * e[0] receives the correction. */
-int pb_coarse_cycle_f32(int64_t count, const int64_t *sizes, float *const *e, float *const *rhs,
-                        float *const *res, const float *const *D, const float *const *invD,
-                        int64_t pre, int64_t post, int64_t coarsest_sweeps, void *stream);
+/* ---- FP32 preconditioner levels (no counterpart in the reference) ----------
+ * The reference's V-cycle (core.py:141-193) rediscretises coarse levels; the
+ * FP32 preconditioner of the refined solvers uses Galerkin coarse levels
+ * A_c = P_s^T A P_s / 8 with the screening-scaled prolongation P_s = S P.
+ * 27-point levels store 14 planes (plane stride = padded count of the level):
+ * the diagonal, then the couplings to the 13 forward neighbours. */
+
+/* Level 0: coarse_rhs (side (n+1)/2) = P^T (s (rhs - A e)) / 8 with A the
+ * reference's operator (diagonal D) and s its weights, without writing the
+ * fine residual. */
+int pb_residual_restrict_f32(const float *e, const float *rhs, const float *D, const float *weights,
+                             float *coarse_rhs, int64_t n, void *stream);
+/* 14 planes of the Galerkin operator of the level below a level of side
+ * fine_n with prolongation weights fine_weights: from level 0 (fine_is_7pt
+ * != 0, `fine` = D) or from 14 planes. */
+int pb_galerkin_f32(const float *fine, int64_t fine_n, int fine_is_7pt, const float *fine_weights,
+                    float *coarse, void *stream);
+/* 14 planes of a 7-point level (diagonal D, off-diagonals -(n-1)^2). */
+int pb_level27_from7_f32(const float *D, int64_t n, float *coef, void *stream);
+/* invD = 1 / diagonal and the prolongation weights of a 27-point level. */
+int pb_level27_finish_f32(const float *coef, int64_t n, float *invD, float *weights, void *stream);
+/* One red-black ordered sweep e_next <- S(e_prev) on a 27-point level, the
+ * same-colour couplings from e_prev (e_prev NULL: from zero). */
+int pb_relax27_f32(const float *e_prev, float *e_next, const float *rhs, const float *coef,
+                   const float *invD, int64_t n, void *stream);
+/* res = weights * (rhs - A e) on a 27-point level, then coarse_rhs = P^T res / 8. */
+int pb_residual_restrict27_f32(const float *e, const float *rhs, const float *coef, const float *weights,
+                               int64_t n, float *res, float *coarse_rhs, void *stream);
+/* Inverse (27 x 27, FP32 row-major) of the 27-point level of side 3. */
+int pb_coarse_inverse_f32(const float *coef, int64_t n, float *inverse, void *stream);
+/* The V-cycle below a 27-point level of side <= 17 in one block: count
+ * levels, finest first, the last of side 3 and solved with `inverse` (host
+ * arrays of device pointers); (pre, post) sweeps on the first level, `inner`
+ * each way on the others; rhs[0] holds the right-hand side, e[0] receives the
+ * correction. */
+int pb_coarse27_cycle_f32(int64_t count, const int64_t *sizes, const float *const *coef,
+                          const float *const *invD, const float *const *weights, float *const *e,
+                          float *const *rhs, float *const *res, int64_t pre, int64_t post, int64_t inner,
+                          const float *inverse, void *stream);
 
 /* ---- host-orchestration helpers (core.py steps done on the device) ---------- */
 

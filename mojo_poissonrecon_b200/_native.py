@@ -56,7 +56,7 @@ _SIGNATURES = {
     "pb_unit_cube_check_f64": ([P, I, P, P], C),
     "pb_map_vertices_f64": ([P, I, P, P], C),
     "pb_level_geometry": ([I, P, P], C),
-    "pb_level_setup_f32": ([P, I, F, P, P, P], C),
+    "pb_level_setup_f32": ([P, I, F, P, P, P, P], C),
     "pb_defect_workspace_size": ([I], S),
     "pb_defect_f64": ([P, P, P, P, P, I, F, P, P, P, P, S, P], C),
     "pb_fcg_workspace_size": ([I], S),
@@ -69,9 +69,15 @@ _SIGNATURES = {
     "pb_graph_destroy": ([P, P], C),
     "pb_note_launches": ([ctypes.c_longlong], C),
     "pb_sweep_tma_f32": ([P, P, P, P, I, I, I, P, P], C),
-    "pb_prolong_add_f32": ([P, P, I, P], C),
-    "pb_residual_restrict_f32": ([P, P, P, P, I, P], C),
-    "pb_coarse_cycle_f32": ([I, P, P, P, P, P, P, I, I, I, P], C),
+    "pb_prolong_fac_f32": ([P, P, P, I, P], C),
+    "pb_residual_restrict_f32": ([P, P, P, P, P, I, P], C),
+    "pb_galerkin_f32": ([P, I, C, P, P, P], C),
+    "pb_level27_from7_f32": ([P, I, P, P], C),
+    "pb_level27_finish_f32": ([P, I, P, P, P], C),
+    "pb_relax27_f32": ([P, P, P, P, P, I, P], C),
+    "pb_residual_restrict27_f32": ([P, P, P, P, I, P, P, P], C),
+    "pb_coarse_inverse_f32": ([P, I, P, P], C),
+    "pb_coarse27_cycle_f32": ([I, P, P, P, P, P, P, P, I, I, I, P, P], C),
 }
 
 LIBRARY_PATH = _build.LIBRARY

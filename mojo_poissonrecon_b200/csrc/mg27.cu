@@ -1,0 +1,562 @@
+// Galerkin coarse levels of the FP32 preconditioner.
+//
+// The reference's coarse levels rediscretise the operator (screen restricted
+// and scaled by 4 per level, python/mojo_poissonrecon/core.py:267-269) and
+// transfer with trilinear prolongation and boundary-normalised full weighting
+// (src/capi.mojo:557-742).  The screening term pw*screen is concentrated on a
+// thin shell of nodes around the samples, where it outweighs the Laplacian by
+// one to two orders of magnitude; across that shell a trilinear coarse
+// correction is wrong by O(1), and the reference-shaped cycle reduces the
+// residual by only about 0.35 per cycle even with an exact coarse solve.  The
+// FP32 preconditioner keeps the reference's fine operator and red-black
+// smoother on level 0 and replaces the coarse side:
+//   prolongation  P_s = S P, P trilinear, S = diag(s) with s_i = 1 where the
+//                 fine node coincides with a coarse node, else
+//                 s_i = (sum_{j != i} -a_ij) / a_ii  (deg / (deg + pw*screen)
+//                 on level 0): a correction is damped where screening
+//                 dominates the row;
+//   restriction   R = P_s^T / 8 (full weighting scaled by s, not renormalised);
+//   coarse ops    A_c = R A P_s (Galerkin), 27-point and symmetric;
+//   coarsest      the 3^3 level solved exactly with its inverse.
+// That cycle reduces the residual by about 0.03-0.05 per cycle independent of
+// depth.  The FP64 outer loop still measures convergence with the reference's
+// operator, so the answer is the reference's to the requested tolerance.
+//
+// Smoothing on 27-point levels: red-black ordered, same-colour couplings
+// taken from the previous iterate (two passes per sweep, e_prev -> e_next,
+// no in-place race).
+//
+// Storage of a 27-point level: 14 coefficient planes in the padded layout
+// (level32.cuh), plane stride = padded_size(n); plane 0 the diagonal, planes
+// 1..13 the couplings to the 13 "forward" neighbours J+K (K.z > 0; or K.z == 0
+// and K.y > 0; or K = (1,0,0)).  The coupling to a backward neighbour J-K is
+// plane k(K) at J-K (symmetry).  Ghost entries are zero.
+#include "common.cuh"
+#include "level32.cuh"
+
+namespace pb {
+
+__host__ __device__ constexpr bool is_forward(int dx, int dy, int dz) {
+    return dz > 0 || (dz == 0 && (dy > 0 || (dy == 0 && dx > 0)));
+}
+__host__ __device__ constexpr int fwd_index(int dx, int dy, int dz) {
+    return dz == 1 ? 1 + (dy + 1) * 3 + (dx + 1) : (dy == 1 ? 10 + (dx + 1) : 13);
+}
+__host__ __device__ constexpr float wt(int d) { return d == 0 ? 1.0f : 0.5f; }
+
+__device__ __forceinline__ int64_t offset_of(const Geom& g, int dx, int dy, int dz) {
+    return (int64_t)dx + (int64_t)dy * g.P + (int64_t)dz * g.plane;
+}
+
+// a(J, J+K) for the node at padded index p.
+__device__ __forceinline__ float coupling(const float* __restrict__ c, int64_t cs, const Geom& g, int64_t p, int dx,
+                                          int dy, int dz) {
+    if (dx == 0 && dy == 0 && dz == 0) return c[p];
+    if (is_forward(dx, dy, dz)) return c[fwd_index(dx, dy, dz) * cs + p];
+    return c[fwd_index(-dx, -dy, -dz) * cs + p + offset_of(g, dx, dy, dz)];
+}
+
+__device__ __forceinline__ bool inside(int x, int y, int z, int n) {
+    return (unsigned)x < (unsigned)n && (unsigned)y < (unsigned)n && (unsigned)z < (unsigned)n;
+}
+
+// ---- Galerkin product A_c = P_s^T A P_s / 8 -----------------------------------
+// One thread per coarse node J streams once over the fine nodes i = 2J + o of
+// J's support (27) and their stencil neighbours j = i + K (7 on level 0, 27
+// below), and scatters the product p_iJ a_ij s_j into the stored entries
+// A_c[J, J+m] (m = 0 or forward) whose column support holds j, with weight
+// P(d - 2m), d = o + K.  Every index and weight is resolved at compile time,
+// so the 14 sums stay in registers.
+__device__ __forceinline__ void scatter14(float v, int dx, int dy, int dz, float* acc) {
+#pragma unroll
+    for (int mz = -1; mz <= 1; ++mz)
+#pragma unroll
+        for (int my = -1; my <= 1; ++my)
+#pragma unroll
+            for (int mx = -1; mx <= 1; ++mx) {
+                const int ex = dx - 2 * mx, ey = dy - 2 * my, ez = dz - 2 * mz;
+                if (ex < -1 || ex > 1 || ey < -1 || ey > 1 || ez < -1 || ez > 1) continue;
+                const bool centre = mx == 0 && my == 0 && mz == 0;
+                if (!centre && !is_forward(mx, my, mz)) continue;
+                acc[centre ? 0 : fwd_index(mx, my, mz)] += v * (wt(ex) * wt(ey) * wt(ez));
+            }
+}
+
+// FINE7: `fc` is the level-0 diagonal D (couplings -h2 to in-grid face
+// neighbours); otherwise `fc` holds the fine level's 14 planes.  S: the fine
+// level's prolongation weights.
+template <bool FINE7>
+__global__ void __launch_bounds__(128) galerkin_kernel(const float* __restrict__ fc, int64_t fs,
+                                                       const float* __restrict__ S, Geom gf, float h2,
+                                                       float* __restrict__ cc, int64_t cs, Geom gc) {
+    const int xc = blockIdx.x * blockDim.x + threadIdx.x, yc = blockIdx.y * blockDim.y + threadIdx.y;
+    const int zc = blockIdx.z;
+    const int cn = gc.n, fn = gf.n;
+    if (xc >= cn || yc >= cn) return;
+    // every i and j of J inside the fine grid
+    const bool interior = xc >= 1 && yc >= 1 && zc >= 1 && xc <= cn - 2 && yc <= cn - 2 && zc <= cn - 2;
+    float acc[14];
+#pragma unroll
+    for (int k = 0; k < 14; ++k) acc[k] = 0.0f;
+#pragma unroll
+    for (int oz = -1; oz <= 1; ++oz)
+#pragma unroll
+        for (int oy = -1; oy <= 1; ++oy)
+#pragma unroll
+            for (int ox = -1; ox <= 1; ++ox) {
+                const int xi = 2 * xc + ox, yi = 2 * yc + oy, zi = 2 * zc + oz;
+                if (!interior && !inside(xi, yi, zi, fn)) continue;
+                const int64_t pi = gf.at(xi, yi, zi);
+                const float si = wt(ox) * wt(oy) * wt(oz) * S[pi];
+#pragma unroll
+                for (int kz = -1; kz <= 1; ++kz)
+#pragma unroll
+                    for (int ky = -1; ky <= 1; ++ky)
+#pragma unroll
+                        for (int kx = -1; kx <= 1; ++kx) {
+                            if (FINE7 && (kx != 0) + (ky != 0) + (kz != 0) > 1) continue;
+                            if (!interior && !inside(xi + kx, yi + ky, zi + kz, fn)) continue;
+                            float a;
+                            if (kx == 0 && ky == 0 && kz == 0)
+                                a = fc[pi];
+                            else if (FINE7)
+                                a = -h2;
+                            else
+                                a = coupling(fc, fs, gf, pi, kx, ky, kz);
+                            scatter14(si * a * S[pi + offset_of(gf, kx, ky, kz)], ox + kx, oy + ky, oz + kz, acc);
+                        }
+            }
+    const int64_t p = gc.at(xc, yc, zc);
+    cc[p] = acc[0] * 0.125f;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx)
+                if (is_forward(dx, dy, dz)) {
+                    const int k = fwd_index(dx, dy, dz);
+                    cc[k * cs + p] = inside(xc + dx, yc + dy, zc + dz, cn) ? acc[k] * 0.125f : 0.0f;
+                }
+}
+
+// A 7-point level (diagonal D, off-diagonals -h2 inside the grid) as 14 planes.
+__global__ void level7_to_27_kernel(const float* __restrict__ D, Geom g, float h2, float* __restrict__ c, int64_t cs) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    const int n = g.n;
+    if (x >= n || y >= n) return;
+    const int64_t p = g.at(x, y, z);
+    c[p] = D[p];
+#pragma unroll
+    for (int k = 1; k <= 13; ++k) c[k * cs + p] = 0.0f;
+    c[fwd_index(1, 0, 0) * cs + p] = x + 1 < n ? -h2 : 0.0f;
+    c[fwd_index(0, 1, 0) * cs + p] = y + 1 < n ? -h2 : 0.0f;
+    c[fwd_index(0, 0, 1) * cs + p] = z + 1 < n ? -h2 : 0.0f;
+}
+
+// 1/a_JJ and the prolongation weight s_J of a 27-point level.
+__global__ void level27_finish_kernel(const float* __restrict__ c, int64_t cs, Geom g, float* __restrict__ invD,
+                                      float* __restrict__ fac) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    const int n = g.n;
+    if (x >= n || y >= n) return;
+    const int64_t p = g.at(x, y, z);
+    float off = 0.0f;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx)
+                if (dx || dy || dz) off -= coupling(c, cs, g, p, dx, dy, dz);
+    const float d = c[p];
+    invD[p] = 1.0f / d;
+    float s = 1.0f;
+    if ((x | y | z) & 1) s = fminf(fmaxf(off / d, 0.0f), 1.0f);
+    fac[p] = s;
+}
+
+// ---- 27-point smoothing, residual, transfers ------------------------------------
+// One colour pass: nodes of colour COLOUR get (rhs - sum_{K != 0} a e) / a_JJ,
+// neighbours of the other colour read from `next` when COLOUR == 1 (updated in
+// pass 0), everything else from `prev` (zero when ZERO).
+template <int COLOUR, bool ZERO>
+__global__ void __launch_bounds__(256) relax27_kernel(const float* __restrict__ prev, float* next,
+                                                      const float* __restrict__ rhs, const float* __restrict__ c,
+                                                      int64_t cs, const float* __restrict__ invD, Geom g) {
+    const int y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    const int x = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((y + z + COLOUR) & 1);
+    const int n = g.n;
+    if (x >= n || y >= n) return;
+    const int64_t p = g.at(x, y, z);
+    float s = 0.0f;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx) {
+                if (!(dx || dy || dz)) continue;
+                const bool other = ((dx + dy + dz) & 1) != 0;  // neighbour of the other colour
+                if (ZERO && !(COLOUR == 1 && other)) continue;
+                const int64_t q = p + offset_of(g, dx, dy, dz);
+                const float v = (COLOUR == 1 && other) ? next[q] : prev[q];
+                s += coupling(c, cs, g, p, dx, dy, dz) * v;
+            }
+    next[p] = (rhs[p] - s) * invD[p];
+}
+
+// res = s (rhs - A e) on the grid (ghosts untouched, zero).
+__global__ void __launch_bounds__(256) residual27_kernel(const float* __restrict__ e, const float* __restrict__ rhs,
+                                                         const float* __restrict__ c, int64_t cs,
+                                                         const float* __restrict__ fac, Geom g,
+                                                         float* __restrict__ res) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    const int n = g.n;
+    if (x >= n || y >= n) return;
+    const int64_t p = g.at(x, y, z);
+    float s = 0.0f;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx) s += coupling(c, cs, g, p, dx, dy, dz) * e[p + offset_of(g, dx, dy, dz)];
+    res[p] = fac[p] * (rhs[p] - s);
+}
+
+// coarse[J] = sum_o w(o)/64 res[2J+o], w = prod (2 on the axis, 1 off it);
+// out-of-grid fine nodes are ghosts holding zero.
+__global__ void __launch_bounds__(256) restrict27_kernel(const float* __restrict__ res, Geom gf,
+                                                         float* __restrict__ coarse, Geom gc) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    if (x >= gc.n || y >= gc.n) return;
+    const int64_t p = gf.at(2 * x, 2 * y, 2 * z);
+    float s = 0.0f;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx)
+                s += res[p + offset_of(gf, dx, dy, dz)] * (float)((dx ? 1 : 2) * (dy ? 1 : 2) * (dz ? 1 : 2));
+    coarse[gc.at(x, y, z)] = s * (1.0f / 64.0f);
+}
+
+// ---- exact solve on the 3^3 level -----------------------------------------------
+// The 27 x 27 operator of the coarsest level inverted once per set-up by one
+// warp: FP64 Gauss-Jordan without pivoting (the Galerkin operator is
+// symmetric positive definite), lane i owning row i; stored FP32 row-major.
+constexpr int kInvN = 27;
+
+__global__ void __launch_bounds__(32) coarse_inverse_kernel(const float* __restrict__ c, int64_t cs, Geom g,
+                                                            float* __restrict__ inv) {
+    __shared__ double a[kInvN][kInvN + 1];
+    const int lane = threadIdx.x;
+    if (lane < kInvN) {
+        const int x = lane % 3, y = (lane / 3) % 3, z = lane / 9;
+        const int64_t p = g.at(x, y, z);
+        for (int j = 0; j < kInvN; ++j) a[lane][j] = 0.0;
+#pragma unroll
+        for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+            for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+                for (int dx = -1; dx <= 1; ++dx)
+                    if (inside(x + dx, y + dy, z + dz, 3))
+                        a[lane][lane + dx + 3 * dy + 9 * dz] = (double)coupling(c, cs, g, p, dx, dy, dz);
+    }
+    __syncwarp();
+    for (int k = 0; k < kInvN; ++k) {
+        const double piv = a[k][k];
+        __syncwarp();
+        if (lane == k) {
+            a[k][k] = 1.0;
+            for (int j = 0; j < kInvN; ++j) a[k][j] /= piv;
+        }
+        __syncwarp();
+        if (lane < kInvN && lane != k) {
+            const double f = a[lane][k];
+            a[lane][k] = 0.0;
+            for (int j = 0; j < kInvN; ++j) a[lane][j] -= f * a[k][j];
+        }
+        __syncwarp();
+    }
+    if (lane < kInvN)
+        for (int j = 0; j < kInvN; ++j) inv[lane * kInvN + j] = (float)a[lane][j];
+}
+
+// ---- levels with n <= kC27N in one block ----------------------------------------
+constexpr int kC27N = 17;
+constexpr int kC27Threads = 1024;
+constexpr int kC27PerThread = (kC27N * kC27N * kC27N + kC27Threads - 1) / kC27Threads;
+constexpr int kC27MaxLevels = 8;
+
+struct Coarse27 {
+    int count;
+    Geom g[kC27MaxLevels];
+    int64_t cs[kC27MaxLevels];
+    const float* c[kC27MaxLevels];
+    const float* invD[kC27MaxLevels];
+    const float* fac[kC27MaxLevels];
+    float* e[kC27MaxLevels];
+    float* rhs[kC27MaxLevels];
+    float* res[kC27MaxLevels];
+    const float* inverse;  // of the last level (side 3)
+};
+
+__device__ __forceinline__ void unflatten(int i, int n, int& x, int& y, int& z) {
+    x = i % n;
+    y = (i / n) % n;
+    z = i / (n * n);
+}
+
+__device__ float stencil27(const float* __restrict__ c, int64_t cs, const Geom& g, int64_t p, const float* e,
+                           bool skip_centre) {
+    float s = 0.0f;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx) {
+                if (skip_centre && !(dx || dy || dz)) continue;
+                s += coupling(c, cs, g, p, dx, dy, dz) * e[p + offset_of(g, dx, dy, dz)];
+            }
+    return s;
+}
+
+// Red-black ordered sweeps in place: each colour's new values are staged in
+// registers and written after a barrier, so same-colour neighbours are read
+// from the previous iterate, as relax27_kernel does.
+__device__ void c27_relax(const Coarse27& L, int l, int iters) {
+    const Geom g = L.g[l];
+    const int n = g.n, total = n * n * n;
+    float* e = L.e[l];
+    for (int it = 0; it < iters; ++it)
+        for (int colour = 0; colour < 2; ++colour) {
+            float v[kC27PerThread];
+#pragma unroll
+            for (int k = 0; k < kC27PerThread; ++k) {
+                const int i = threadIdx.x + k * kC27Threads;
+                v[k] = 0.0f;
+                if (i < total) {
+                    int x, y, z;
+                    unflatten(i, n, x, y, z);
+                    if (((x + y + z) & 1) == colour) {
+                        const int64_t p = g.at(x, y, z);
+                        v[k] = (L.rhs[l][p] - stencil27(L.c[l], L.cs[l], g, p, e, true)) * L.invD[l][p];
+                    }
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < kC27PerThread; ++k) {
+                const int i = threadIdx.x + k * kC27Threads;
+                if (i < total) {
+                    int x, y, z;
+                    unflatten(i, n, x, y, z);
+                    if (((x + y + z) & 1) == colour) e[g.at(x, y, z)] = v[k];
+                }
+            }
+            __syncthreads();
+        }
+}
+
+__global__ void __launch_bounds__(kC27Threads) coarse27_kernel(Coarse27 L, int pre, int post, int inner) {
+    for (int l = 0; l < L.count; ++l) {
+        const Geom g = L.g[l];
+        const int n = g.n, total = n * n * n;
+        if (l == L.count - 1) {  // side 3: e = A^-1 rhs
+            if (threadIdx.x < kInvN) {
+                float v = 0.0f;
+                for (int j = 0; j < kInvN; ++j)
+                    v += L.inverse[threadIdx.x * kInvN + j] * L.rhs[l][g.at(j % 3, (j / 3) % 3, j / 9)];
+                const int t = threadIdx.x;
+                L.e[l][g.at(t % 3, (t / 3) % 3, t / 9)] = v;
+            }
+            __syncthreads();
+            break;
+        }
+        for (int i = threadIdx.x; i < total; i += blockDim.x) {
+            int x, y, z;
+            unflatten(i, n, x, y, z);
+            L.e[l][g.at(x, y, z)] = 0.0f;
+        }
+        __syncthreads();
+        c27_relax(L, l, l == 0 ? pre : inner);
+        for (int i = threadIdx.x; i < total; i += blockDim.x) {
+            int x, y, z;
+            unflatten(i, n, x, y, z);
+            const int64_t p = g.at(x, y, z);
+            L.res[l][p] = L.fac[l][p] * (L.rhs[l][p] - stencil27(L.c[l], L.cs[l], g, p, L.e[l], false));
+        }
+        __syncthreads();
+        const Geom gc = L.g[l + 1];
+        const int cn = gc.n;
+        for (int i = threadIdx.x; i < cn * cn * cn; i += blockDim.x) {
+            int x, y, z;
+            unflatten(i, cn, x, y, z);
+            const int64_t p = g.at(2 * x, 2 * y, 2 * z);
+            float s = 0.0f;
+            for (int dz = -1; dz <= 1; ++dz)
+                for (int dy = -1; dy <= 1; ++dy)
+                    for (int dx = -1; dx <= 1; ++dx)
+                        s += L.res[l][p + offset_of(g, dx, dy, dz)] *
+                             (float)((dx ? 1 : 2) * (dy ? 1 : 2) * (dz ? 1 : 2));
+            L.rhs[l + 1][gc.at(x, y, z)] = s * (1.0f / 64.0f);
+        }
+        __syncthreads();
+    }
+    for (int l = L.count - 2; l >= 0; --l) {
+        const Geom g = L.g[l], gc = L.g[l + 1];
+        const int n = g.n, total = n * n * n;
+        const float* ec = L.e[l + 1];
+        for (int i = threadIdx.x; i < total; i += blockDim.x) {
+            int x, y, z;
+            unflatten(i, n, x, y, z);
+            // trilinear: the mean of the 8 corners, a corner repeated on even axes
+            const int x0 = x >> 1, y0 = y >> 1, z0 = z >> 1;
+            const int x1 = x0 + (x & 1), y1 = y0 + (y & 1), z1 = z0 + (z & 1);
+            const float v = 0.125f * (ec[gc.at(x0, y0, z0)] + ec[gc.at(x1, y0, z0)] + ec[gc.at(x0, y1, z0)] +
+                                      ec[gc.at(x1, y1, z0)] + ec[gc.at(x0, y0, z1)] + ec[gc.at(x1, y0, z1)] +
+                                      ec[gc.at(x0, y1, z1)] + ec[gc.at(x1, y1, z1)]);
+            const int64_t p = g.at(x, y, z);
+            L.e[l][p] += L.fac[l][p] * v;
+        }
+        __syncthreads();
+        c27_relax(L, l, l == 0 ? post : inner);
+    }
+}
+
+inline dim3 node_grid(int n, dim3 block) { return dim3((n + block.x - 1) / block.x, (n + block.y - 1) / block.y, n); }
+
+}  // namespace pb
+
+using namespace pb;
+
+static bool level_side_ok(int64_t n) { return n >= 3 && n <= 4097 && ((n - 1) & (n - 2)) == 0; }
+
+// Coarse 27-point operator (14 planes, plane stride padded_size(cn)) of the
+// level below a fine level of side fine_n with prolongation weights
+// fine_weights.  fine_is_7pt: `fine` is the level-0 diagonal D (couplings
+// -(n-1)^2); otherwise `fine` holds 14 planes.
+extern "C" int pb_galerkin_f32(const float* fine, int64_t fine_n, int fine_is_7pt, const float* fine_weights,
+                               float* coarse, void* stream) {
+    if (!level_side_ok(fine_n) || !fine || !coarse || !fine_weights) return fail(PB_ERR_INVALID, "galerkin: bad args");
+    const int fn = (int)fine_n, cn = (fn + 1) / 2;
+    const Geom gf = geom(fn), gc = geom(cn);
+    const float h2 = (float)(fn - 1) * (float)(fn - 1);
+    const dim3 block(32, 4);
+    if (fine_is_7pt)
+        galerkin_kernel<true><<<node_grid(cn, block), block, 0, (cudaStream_t)stream>>>(
+            fine, 0, fine_weights, gf, h2, coarse, padded_size(cn), gc);
+    else
+        galerkin_kernel<false><<<node_grid(cn, block), block, 0, (cudaStream_t)stream>>>(
+            fine, padded_size(fn), fine_weights, gf, h2, coarse, padded_size(cn), gc);
+    PB_CHECK_LAUNCH("galerkin_kernel");
+    return PB_OK;
+}
+
+// 14 planes of a 7-point level (diagonal D, off-diagonals -(n-1)^2).
+extern "C" int pb_level27_from7_f32(const float* D, int64_t n, float* coef, void* stream) {
+    if (!level_side_ok(n) || !D || !coef) return fail(PB_ERR_INVALID, "level27 from 7: bad args");
+    const dim3 block(32, 4);
+    level7_to_27_kernel<<<node_grid((int)n, block), block, 0, (cudaStream_t)stream>>>(
+        D, geom((int)n), (float)(n - 1) * (float)(n - 1), coef, padded_size((int)n));
+    PB_CHECK_LAUNCH("level7_to_27_kernel");
+    return PB_OK;
+}
+
+// invD = 1 / diagonal and the prolongation weights of a 27-point level.
+extern "C" int pb_level27_finish_f32(const float* coef, int64_t n, float* invD, float* weights, void* stream) {
+    if (!level_side_ok(n) || !coef || !invD || !weights) return fail(PB_ERR_INVALID, "level27 finish: bad args");
+    const dim3 block(32, 4);
+    level27_finish_kernel<<<node_grid((int)n, block), block, 0, (cudaStream_t)stream>>>(
+        coef, padded_size((int)n), geom((int)n), invD, weights);
+    PB_CHECK_LAUNCH("level27_finish_kernel");
+    return PB_OK;
+}
+
+// One red-black sweep e_next <- S(e_prev) on a 27-point level (e_prev null:
+// from zero).  e_next must not alias e_prev.
+extern "C" int pb_relax27_f32(const float* e_prev, float* e_next, const float* rhs, const float* coef,
+                              const float* invD, int64_t n, void* stream) {
+    if (!level_side_ok(n) || !e_next || !rhs || !coef || !invD || e_prev == e_next)
+        return fail(PB_ERR_INVALID, "relax27: bad args");
+    cudaStream_t s = (cudaStream_t)stream;
+    const Geom g = geom((int)n);
+    const int64_t cs = padded_size((int)n);
+    const dim3 block(32, 8);
+    const dim3 grid(((int)(n + 1) / 2 + 31) / 32, ((int)n + 7) / 8, (int)n);
+    if (e_prev) {
+        relax27_kernel<0, false><<<grid, block, 0, s>>>(e_prev, e_next, rhs, coef, cs, invD, g);
+        PB_CHECK_LAUNCH("relax27_kernel");
+        relax27_kernel<1, false><<<grid, block, 0, s>>>(e_prev, e_next, rhs, coef, cs, invD, g);
+    } else {
+        relax27_kernel<0, true><<<grid, block, 0, s>>>(nullptr, e_next, rhs, coef, cs, invD, g);
+        PB_CHECK_LAUNCH("relax27_kernel");
+        relax27_kernel<1, true><<<grid, block, 0, s>>>(nullptr, e_next, rhs, coef, cs, invD, g);
+    }
+    PB_CHECK_LAUNCH("relax27_kernel");
+    return PB_OK;
+}
+
+// res = weights * (rhs - A e), then coarse_rhs = P^T res / 8 on the next level.
+extern "C" int pb_residual_restrict27_f32(const float* e, const float* rhs, const float* coef, const float* weights,
+                                          int64_t n, float* res, float* coarse_rhs, void* stream) {
+    if (!level_side_ok(n) || n < 5 || !e || !rhs || !coef || !weights || !res || !coarse_rhs)
+        return fail(PB_ERR_INVALID, "residual_restrict27: bad args");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int fn = (int)n, cn = (fn + 1) / 2;
+    const dim3 block(32, 8);
+    residual27_kernel<<<node_grid(fn, block), block, 0, s>>>(e, rhs, coef, padded_size(fn), weights, geom(fn), res);
+    PB_CHECK_LAUNCH("residual27_kernel");
+    restrict27_kernel<<<node_grid(cn, block), block, 0, s>>>(res, geom(fn), coarse_rhs, geom(cn));
+    PB_CHECK_LAUNCH("restrict27_kernel");
+    return PB_OK;
+}
+
+// Inverse (27 x 27, FP32 row-major) of a 27-point level of side 3.
+extern "C" int pb_coarse_inverse_f32(const float* coef, int64_t n, float* inverse, void* stream) {
+    if (n != 3 || !coef || !inverse) return fail(PB_ERR_INVALID, "coarse inverse: side must be 3");
+    coarse_inverse_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(coef, padded_size(3), geom(3), inverse);
+    PB_CHECK_LAUNCH("coarse_inverse_kernel");
+    return PB_OK;
+}
+
+// Levels with side <= 17 in one block (27-point operators, V(pre, post) on the
+// first of them and `inner` sweeps each way on the others, the last level, of
+// side 3, solved with its inverse from pb_coarse_inverse_f32).  Arrays per
+// level, finest first; rhs[0] holds the restricted residual from above; e[0]
+// receives the correction.
+extern "C" int pb_coarse27_cycle_f32(int64_t count, const int64_t* sizes, const float* const* coef,
+                                     const float* const* invD, const float* const* weights, float* const* e,
+                                     float* const* rhs, float* const* res, int64_t pre, int64_t post,
+                                     int64_t inner, const float* inverse, void* stream) {
+    if (count < 1 || count > kC27MaxLevels || !sizes || !coef || !invD || !weights || !e || !rhs || !res || !inverse)
+        return fail(PB_ERR_INVALID, "coarse27 cycle: bad args");
+    if (pre < 0 || post < 0 || inner < 0 || pre > 64 || post > 64 || inner > 64)
+        return fail(PB_ERR_INVALID, "coarse27 cycle: sweep counts must be in [0, 64]");
+    Coarse27 L;
+    L.count = (int)count;
+    L.inverse = inverse;
+    for (int l = 0; l < count; ++l) {
+        if (!level_side_ok(sizes[l]) || sizes[l] > kC27N || (l && sizes[l] != (sizes[l - 1] + 1) / 2))
+            return fail(PB_ERR_INVALID, "coarse27 cycle: bad level sizes");
+        if (!coef[l] || !invD[l] || !weights[l] || !e[l] || !rhs[l] || !res[l])
+            return fail(PB_ERR_INVALID, "coarse27 cycle: null level array");
+        L.g[l] = geom((int)sizes[l]);
+        L.cs[l] = padded_size((int)sizes[l]);
+        L.c[l] = coef[l];
+        L.invD[l] = invD[l];
+        L.fac[l] = weights[l];
+        L.e[l] = e[l];
+        L.rhs[l] = rhs[l];
+        L.res[l] = res[l];
+    }
+    if (sizes[count - 1] != 3) return fail(PB_ERR_INVALID, "coarse27 cycle: the last level must have side 3");
+    coarse27_kernel<<<1, kC27Threads, 0, (cudaStream_t)stream>>>(L, (int)pre, (int)post, (int)inner);
+    PB_CHECK_LAUNCH("coarse27_kernel");
+    return PB_OK;
+}

@@ -1,37 +1,23 @@
-// FP32 multigrid inside an FP64 defect-correction loop.
+// FP32 multigrid level 0 and the FP64 defect of the refined solvers.
 //
 // The reference solves A x = b with FP64 V-cycles (src/capi.mojo:310-742,
-// python/mojo_poissonrecon/core.py:141-193).  Here the FP64 iterate x is
-// refined by corrections e from FP32 V-cycles on A e = r, r = b - A x taken in
-// FP64.  The operator, smoother, transfers and cycle shape are the
-// reference's; only the precision of the inner cycle changes.
-//
-// FP32 level layout ("padded"): side n grid stored with a one-node ghost
-// layer of zeros on every face, x offset 4, row pitch P (multiple of 8):
-//   index(x, y, z) = ((z+1)*(n+2) + (y+1))*P + (x+4),  x,y,z in [-1, n].
-// Ghosts stay zero, so a 6-neighbour sum over the padded array equals the
-// reference's Neumann sum over in-grid neighbours; the degree term lives in
-// the stored diagonal D = (deg + pw*screen) * (n-1)^2.
+// python/mojo_poissonrecon/core.py:141-193).  The refined solvers keep x in
+// FP64 and precondition with FP32 V-cycles on A e = r.  Level 0 of those
+// cycles uses the reference's operator in the padded FP32 layout
+// (level32.cuh): ghosts are zero, so a 6-neighbour sum over the padded array
+// equals the reference's Neumann sum over in-grid neighbours, and the degree
+// term lives in the stored diagonal D = (deg + pw*screen) * (n-1)^2.  The
+// coarse levels are Galerkin operators (mg27.cu).
 #include "common.cuh"
+#include "level32.cuh"
 
 namespace pb {
 
-struct Geom {
-    int n;          // grid side
-    int P;          // row pitch (floats)
-    int64_t plane;  // (n+2)*P
-    __host__ __device__ __forceinline__ int64_t at(int x, int y, int z) const {
-        return ((int64_t)(z + 1) * (n + 2) + (y + 1)) * P + (x + 4);
-    }
-};
-
-__host__ __device__ inline int pitch_of(int n) { return ((n + 5) + 7) & ~7; }
-inline Geom geom(int n) { return Geom{n, pitch_of(n), (int64_t)(n + 2) * pitch_of(n)}; }
-inline int64_t padded_size(int n) { return (int64_t)(n + 2) * geom(n).plane; }
-
-// ---- level set-up: D and 1/D from the FP64 screen (dense layout) --------------
+// ---- level set-up: D, 1/D and the prolongation weights from the FP64 screen ----
+// weights (may be null): s = 1 on nodes of the coarse grid (all coordinates
+// even), else deg (n-1)^2 / D (mg27.cu).
 __global__ void level_setup_kernel(const double* __restrict__ screen, Geom g, double pw, float* __restrict__ D,
-                                   float* __restrict__ invD) {
+                                   float* __restrict__ invD, float* __restrict__ weights) {
     const int n = g.n;
     const int64_t total = (int64_t)n * n * n;
     const double h = (double)(n - 1), h2 = h * h;
@@ -42,6 +28,7 @@ __global__ void level_setup_kernel(const double* __restrict__ screen, Geom g, do
         const int64_t p = g.at(x, y, z);
         D[p] = (float)d;
         invD[p] = (float)(1.0 / d);
+        if (weights) weights[p] = ((x | y | z) & 1) ? (float)((double)deg * h2 / d) : 1.0f;
     }
 }
 
@@ -123,36 +110,22 @@ __global__ void sum_partials_kernel(const double* __restrict__ partial, int coun
     if (threadIdx.x == 0) *out = t;
 }
 
-// Trilinear prolongation of the coarse correction at fine node (x, y, z)
-// (capi.mojo:677-742 in FP32).
-__device__ __forceinline__ float prolong_at(const float* __restrict__ c, const Geom& gc, int x, int y, int z) {
-    const int x0 = x >> 1, y0 = y >> 1, z0 = z >> 1;
-    const int x1 = min(x0 + 1, gc.n - 1), y1 = min(y0 + 1, gc.n - 1), z1 = min(z0 + 1, gc.n - 1);
-    const float tx = (x & 1) ? 0.5f : 0.0f, ty = (y & 1) ? 0.5f : 0.0f, tz = (z & 1) ? 0.5f : 0.0f;
-    const float c00 = c[gc.at(x0, y0, z0)] * (1.f - tx) + c[gc.at(x1, y0, z0)] * tx;
-    const float c10 = c[gc.at(x0, y1, z0)] * (1.f - tx) + c[gc.at(x1, y1, z0)] * tx;
-    const float c01 = c[gc.at(x0, y0, z1)] * (1.f - tx) + c[gc.at(x1, y0, z1)] * tx;
-    const float c11 = c[gc.at(x0, y1, z1)] * (1.f - tx) + c[gc.at(x1, y1, z1)] * tx;
-    const float c0 = c00 * (1.f - ty) + c10 * ty;
-    const float c1 = c01 * (1.f - ty) + c11 * ty;
-    return c0 * (1.f - tz) + c1 * tz;
-}
-
-// ---- FP32 residual fused with full-weighting restriction -----------------------
-// coarse_rhs = restrict(rhs - A e) (capi.mojo:413-470 then :557-673, in FP32)
-// without writing the fine residual.  A block owns a 32 x 4 tile of coarse
-// (x, y) and marches coarse z; fine residual planes of the tile plus a halo of
-// one (65 x 9 nodes) are computed into a three-plane ring in shared memory,
-// plane 2zc+1 being reused as plane 2(zc+1)-1 of the next coarse plane.  The
-// restriction weights (1,2,1)^3 over in-grid fine nodes, normalised by their
-// sum, as in the reference.
+// ---- level-0 residual fused with the scaled restriction -------------------------
+// coarse_rhs = P^T (s (rhs - A e)) / 8 (mg27.cu) without writing the fine
+// residual.  A block owns a 32 x 4 tile of coarse (x, y) and marches coarse z;
+// fine residual planes of the tile plus a halo of one (65 x 9 nodes), already
+// multiplied by the prolongation weight s, are computed into a three-plane
+// ring in shared memory, plane 2zc+1 being reused as plane 2(zc+1)-1 of the
+// next coarse plane.  Out-of-grid ring entries are zero, so the restriction
+// sums all 27 entries with weights (1,2,1)^3 / 64.
 constexpr int kRrCX = 32, kRrCY = 4, kRrCZ = 8;
 constexpr int kRrFX = 2 * kRrCX + 1, kRrFY = 2 * kRrCY + 1;  // 65 x 9 fine nodes
 constexpr int kRrThreads = 256;
 
 __global__ void __launch_bounds__(kRrThreads) residual_restrict32_kernel(const float* __restrict__ e,
                                                                           const float* __restrict__ rhs,
-                                                                          const float* __restrict__ D, Geom gf,
+                                                                          const float* __restrict__ D,
+                                                                          const float* __restrict__ w, Geom gf,
                                                                           float h2, float* __restrict__ coarse,
                                                                           Geom gc) {
     __shared__ float ring[3][kRrFY][kRrFX + 3];
@@ -170,7 +143,7 @@ __global__ void __launch_bounds__(kRrThreads) residual_restrict32_kernel(const f
             if (f >= 0 && f < fn && x >= 0 && x < fn && y >= 0 && y < fn) {
                 const int64_t p = gf.at(x, y, f);
                 const float sum = e[p - 1] + e[p + 1] + e[p - gf.P] + e[p + gf.P] + e[p - gf.plane] + e[p + gf.plane];
-                r = rhs[p] - (D[p] * e[p] - sum * h2);
+                r = w[p] * (rhs[p] - (D[p] * e[p] - sum * h2));
             }
             dst[ly][lx] = r;
         }
@@ -184,129 +157,22 @@ __global__ void __launch_bounds__(kRrThreads) residual_restrict32_kernel(const f
             const int cy = tid / kRrCX, cx = tid - cy * kRrCX;
             const int xc = xc0 + cx, yc = yc0 + cy;
             if (xc < cn && yc < cn) {
-                float sum = 0.0f, wsum = 0.0f;
+                float sum = 0.0f;
+#pragma unroll
                 for (int oz = -1; oz <= 1; ++oz) {
                     const int zz = 2 * zc + oz;
-                    if (zz < 0 || zz >= fn) continue;
-                    const float wz = oz == 0 ? 2.f : 1.f;
+#pragma unroll
                     for (int oy = -1; oy <= 1; ++oy) {
-                        const int yy = 2 * yc + oy;
-                        if (yy < 0 || yy >= fn) continue;
-                        const float wy = oy == 0 ? 2.f : 1.f;
                         const float* row = ring[(zz + 3) % 3][2 * cy + 1 + oy];
-                        for (int ox = -1; ox <= 1; ++ox) {
-                            const int xx = 2 * xc + ox;
-                            if (xx < 0 || xx >= fn) continue;
-                            const float w = (ox == 0 ? 2.f : 1.f) * wy * wz;
-                            sum += row[2 * cx + 1 + ox] * w;
-                            wsum += w;
-                        }
+#pragma unroll
+                        for (int ox = -1; ox <= 1; ++ox)
+                            sum += row[2 * cx + 1 + ox] * (float)((ox ? 1 : 2) * (oy ? 1 : 2) * (oz ? 1 : 2));
                     }
                 }
-                coarse[gc.at(xc, yc, zc)] = sum / wsum;
+                coarse[gc.at(xc, yc, zc)] = sum * (1.0f / 64.0f);
             }
         }
         __syncthreads();  // the ring slots of planes 2zc-1 and 2zc are rewritten next
-    }
-}
-
-// ---- all levels with n <= kCoarseN in one block ---------------------------------
-// The reference's recursion below that size (V(3,3), 40 sweeps at n = 3) with
-// __syncthreads between colour passes; arrays stay in the padded layout.
-constexpr int kCoarseN = 17;
-constexpr int kCoarseThreads = 1024;
-constexpr int kMaxLevels = 8;
-
-struct CoarseLevels {
-    int count;
-    Geom g[kMaxLevels];
-    float* e[kMaxLevels];
-    float* rhs[kMaxLevels];
-    float* res[kMaxLevels];
-    const float* D[kMaxLevels];
-    const float* invD[kMaxLevels];
-};
-
-__device__ void coarse_relax(const CoarseLevels& L, int l, int iters) {
-    const Geom g = L.g[l];
-    const int n = g.n;
-    const float h2 = (float)(n - 1) * (float)(n - 1);
-    float* e = L.e[l];
-    const float* rhs = L.rhs[l];
-    const float* invD = L.invD[l];
-    const int total = n * n * n;
-    for (int it = 0; it < iters; ++it)
-        for (int colour = 0; colour < 2; ++colour) {
-            for (int i = threadIdx.x; i < total; i += blockDim.x) {
-                const int x = i % n, y = (i / n) % n, z = i / (n * n);
-                if (((x + y + z) & 1) != colour) continue;
-                const int64_t p = g.at(x, y, z);
-                const float s = e[p - 1] + e[p + 1] + e[p - g.P] + e[p + g.P] + e[p - g.plane] + e[p + g.plane];
-                e[p] = (rhs[p] + s * h2) * invD[p];
-            }
-            __syncthreads();
-        }
-}
-
-__global__ void __launch_bounds__(kCoarseThreads) coarse_cycle_kernel(CoarseLevels L, int pre, int post, int coarsest) {
-    // descend
-    for (int l = 0; l < L.count; ++l) {
-        const Geom g = L.g[l];
-        const int n = g.n;
-        // e = 0 on the interior (ghosts are already zero)
-        for (int i = threadIdx.x; i < n * n * n; i += blockDim.x) {
-            const int x = i % n, y = (i / n) % n, z = i / (n * n);
-            L.e[l][g.at(x, y, z)] = 0.0f;
-        }
-        __syncthreads();
-        if (l == L.count - 1) {
-            coarse_relax(L, l, coarsest);
-            break;
-        }
-        coarse_relax(L, l, pre);
-        const float h2 = (float)(n - 1) * (float)(n - 1);
-        for (int i = threadIdx.x; i < n * n * n; i += blockDim.x) {
-            const int x = i % n, y = (i / n) % n, z = i / (n * n);
-            const int64_t p = g.at(x, y, z);
-            const float* e = L.e[l];
-            const float s = e[p - 1] + e[p + 1] + e[p - g.P] + e[p + g.P] + e[p - g.plane] + e[p + g.plane];
-            L.res[l][p] = L.rhs[l][p] - (L.D[l][p] * e[p] - s * h2);
-        }
-        __syncthreads();
-        const Geom gc = L.g[l + 1];
-        const int cn = gc.n;
-        for (int i = threadIdx.x; i < cn * cn * cn; i += blockDim.x) {
-            const int x = i % cn, y = (i / cn) % cn, z = i / (cn * cn);
-            float sum = 0.0f, wsum = 0.0f;
-            for (int oz = -1; oz <= 1; ++oz) {
-                const int zz = 2 * z + oz;
-                if (zz < 0 || zz >= n) continue;
-                for (int oy = -1; oy <= 1; ++oy) {
-                    const int yy = 2 * y + oy;
-                    if (yy < 0 || yy >= n) continue;
-                    for (int ox = -1; ox <= 1; ++ox) {
-                        const int xx = 2 * x + ox;
-                        if (xx < 0 || xx >= n) continue;
-                        const float w = (ox == 0 ? 2.f : 1.f) * (oy == 0 ? 2.f : 1.f) * (oz == 0 ? 2.f : 1.f);
-                        sum += L.res[l][g.at(xx, yy, zz)] * w;
-                        wsum += w;
-                    }
-                }
-            }
-            L.rhs[l + 1][gc.at(x, y, z)] = sum / wsum;
-        }
-        __syncthreads();
-    }
-    // ascend
-    for (int l = L.count - 2; l >= 0; --l) {
-        const Geom g = L.g[l], gc = L.g[l + 1];
-        const int n = g.n;
-        for (int i = threadIdx.x; i < n * n * n; i += blockDim.x) {
-            const int x = i % n, y = (i / n) % n, z = i / (n * n);
-            L.e[l][g.at(x, y, z)] += prolong_at(L.e[l + 1], gc, x, y, z);
-        }
-        __syncthreads();
-        coarse_relax(L, l, post);
     }
 }
 
@@ -338,10 +204,10 @@ extern "C" int pb_level_geometry(int64_t n, int64_t* pitch, int64_t* padded_coun
 }
 
 extern "C" int pb_level_setup_f32(const double* screen, int64_t n, double point_weight, float* D, float* invD,
-                                  void* stream) {
+                                  float* weights, void* stream) {
     if (n < 2 || n > 4097 || !screen || !D || !invD) return fail(PB_ERR_INVALID, "level setup: bad args");
     level_setup_kernel<<<stride_grid(n * n * n, 256), 256, 0, (cudaStream_t)stream>>>(screen, geom((int)n),
-                                                                                     point_weight, D, invD);
+                                                                                     point_weight, D, invD, weights);
     PB_CHECK_LAUNCH("level_setup_kernel");
     return PB_OK;
 }
@@ -371,39 +237,17 @@ extern "C" int pb_defect_f64(const double* x_old, const float* e, double* x_new,
     return PB_OK;
 }
 
-// coarse_rhs (side (n+1)/2) = full-weighting restriction of rhs - A e on side n.
-extern "C" int pb_residual_restrict_f32(const float* e, const float* rhs, const float* D, float* coarse_rhs,
-                                        int64_t n, void* stream) {
-    if (n < 3 || n > 4097 || !e || !rhs || !D || !coarse_rhs) return fail(PB_ERR_INVALID, "residual_restrict: bad args");
+// coarse_rhs (side (n+1)/2) = P^T (s (rhs - A e)) / 8 on level 0 (side n, diagonal D, weights s).
+extern "C" int pb_residual_restrict_f32(const float* e, const float* rhs, const float* D, const float* weights,
+                                        float* coarse_rhs, int64_t n, void* stream) {
+    if (n < 3 || n > 4097 || !e || !rhs || !D || !weights || !coarse_rhs)
+        return fail(PB_ERR_INVALID, "residual_restrict: bad args");
     const int cn = (int)((n + 1) / 2);
     const float h2 = (float)((n - 1) * (n - 1));
     const dim3 grid((cn + kRrCX - 1) / kRrCX, (cn + kRrCY - 1) / kRrCY, (cn + kRrCZ - 1) / kRrCZ);
-    residual_restrict32_kernel<<<grid, kRrThreads, 0, (cudaStream_t)stream>>>(e, rhs, D, geom((int)n), h2,
+    residual_restrict32_kernel<<<grid, kRrThreads, 0, (cudaStream_t)stream>>>(e, rhs, D, weights, geom((int)n), h2,
                                                                               coarse_rhs, geom(cn));
     PB_CHECK_LAUNCH("residual_restrict32_kernel");
     return PB_OK;
 }
 
-// Levels with side <= 17 in one block.  Arrays of `count` levels, finest first,
-// each in the padded layout; rhs[0] holds the restricted residual from above.
-extern "C" int pb_coarse_cycle_f32(int64_t count, const int64_t* sizes, float* const* e, float* const* rhs,
-                                   float* const* res, const float* const* D, const float* const* invD, int64_t pre,
-                                   int64_t post, int64_t coarsest_sweeps, void* stream) {
-    if (count < 1 || count > kMaxLevels || !sizes || !e || !rhs || !res || !D || !invD)
-        return fail(PB_ERR_INVALID, "coarse cycle: bad args");
-    CoarseLevels L;
-    L.count = (int)count;
-    for (int l = 0; l < count; ++l) {
-        if (sizes[l] < 2 || sizes[l] > kCoarseN || (l && sizes[l] != (sizes[l - 1] + 1) / 2))
-            return fail(PB_ERR_INVALID, "coarse cycle: bad level sizes");
-        L.g[l] = geom((int)sizes[l]);
-        L.e[l] = e[l];
-        L.rhs[l] = rhs[l];
-        L.res[l] = res[l];
-        L.D[l] = D[l];
-        L.invD[l] = invD[l];
-    }
-    coarse_cycle_kernel<<<1, kCoarseThreads, 0, (cudaStream_t)stream>>>(L, (int)pre, (int)post, (int)coarsest_sweeps);
-    PB_CHECK_LAUNCH("coarse_cycle_kernel");
-    return PB_OK;
-}

@@ -275,7 +275,9 @@ static int make_map(CUtensorMap* map, const float* base, int n, int P, int rows)
 
 }  // namespace tma
 
-// ---- prolongation add on the padded layout (capi.mojo:677-742 in FP32) -------
+// ---- scaled prolongation add on the padded layout -------------------------------
+// fine += s * trilinear(coarse) (the P_s of mg27.cu; trilinear as in
+// capi.mojo:677-742), s the fine level's prolongation weights.
 // Tiled: a block owns a 64 x 4 (x, y) fine tile and 16 fine planes; the fine
 // coordinates come from the launch shape, rows are read and written
 // coalesced, and the coarse values (one coarse node per 2 x 2 x 2 fine nodes)
@@ -283,8 +285,9 @@ static int make_map(CUtensorMap* map, const float* base, int n, int P, int rows)
 constexpr int kProTX = 64, kProTY = 4, kProTZ = 16;
 
 __global__ void __launch_bounds__(kProTX* kProTY) prolong_add32_kernel(const float* __restrict__ c,
-                                                                       float* __restrict__ f, int n, int P, int cn,
-                                                                       int cP) {
+                                                                       float* __restrict__ f,
+                                                                       const float* __restrict__ w, int n, int P,
+                                                                       int cn, int cP) {
     const int x = blockIdx.x * kProTX + threadIdx.x, y = blockIdx.y * kProTY + threadIdx.y;
     if (x >= n || y >= n) return;
     const int z0 = blockIdx.z * kProTZ, z1 = min(n, z0 + kProTZ);
@@ -304,7 +307,8 @@ __global__ void __launch_bounds__(kProTX* kProTY) prolong_add32_kernel(const flo
         const float c01 = c1[0] * (1.f - tx) + c1[dx] * tx;
         const float c11 = c1[dy] * (1.f - tx) + c1[dy + dx] * tx;
         const float v = (c00 * (1.f - ty) + c10 * ty) * (1.f - tz) + (c01 * (1.f - ty) + c11 * ty) * tz;
-        f[((int64_t)(z + 1) * (n + 2) + (y + 1)) * P + (x + 4)] += v;
+        const int64_t p = ((int64_t)(z + 1) * (n + 2) + (y + 1)) * P + (x + 4);
+        f[p] += w[p] * v;
     }
 }
 
@@ -364,13 +368,15 @@ extern "C" int pb_sweep_tma_f32(const float* e_in, float* e_out, const float* rh
     return mode == 1 ? launch(sweep_kernel<true, kSlots>) : launch(sweep_kernel<false, kSlots>);
 }
 
-// fine += trilinear prolongation of coarse (side (n+1)/2), padded layouts.
-extern "C" int pb_prolong_add_f32(const float* coarse, float* fine, int64_t fine_n, void* stream) {
-    if (fine_n < 3 || fine_n > 4097 || !coarse || !fine) return fail(PB_ERR_INVALID, "prolong32: bad args");
+// fine += s * trilinear(coarse) (coarse side (n+1)/2), padded layouts, s the
+// fine level's prolongation weights.
+extern "C" int pb_prolong_fac_f32(const float* coarse, float* fine, const float* weights, int64_t fine_n,
+                                  void* stream) {
+    if (fine_n < 3 || fine_n > 4097 || !coarse || !fine || !weights) return fail(PB_ERR_INVALID, "prolong32: bad args");
     const int n = (int)fine_n, cn = (n + 1) / 2;
     const dim3 grid((n + kProTX - 1) / kProTX, (n + kProTY - 1) / kProTY, (n + kProTZ - 1) / kProTZ);
-    prolong_add32_kernel<<<grid, dim3(kProTX, kProTY), 0, (cudaStream_t)stream>>>(coarse, fine, n, pitch_for(n), cn,
-                                                                                   pitch_for(cn));
+    prolong_add32_kernel<<<grid, dim3(kProTX, kProTY), 0, (cudaStream_t)stream>>>(coarse, fine, weights, n,
+                                                                                   pitch_for(n), cn, pitch_for(cn));
     PB_CHECK_LAUNCH("prolong_add32_kernel");
     return PB_OK;
 }

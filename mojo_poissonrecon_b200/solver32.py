@@ -6,7 +6,7 @@ flexible conjugate gradients:
     x = 0.5                                  (the reference's initial guess, core.py:270)
     r = b - A x                              FP64 (pb_defect_f64)
     while ||r|| > tol * ||b||:               evaluated on the device
-        z = V(3,3)-cycle on A e = r, e = 0   FP32 (the reference's operator and cycle shape)
+        z = V-cycle on A e = r, e = 0        FP32
         p = z - beta p;  q = A p;  x += alpha p;  r -= alpha q      FP64 (pb_fcg_step_inplace_f64)
 
 One iteration touches the same buffers every time, so the engine captures it
@@ -16,11 +16,16 @@ no host synchronisation per iteration.  Engines (hierarchy, vectors, graph)
 are cached per device, grid side and point weight and reused across solves.
 
 Defect correction (``precision="fp32_defect"``): x += V(r), one FP32 V-cycle
-per FP64 residual, eager launches; about 2.5x more V-cycles than FCG(1).
+per FP64 residual, eager launches.
 
-The FP32 cycle reuses the reference's operator, red-black smoother, boundary-
-normalised full weighting, trilinear prolongation and 40 sweeps on the 3^3
-grid (core.py:141-193); levels of side <= 17 run in a single launch.
+The FP32 cycle: level 0 is the reference's operator with its red-black
+Gauss-Seidel smoother, 3 sweeps each way (core.py:141-193); the coarser
+levels are Galerkin operators with screening-scaled transfers (mg27.cu),
+smoothed by COARSE_SWEEPS sweeps each way, which cut the cycles needed for a
+given residual 2-4x against the reference's rediscretised hierarchy.  Levels
+of side <= 17 run in a single launch, the 3^3 level solved exactly with its
+inverse (built once per set-up).  Convergence is always measured with the
+reference's FP64 operator.
 """
 
 from __future__ import annotations
@@ -36,6 +41,7 @@ from . import _native as nat
 from .solver import SolveStats, level_sizes, norm
 
 COARSE_N = 17  # levels of this side or smaller: one single-block launch
+COARSE_SWEEPS = 2  # pre- and post-smoothing sweeps on every level below level 0
 MAX_ITER = 512  # capacity of the device iteration history (and hard cap)
 
 # When set to a list, every finest-level sweep launched eagerly appends
@@ -44,43 +50,60 @@ PROBE: list | None = None
 
 
 class Level32:
-    """Padded FP32 arrays of one level (zero-filled so the ghosts stay zero)."""
+    """Padded FP32 arrays of one level (zero-filled so the ghosts stay zero).
 
-    def __init__(self, n: int, device: torch.device, lib):
+    Every level has work arrays (rhs, res, ea, eb), 1/diagonal (invD) and its
+    prolongation weights (weights).  Level 0 also keeps the reference's
+    7-point operator as its diagonal D.  Levels that run the 27-point kernels
+    (all but a level 0 of side >= 33) hold their operator as 14 planes `coef`."""
+
+    def __init__(self, n: int, device: torch.device, lib, first: bool):
         self.n = n
         pitch, count = ctypes.c_int64(), ctypes.c_int64()
         nat.check(lib.pb_level_geometry(n, ctypes.byref(pitch), ctypes.byref(count)), "level geometry")
         self.count = count.value
 
-        def zeros():
-            return torch.zeros(self.count, dtype=torch.float32, device=device)
+        def zeros(*lead):
+            return torch.zeros(*lead, self.count, dtype=torch.float32, device=device)
 
-        self.D, self.invD, self.rhs, self.res, self.ea, self.eb = (zeros() for _ in range(6))
+        self.invD, self.rhs, self.res, self.ea, self.eb, self.weights = (zeros() for _ in range(6))
+        self.seven = first and n > COARSE_N
+        self.D = zeros() if first else None
+        self.coef = None if self.seven else zeros(14)
+
+    def tensors(self) -> list:
+        return [t for t in (self.invD, self.rhs, self.res, self.ea, self.eb, self.weights, self.D, self.coef)
+                if t is not None]
 
 
 class Hierarchy32:
-    """FP32 levels (padded layout); `setup` fills D and 1/D from an FP64 screen."""
+    """FP32 preconditioner levels.  Level 0 is the reference's operator (its
+    red-black sweeps staged by TMA); the levels below are Galerkin operators
+    P_s^T A P_s / 8 built on the device by `setup` (mg27.cu), down to 3^3,
+    which is solved exactly with its inverse."""
 
-    def __init__(self, n: int, device: torch.device, z_chunk: int = 0):
+    def __init__(self, n: int, device: torch.device, z_chunk: int = 0, coarse_sweeps: int | None = None):
         self.status = torch.zeros(1, dtype=torch.int32, device=device)
         self.lib = nat.lib()
         self.device = device
         self.z_chunk = int(z_chunk)
+        self.coarse_sweeps = COARSE_SWEEPS if coarse_sweeps is None else int(coarse_sweeps)
         self.sizes = level_sizes(n)
-        self.levels = [Level32(m, device, self.lib) for m in self.sizes]
-        self.coarse_screens = [torch.empty((m, m, m), dtype=torch.float64, device=device) for m in self.sizes[1:]]
+        self.levels = [Level32(m, device, self.lib, i == 0) for i, m in enumerate(self.sizes)]
         self.first_coarse = next(i for i, m in enumerate(self.sizes) if m <= COARSE_N)
+        self.inverse = torch.zeros(27 * 27, dtype=torch.float32, device=device)  # of the 3^3 level
         tail = self.levels[self.first_coarse:]
         k = len(tail)
         ptrs = lambda ts: (ctypes.c_void_p * k)(*[t.data_ptr() for t in ts])
         self._coarse_args = (
             k,
             (ctypes.c_int64 * k)(*[lv.n for lv in tail]),
+            ptrs([lv.coef for lv in tail]),
+            ptrs([lv.invD for lv in tail]),
+            ptrs([lv.weights for lv in tail]),
             ptrs([lv.ea for lv in tail]),
             ptrs([lv.rhs for lv in tail]),
             ptrs([lv.res for lv in tail]),
-            ptrs([lv.D for lv in tail]),
-            ptrs([lv.invD for lv in tail]),
         )
         self.pw = None
 
@@ -88,25 +111,43 @@ class Hierarchy32:
     def stream(self) -> int:
         return nat.stream_handle()
 
+    def nbytes(self) -> int:
+        return sum(t.numel() * t.element_size() for lv in self.levels for t in lv.tensors()) + \
+            self.inverse.numel() * 4
+
     def setup(self, screen: torch.Tensor, point_weight: float) -> None:
-        """core.py:267-269 screening hierarchy (FP64), then D and 1/D per level."""
+        """Level 0 from the FP64 screen (D = (deg + pw*screen) h^-2, core.py:150-163),
+        then each coarser level's Galerkin operator from the one above it."""
         L, s = self.lib, self.stream
         self.pw = float(point_weight)
-        screens = [screen] + self.coarse_screens
-        for fine, coarse in zip(screens[:-1], screens[1:]):
-            nat.check(L.pb_restrict_f64(fine.data_ptr(), coarse.data_ptr(), fine.shape[0], s), "restrict")
-            nat.check(L.pb_scale_f64(coarse.data_ptr(), coarse.numel(), 4.0, s), "scale")
-        for lv, scr in zip(self.levels, screens):
-            nat.check(L.pb_level_setup_f32(scr.data_ptr(), lv.n, self.pw, lv.D.data_ptr(), lv.invD.data_ptr(), s),
-                      "level setup")
+        top = self.levels[0]
+        nat.check(L.pb_level_setup_f32(screen.data_ptr(), top.n, self.pw, top.D.data_ptr(), top.invD.data_ptr(),
+                                       top.weights.data_ptr(), s), "level setup")
+        if not top.seven:
+            nat.check(L.pb_level27_from7_f32(top.D.data_ptr(), top.n, top.coef.data_ptr(), s), "level27 from 7")
+            nat.check(L.pb_level27_finish_f32(top.coef.data_ptr(), top.n, top.invD.data_ptr(),
+                                              top.weights.data_ptr(), s), "level27 finish")
+        for fine, lv in zip(self.levels[:-1], self.levels[1:]):
+            src, seven = (fine.D, 1) if fine.seven else (fine.coef, 0)
+            nat.check(L.pb_galerkin_f32(src.data_ptr(), fine.n, seven, fine.weights.data_ptr(), lv.coef.data_ptr(),
+                                        s), "galerkin")
+            nat.check(L.pb_level27_finish_f32(lv.coef.data_ptr(), lv.n, lv.invD.data_ptr(), lv.weights.data_ptr(), s),
+                      "level27 finish")
+        nat.check(L.pb_coarse_inverse_f32(self.levels[-1].coef.data_ptr(), 3, self.inverse.data_ptr(), s),
+                  "coarse inverse")
 
     def _sweep(self, lv: Level32, src, dst, mode: int, coarse=None) -> None:
         """One red-black sweep dst <- S(src); mode 1 starts from zero, mode 2
         first adds the prolongated coarse correction to src in place."""
         L, s = self.lib, self.stream
         if mode == 2:
-            nat.check(L.pb_prolong_add_f32(coarse.data_ptr(), src.data_ptr(), lv.n, s), "prolong32")
+            nat.check(L.pb_prolong_fac_f32(coarse.data_ptr(), src.data_ptr(), lv.weights.data_ptr(), lv.n, s),
+                      "prolong32")
             mode = 0
+        if not lv.seven:
+            nat.check(L.pb_relax27_f32(None if mode == 1 else src.data_ptr(), dst.data_ptr(), lv.rhs.data_ptr(),
+                                       lv.coef.data_ptr(), lv.invD.data_ptr(), lv.n, s), "relax27")
+            return
         probe = PROBE if (PROBE is not None and lv is self.levels[0]) else None
         if probe is not None:
             start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -123,11 +164,14 @@ class Hierarchy32:
             raise RuntimeError("FP32 sweep: a bounded wait on a TMA barrier gave up (status word set)")
 
     def v_cycle(self, level: int = 0, pre: int = 3, post: int = 3) -> torch.Tensor:
-        """Correction for levels[level].rhs from a zero start; returns its tensor."""
+        """Correction for levels[level].rhs from a zero start; returns its tensor.
+        (pre, post) sweeps on level 0, `coarse_sweeps` each way below it."""
         L, s = self.lib, self.stream
+        if level > 0:
+            pre = post = self.coarse_sweeps
         if level >= self.first_coarse:
-            k, sizes, e, rhs, res, D, invD = self._coarse_args
-            nat.check(L.pb_coarse_cycle_f32(k, sizes, e, rhs, res, D, invD, pre, post, 40, s), "coarse cycle")
+            nat.check(L.pb_coarse27_cycle_f32(*self._coarse_args, pre, post, self.coarse_sweeps,
+                                              self.inverse.data_ptr(), s), "coarse cycle")
             return self.levels[level].ea
         lv = self.levels[level]
         a, b = lv.ea, lv.eb
@@ -137,8 +181,14 @@ class Hierarchy32:
             self._sweep(lv, src, dst, 0)
             src, dst = dst, src
         nxt = self.levels[level + 1]
-        nat.check(L.pb_residual_restrict_f32(src.data_ptr(), lv.rhs.data_ptr(), lv.D.data_ptr(), nxt.rhs.data_ptr(),
-                                             lv.n, s), "residual_restrict32")
+        if lv.seven:
+            nat.check(L.pb_residual_restrict_f32(src.data_ptr(), lv.rhs.data_ptr(), lv.D.data_ptr(),
+                                                 lv.weights.data_ptr(), nxt.rhs.data_ptr(), lv.n, s),
+                      "residual_restrict32")
+        else:
+            nat.check(L.pb_residual_restrict27_f32(src.data_ptr(), lv.rhs.data_ptr(), lv.coef.data_ptr(),
+                                                   lv.weights.data_ptr(), lv.n, lv.res.data_ptr(),
+                                                   nxt.rhs.data_ptr(), s), "residual_restrict27")
         coarse = self.v_cycle(level + 1, pre, post)
         self._sweep(lv, src, dst, 2, coarse)  # post-smoothing; the first adds the correction
         src, dst = dst, src
@@ -192,9 +242,8 @@ class RefinedEngine:
             pass
 
     def nbytes(self) -> int:
-        return sum(t.numel() * t.element_size() for t in
-                   (self.screen, self.x, self.r, self.p, self.q)) + sum(
-            6 * lv.count * 4 for lv in self.h.levels)
+        return sum(t.numel() * t.element_size() for t in (self.screen, self.x, self.r, self.p, self.q)) + \
+            self.h.nbytes()
 
     def _iteration(self, handle: int) -> None:
         L, s = self.lib, nat.stream_handle()

@@ -1,0 +1,167 @@
+"""CPU restatement of the FP32 preconditioner's levels (csrc/mg27.cu and the
+level-0 transfers) for the GPU tests: FP64 scipy.sparse on dense (z, y, x)
+arrays of side n.
+
+  A0       the reference's operator: diagonal D = (deg + pw*screen) (n-1)^2,
+           couplings -(n-1)^2 to in-grid face neighbours
+  s        prolongation weights: 1 on nodes of the coarse grid (all coordinates
+           even), else clip((sum_{j != i} -a_ij) / a_ii, 0, 1)
+  P_s      diag(s) P, P trilinear
+  A_c      P_s^T A P_s / 8  (27-point)
+  restrict R r = P^T (s r) / 8
+  relax    red-black ordered sweep, same-colour couplings from the previous iterate
+  cycle    V(pre, post) on level 0, coarse_sweeps each way below, 3^3 solved exactly
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sp
+
+
+def forward_offsets():
+    return [(dx, dy, dz) for dz in (-1, 0, 1) for dy in (-1, 0, 1) for dx in (-1, 0, 1)
+            if dz > 0 or (dz == 0 and (dy > 0 or (dy == 0 and dx > 0)))]
+
+
+def fwd_index(dx, dy, dz):
+    if dz == 1:
+        return 1 + (dy + 1) * 3 + (dx + 1)
+    return 10 + (dx + 1) if dy == 1 else 13
+
+
+def coords(n):
+    z, y, x = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    return z.ravel(), y.ravel(), x.ravel()
+
+
+def degree(n):
+    z, y, x = coords(n)
+    return ((x > 0).astype(int) + (x < n - 1) + (y > 0) + (y < n - 1) + (z > 0) + (z < n - 1)).reshape(n, n, n)
+
+
+def level0_diagonal(screen, pw):
+    n = screen.shape[0]
+    h2 = float(n - 1) ** 2
+    return (degree(n) + pw * screen) * h2
+
+
+def operator7(D):
+    n = D.shape[0]
+    h2 = float(n - 1) ** 2
+    one = sp.diags([np.ones(n - 1), np.ones(n - 1)], [-1, 1])
+    I = sp.identity(n)
+    adj = sp.kron(sp.kron(one, I), I) + sp.kron(sp.kron(I, one), I) + sp.kron(sp.kron(I, I), one)
+    return (sp.diags(D.ravel()) - h2 * adj).tocsr()
+
+
+def weights(A, n):
+    d = A.diagonal()
+    off = -(np.asarray(A.sum(axis=1)).ravel() - d)
+    z, y, x = coords(n)
+    on_coarse = ((x | y | z) & 1) == 0
+    return np.where(on_coarse, 1.0, np.clip(off / d, 0.0, 1.0))
+
+
+def trilinear(n):
+    cn = (n + 1) // 2
+    p = sp.lil_matrix((n, cn))
+    for i in range(n):
+        if i % 2 == 0:
+            p[i, i // 2] = 1.0
+        else:
+            p[i, i // 2] = 0.5
+            p[i, i // 2 + 1] = 0.5
+    p = p.tocsr()
+    return sp.kron(sp.kron(p, p), p).tocsr()
+
+
+def galerkin(A, s, n):
+    Ps = (sp.diags(s) @ trilinear(n)).tocsr()
+    return ((Ps.T @ A @ Ps) / 8.0).tocsr()
+
+
+def planes(A, n):
+    """14 dense (n, n, n) planes: the diagonal, then a(J, J+K) for forward K."""
+    out = np.zeros((14, n, n, n))
+    coo = A.tocoo()
+    z, y, x = coords(n)
+    dz, dy, dx = z[coo.col] - z[coo.row], y[coo.col] - y[coo.row], x[coo.col] - x[coo.row]
+    flat = out.reshape(14, -1)
+    for k, (ox, oy, oz) in [(0, (0, 0, 0))] + [(fwd_index(*K), K) for K in forward_offsets()]:
+        sel = (dx == ox) & (dy == oy) & (dz == oz)
+        flat[k, coo.row[sel]] = coo.data[sel]
+    return out
+
+
+def from_planes(pl, n):
+    """Symmetric sparse operator from 14 dense planes (inverse of `planes`)."""
+    z, y, x = coords(n)
+    idx = np.arange(n ** 3)
+    rows, cols, vals = [idx], [idx], [pl[0].ravel()]
+    for K in forward_offsets():
+        dx, dy, dz = K
+        ok = (x + dx >= 0) & (x + dx < n) & (y + dy >= 0) & (y + dy < n) & (z + dz >= 0) & (z + dz < n)
+        j = idx + dx + dy * n + dz * n * n
+        v = pl[fwd_index(*K)].ravel()
+        rows += [idx[ok], j[ok]]
+        cols += [j[ok], idx[ok]]
+        vals += [v[ok], v[ok]]
+    return sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                         shape=(n ** 3, n ** 3)).tocsr()
+
+
+def hierarchy(screen, pw):
+    """Operators and weights of every level, finest first (side down to 3)."""
+    n = screen.shape[0]
+    A = operator7(level0_diagonal(screen, pw))
+    ops, ws, sizes = [A], [weights(A, n)], [n]
+    while n > 3:
+        A = galerkin(A, ws[-1], n)
+        n = (n + 1) // 2
+        ops.append(A)
+        ws.append(weights(A, n))
+        sizes.append(n)
+    return ops, ws, sizes
+
+
+def relax(A, e_prev, rhs, n, zero=False):
+    d = A.diagonal()
+    z, y, x = coords(n)
+    colour = (x + y + z) & 1
+    prev = np.zeros(n ** 3) if zero else e_prev.ravel().copy()
+    nxt = prev.copy()
+    b = rhs.ravel()
+    for c in (0, 1):
+        src = prev if c == 0 else nxt
+        new = (b - (A @ src - d * src)) / d
+        nxt = np.where(colour == c, new, nxt)
+    return nxt.reshape(n, n, n)
+
+
+def residual_restrict(A, s, e, rhs, n):
+    res = s * (rhs.ravel() - A @ e.ravel())
+    cn = (n + 1) // 2
+    return (trilinear(n).T @ res / 8.0).reshape(cn, cn, cn), res.reshape(n, n, n)
+
+
+def prolong(fine, coarse, s, n):
+    return fine + (s * (trilinear(n) @ coarse.ravel())).reshape(n, n, n)
+
+
+def v_cycle(ops, ws, sizes, level, rhs, pre=3, post=3, coarse_sweeps=2):
+    """The cycle below `level` from a zero start, as the GPU runs it."""
+    A, n = ops[level], sizes[level]
+    if level > 0:
+        pre = post = coarse_sweeps
+    if level == len(ops) - 1:
+        return np.linalg.solve(A.toarray(), rhs.ravel()).reshape(n, n, n)
+    e = relax(A, None, rhs, n, zero=True)
+    for _ in range(pre - 1):
+        e = relax(A, e, rhs, n)
+    coarse_rhs, _ = residual_restrict(A, ws[level], e, rhs, n)
+    c = v_cycle(ops, ws, sizes, level + 1, coarse_rhs, pre, post, coarse_sweeps)
+    e = prolong(e, c, ws[level], n)
+    for _ in range(post):
+        e = relax(A, e, rhs, n)
+    return e

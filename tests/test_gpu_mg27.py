@@ -1,0 +1,164 @@
+"""The FP32 preconditioner's Galerkin levels (csrc/mg27.cu, scaled level-0
+transfers) against the CPU restatement in tests/mg_reference.py.
+
+Tolerances (max norm, relative to the largest magnitude of the compared
+quantity): Galerkin planes 3e-5 (FP32 products and sums of up to ~1300 terms,
+compounded over levels); weights and 1/diagonal 1e-5; a single sweep,
+residual, restriction or prolongation 2e-6 to 4e-6 of the largest term,
+evaluated on the GPU's own FP32 planes so only that kernel's rounding is
+measured; the 3^3 inverse 1e-5; whole cycles 1e-4."""
+
+import numpy as np
+import pytest
+
+import mg_reference as mg
+from padded import from_padded, ghosts_zero, to_padded
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def L():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from mojo_poissonrecon_b200 import _native
+
+    return _native.lib()
+
+
+def shell_screen(n, seed):
+    """Screening concentrated on a spherical shell, as splatting gives."""
+    rng = np.random.default_rng(seed)
+    z, y, x = np.meshgrid(*(np.linspace(0, 1, n),) * 3, indexing="ij")
+    r = np.sqrt((x - 0.5) ** 2 + (y - 0.5) ** 2 + (z - 0.5) ** 2)
+    return np.where(np.abs(r - 0.3) < 1.5 / (n - 1), 5.0 + 20.0 * rng.random((n, n, n)), 0.0)
+
+
+def gpu_hierarchy(n, screen):
+    from mojo_poissonrecon_b200.solver32 import Hierarchy32
+
+    h = Hierarchy32(n, torch.device("cuda"))
+    h.setup(torch.from_numpy(screen).cuda(), 4.0)
+    torch.cuda.synchronize()
+    return h
+
+
+def gpu_planes(L, lv):
+    return np.stack([from_padded(L, lv.coef[k], lv.n) for k in range(14)])
+
+
+def stream():
+    return torch.cuda.current_stream().cuda_stream
+
+
+def gpu_ops(L, h):
+    """Operators and weights of the GPU hierarchy as FP64 sparse matrices."""
+    ops, ws = [], []
+    for lv in h.levels:
+        if lv.coef is None:  # level 0 with the reference's 7-point operator
+            ops.append(mg.operator7(from_padded(L, lv.D, lv.n)))
+        else:
+            ops.append(mg.from_planes(gpu_planes(L, lv), lv.n))
+        ws.append(from_padded(L, lv.weights, lv.n).ravel())
+    return ops, ws, [lv.n for lv in h.levels]
+
+
+@pytest.mark.parametrize("n", [9, 17, 33, 65])
+def test_galerkin_levels_match_restatement(L, n):
+    screen = shell_screen(n, n)
+    ops, ws, sizes = mg.hierarchy(screen, 4.0)
+    h = gpu_hierarchy(n, screen)
+    assert [lv.n for lv in h.levels] == sizes
+    for l, lv in enumerate(h.levels):
+        assert np.abs(from_padded(L, lv.weights, lv.n) - ws[l].reshape(lv.n, lv.n, lv.n)).max() <= 1e-5
+        assert ghosts_zero(L, lv.weights, lv.n)
+        if lv.coef is None:
+            continue
+        got, want = gpu_planes(L, lv), mg.planes(ops[l], lv.n)
+        scale = np.abs(want).max()
+        assert np.abs(got - want).max() <= 3e-5 * scale, (l, np.abs(got - want).max() / scale)
+        inv = 1.0 / ops[l].diagonal().reshape(lv.n, lv.n, lv.n)
+        assert np.abs(from_padded(L, lv.invD, lv.n) - inv).max() <= 1e-5 * np.abs(inv).max()
+        for k in range(14):
+            assert ghosts_zero(L, lv.coef[k], lv.n)
+
+
+@pytest.mark.parametrize("n", [33, 65, 129])
+def test_relax27_and_transfers(L, n):
+    """One sweep (from a start and from zero), the residual with the scaled
+    restriction, and the scaled prolongation on level 1 (27-point)."""
+    h = gpu_hierarchy(n, shell_screen(n, 3 * n))
+    lv, nxt = h.levels[1], h.levels[2]
+    m, cm = lv.n, nxt.n
+    A = mg.from_planes(gpu_planes(L, lv), m)
+    s1 = from_padded(L, lv.weights, m).ravel()
+    rng = np.random.default_rng(n)
+    e = rng.normal(size=(m,) * 3).astype(np.float32).astype(np.float64)
+    rhs = (rng.normal(size=(m,) * 3) * np.abs(A.diagonal()).max()).astype(np.float32).astype(np.float64)
+    coarse = rng.normal(size=(cm,) * 3).astype(np.float32).astype(np.float64)
+    lv.rhs.copy_(to_padded(L, rhs))
+    e_in = to_padded(L, e)
+    out = torch.zeros_like(e_in)
+    terms = np.abs(A).sum(axis=1).max() * np.abs(e).max() + np.abs(rhs).max()
+    dmin = A.diagonal().min()
+    for zero in (False, True):
+        assert L.pb_relax27_f32(None if zero else e_in.data_ptr(), out.data_ptr(), lv.rhs.data_ptr(),
+                                lv.coef.data_ptr(), lv.invD.data_ptr(), m, stream()) == 0, L.pb_last_error()
+        want = mg.relax(A, e, rhs, m, zero=zero)
+        # two dependent half-sweeps: an FP32 sum of 27 terms each, divided by the diagonal
+        assert np.abs(from_padded(L, out, m) - want).max() <= 4e-6 * terms / dmin
+        assert ghosts_zero(L, out, m)
+    coarse_rhs = torch.zeros_like(nxt.rhs)
+    assert L.pb_residual_restrict27_f32(e_in.data_ptr(), lv.rhs.data_ptr(), lv.coef.data_ptr(),
+                                        lv.weights.data_ptr(), m, lv.res.data_ptr(), coarse_rhs.data_ptr(),
+                                        stream()) == 0
+    want_c, want_r = mg.residual_restrict(A, s1, e, rhs, m)
+    assert np.abs(from_padded(L, lv.res, m) - want_r).max() <= 2e-6 * terms
+    assert np.abs(from_padded(L, coarse_rhs, cm) - want_c).max() <= 2e-6 * terms
+    assert ghosts_zero(L, coarse_rhs, cm)
+    fine = to_padded(L, e)
+    assert L.pb_prolong_fac_f32(to_padded(L, coarse).data_ptr(), fine.data_ptr(), lv.weights.data_ptr(), m,
+                                stream()) == 0
+    want = mg.prolong(e, coarse, s1, m)
+    assert np.abs(from_padded(L, fine, m) - want).max() <= 2e-6 * np.abs(want).max()
+    assert ghosts_zero(L, fine, m)
+
+
+def test_coarse_inverse(L):
+    """The 3^3 level's inverse against a dense FP64 inverse of its GPU planes."""
+    h = gpu_hierarchy(17, shell_screen(17, 1))
+    A = mg.from_planes(gpu_planes(L, h.levels[-1]), 3).toarray()
+    got = h.inverse.cpu().numpy().reshape(27, 27).astype(np.float64)
+    want = np.linalg.inv(A)
+    assert np.abs(got - want).max() <= 1e-5 * np.abs(want).max()
+
+
+@pytest.mark.parametrize("n", [17, 33])
+def test_coarse_block_cycle(L, n):
+    """The single-block cycle over levels of side <= 17 against the restated cycle."""
+    h = gpu_hierarchy(n, shell_screen(n, 5 * n))
+    k = h.first_coarse
+    ops, ws, sizes = gpu_ops(L, h)
+    m = sizes[k]
+    rhs = np.random.default_rng(n).normal(size=(m,) * 3).astype(np.float32).astype(np.float64)
+    h.levels[k].rhs.copy_(to_padded(L, rhs))
+    got = from_padded(L, h.v_cycle(k), m)
+    want = mg.v_cycle(ops, ws, sizes, k, rhs)
+    assert np.abs(got - want).max() <= 1e-4 * np.abs(want).max()
+
+
+@pytest.mark.parametrize("n", [33, 65])
+def test_full_cycle(L, n):
+    """Level 0 (TMA sweeps, fused scaled transfers) down to 3^3 against the
+    restated cycle on the GPU's own planes."""
+    h = gpu_hierarchy(n, shell_screen(n, 11 * n))
+    D0 = from_padded(L, h.levels[0].D, n)
+    ops, ws, sizes = gpu_ops(L, h)
+    rhs = (np.random.default_rng(n).normal(size=(n,) * 3) * D0.max()).astype(np.float32).astype(np.float64)
+    h.levels[0].rhs.copy_(to_padded(L, rhs))
+    got = from_padded(L, h.v_cycle(0), n)
+    h.check_status()
+    want = mg.v_cycle(ops, ws, sizes, 0, rhs)
+    assert np.abs(got - want).max() <= 1e-4 * np.abs(want).max()
