@@ -194,16 +194,23 @@ size_t pb_defect_workspace_size(int64_t n);
 int pb_defect_f64(const double *x_old, const float *e, double *x_new, const double *rhs,
                   const double *screen, int64_t n, double point_weight, float *r32, double *r64,
                   double *norm2, void *workspace, size_t workspace_bytes, void *stream);
-/* One step of FP64 flexible conjugate gradients, FCG(1), preconditioned by the
- * FP32 V-cycle: from z = M(r) (padded FP32) form p = z - beta p_prev,
- * q = A p, alpha = (p, r)/(p, q), x += alpha p, r -= alpha q, r32 = (float) r,
- * with the scalars kept in scal[0..4] on the device (scal[4] = ||r||^2).
- * first != 0 on the first step (p_prev unused).  No counterpart in the
- * reference, which repeats V-cycles (core.py:274-285). */
+/* FP64 flexible conjugate gradients, FCG(1), preconditioned by the FP32
+ * V-cycle, in two passes per iteration (no counterpart in the reference, which
+ * repeats V-cycles, core.py:274-285).  Device scalars scal[0..4]: (p, Ap),
+ * beta, alpha, (p, r), ||b - A x||^2; flags[0] != 0 on the first step,
+ * flags[1] = iterations done, whose parity selects the buffers: directions
+ * p[it & 1] -> p[(it+1) & 1], iterates x[it & 1] -> x[(it+1) & 1].  Every
+ * iteration touches the same pointers, so one can be captured in a graph. */
 size_t pb_fcg_workspace_size(int64_t n);
-int pb_fcg_step_f64(const float *z, const double *p_prev, double *p, double *q, double *x, double *r,
-                    float *r32, const double *screen, int64_t n, double point_weight, double *scal,
-                    int64_t first, void *workspace, size_t workspace_bytes, void *stream);
+/* Pass 1, after z = M(r32): beta, (p, Ap) and alpha from one stencil pass over z. */
+int pb_fcg_direction_f64(const float *z, const double *p0, const double *p1, const float *r32,
+                         const double *screen, int64_t n, double point_weight, double *scal, const int *flags,
+                         void *workspace, size_t workspace_bytes, void *stream);
+/* Pass 2: p, x += alpha p and the true residual b - A x into r32 (padded FP32),
+ * ||b - A x||^2 into scal[4]. */
+int pb_fcg_update_f64(const float *z, double *p0, double *p1, double *x0, double *x1, const double *b,
+                      const double *screen, float *r32, int64_t n, double point_weight, double *scal,
+                      const int *flags, void *workspace, size_t workspace_bytes, void *stream);
 /* One red-black Gauss-Seidel sweep (colour 0 then colour 1), out of place,
  * with TMA-staged planes (n = 2^k + 1 >= 33): mode 0 from e_in, mode 1 from
  * zero (e_in unused).  z_chunk <= 0 picks one.  A bounded wait that gives up
@@ -215,14 +222,6 @@ int pb_sweep_tma_f32(const float *e_in, float *e_out, const float *rhs, const fl
  * pb_level27_finish_f32 below).  Replaces mpr_prolong_add_f64
  * (capi.mojo:677-742) inside the FP32 cycle. */
 int pb_prolong_fac_f32(const float *coarse, float *fine, const float *weights, int64_t fine_n, void *stream);
-/* Graph-friendly FCG(1) step: p = z - beta p in place (p = z while flags[0]
- * != 0), q = A p, alpha, x += alpha p, r -= alpha q, r32 = (float) r;
- * scal[0..4] as for pb_fcg_step_f64.  Touches the same buffers every call, so
- * an iteration can be captured once and replayed. */
-int pb_fcg_step_inplace_f64(const float *z, double *p, double *q, double *x, double *r, float *r32,
-                            const double *screen, int64_t n, double point_weight, double *scal,
-                            const int *flags, void *workspace, size_t workspace_bytes, void *stream);
-
 /* Device-driven iteration (no counterpart in the reference).  Begin: a graph
  * with one WHILE conditional node; `stream` is captured into its body until
  * pb_loop_capture_end, which instantiates it.  The body's last launch must be

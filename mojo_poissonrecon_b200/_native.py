@@ -60,8 +60,8 @@ _SIGNATURES = {
     "pb_defect_workspace_size": ([I], S),
     "pb_defect_f64": ([P, P, P, P, P, I, F, P, P, P, P, S, P], C),
     "pb_fcg_workspace_size": ([I], S),
-    "pb_fcg_step_f64": ([P, P, P, P, P, P, P, P, I, F, P, I, P, S, P], C),
-    "pb_fcg_step_inplace_f64": ([P, P, P, P, P, P, P, I, F, P, P, P, S, P], C),
+    "pb_fcg_direction_f64": ([P, P, P, P, P, I, F, P, P, P, S, P], C),
+    "pb_fcg_update_f64": ([P, P, P, P, P, P, P, P, I, F, P, P, P, S, P], C),
     "pb_loop_capture_begin": ([P, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_ulonglong)], C),
     "pb_loop_condition": ([ctypes.c_ulonglong, P, P, P, I, P, P], C),
     "pb_loop_capture_end": ([P, P, ctypes.POINTER(ctypes.c_void_p)], C),

@@ -1,22 +1,26 @@
 // FP64 flexible conjugate gradients, FCG(1), around the FP32 V-cycle.
 //
 // The reference solves A x = b by repeating V-cycles (python/mojo_poissonrecon/
-// core.py:274-285).  Used as a preconditioner z = M(r) inside a Krylov loop the
-// same V-cycle needs far fewer applications: on the benchmark torus at depth 7
-// FCG(1) reaches ||r|| / ||b|| <= 1e-8 in 12 cycles where plain repetition
-// needs 27.  Because M is a V-cycle in FP32 (not a fixed symmetric operator),
-// the flexible form is used: each direction is A-orthogonalised against the
-// previous one only.
+// core.py:274-285).  Used as a preconditioner z = M(r) inside a Krylov loop
+// the V-cycle needs fewer applications.  Because M is an FP32 V-cycle (not a
+// fixed symmetric operator), the flexible form is used: each direction is
+// A-orthogonalised against the previous one only.
 //
 //   r = b - A x;  repeat:  z = M(r)
-//                          p = z - beta p_prev,   beta = (z, q_prev) / (p_prev, q_prev)
-//                          q = A p,               alpha = (p, r) / (p, q)
-//                          x += alpha p;  r -= alpha q
+//                          p = z - beta p_prev,   beta  = (z, A p_prev) / (p_prev, A p_prev)
+//                          x += alpha p,          alpha = (p, r) / (p, A p)
+//                          r = b - A x            (the true residual, FP64)
 //
-// All vectors are FP64 except z (the FP32 V-cycle's padded output) and r32
-// (the FP32 copy of r the next V-cycle reads).  The scalars stay on the device:
-// each kernel reads the sums the previous one produced, so an iteration needs
-// no host synchronisation; the host reads ||r||^2 only to decide when to stop.
+// Two passes per iteration.  Pass 1 is one stencil pass over z giving
+// (z, Az), (Az, p_prev) = (z, A p_prev) (A is symmetric), (z, r) and
+// (p_prev, r); beta, (p, Ap) = (z,Az) - 2 beta (z,A p_prev) + beta^2 (p_prev,A p_prev)
+// and alpha follow without forming q = A p.  Pass 2 writes p and x + alpha p
+// and recomputes r = b - A x from them (neighbours formed on the fly), so the
+// residual never drifts from the iterate and no final residual pass is needed.
+// x and p alternate between two buffers by iteration parity (flags[1], on the
+// device), so every iteration launches the same kernels on the same pointers
+// and can be captured once in a graph.  Vectors are FP64 and dense except z
+// and r32 (the FP32 padded copy of r that the next V-cycle reads).
 #include "common.cuh"
 
 namespace pb {
@@ -34,7 +38,7 @@ struct Pad {  // padded FP32 layout of the multigrid levels
 
 __device__ __forceinline__ int lin_tid() { return threadIdx.y * blockDim.x + threadIdx.x; }
 
-// Sums up to 3 values over the block; results valid in linear thread 0.
+// Sums K values over the block; results valid in linear thread 0.
 template <int K>
 __device__ __forceinline__ void block_sums(double (&v)[K], double (*shared)[32]) {
     const int tid = lin_tid(), lane = tid & 31, warp = tid >> 5;
@@ -61,168 +65,135 @@ __device__ __forceinline__ int64_t block_index() {
     return ((int64_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
 }
 
-// (z, q_prev) per block.
-__global__ void __launch_bounds__(kThreads) dot_zq_kernel(const float* __restrict__ z, Pad g,
-                                                          const double* __restrict__ q, double* __restrict__ part) {
-    __shared__ double shared[1][32];
-    const int n = g.n;
-    const int x = blockIdx.x * kTX + threadIdx.x, y = blockIdx.y * kTY + threadIdx.y;
-    const int z0 = blockIdx.z * kTZ, z1 = min(n, z0 + kTZ);
-    double v[1] = {0.0};
-    if (x < n && y < n)
-        for (int k = z0; k < z1; ++k)
-            v[0] += (double)z[g.at(x, y, k)] * q[((int64_t)k * n + y) * n + x];
-    block_sums<1>(v, shared);
-    if (lin_tid() == 0) part[block_index()] = v[0];
-}
-
-// p = z - beta p_prev (beta from the device sums; p = z on the first step),
-// q = A p, and per-block (p, q) and (p, r).
-template <bool FIRST>
-__global__ void __launch_bounds__(kThreads) direction_kernel(const float* __restrict__ zc, Pad g,
-                                                             const double* __restrict__ p_prev,
-                                                             const double* __restrict__ scal,
-                                                             const double* __restrict__ screen,
-                                                             const double* __restrict__ r, double pw,
-                                                             double* __restrict__ p, double* __restrict__ q,
-                                                             double* __restrict__ part) {
-    __shared__ double shared[2][32];
+// Pass 1: per-block (z, Az), (Az, p_prev), (z, r32), (p_prev, r32); flags[1]
+// (iterations done) selects p_prev = p[it & 1]; flags[0] != 0 on the first step.
+__global__ void __launch_bounds__(kThreads) direction_sums_kernel(const float* __restrict__ z, Pad g,
+                                                                  const double* __restrict__ p0,
+                                                                  const double* __restrict__ p1,
+                                                                  const float* __restrict__ r32,
+                                                                  const double* __restrict__ screen, double pw,
+                                                                  const int* __restrict__ flags,
+                                                                  double* __restrict__ part) {
+    __shared__ double shared[4][32];
     const int n = g.n;
     const int x = blockIdx.x * kTX + threadIdx.x, y = blockIdx.y * kTY + threadIdx.y;
     const int z0 = blockIdx.z * kTZ, z1 = min(n, z0 + kTZ);
     const double h = (double)(n - 1), h2 = h * h;
-    // scal[0] = (z, q_prev); scal[2] still holds (p_prev, q_prev) from the previous step
-    const double beta = FIRST ? 0.0 : scal[0] / scal[2];
+    const bool first = flags[0] != 0;
+    const double* __restrict__ pp = (flags[1] & 1) ? p1 : p0;
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    if (x < n && y < n) {
+        const int degxy = (x > 0) + (x + 1 < n) + (y > 0) + (y + 1 < n);
+        for (int k = z0; k < z1; ++k) {
+            const int64_t i = ((int64_t)k * n + y) * n + x;
+            const int64_t c = g.at(x, y, k);
+            // ghosts of the padded z are zero: the 6-neighbour sum needs no tests
+            const double s = (double)z[c - 1] + (double)z[c + 1] + (double)z[c - g.P] + (double)z[c + g.P] +
+                             (double)z[c - g.plane] + (double)z[c + g.plane];
+            const int deg = degxy + (k > 0) + (k + 1 < n);
+            const double zc = (double)z[c];
+            const double az = ((double)deg * h2 + pw * screen[i] * h2) * zc - s * h2;
+            const double rc = (double)r32[c];
+            v[0] += zc * az;
+            v[2] += zc * rc;
+            if (!first) {
+                const double pv = pp[i];
+                v[1] += az * pv;
+                v[3] += pv * rc;
+            }
+        }
+    }
+    block_sums<4>(v, shared);
+    if (lin_tid() == 0)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) part[4 * block_index() + k] = v[k];
+}
+
+// Sums pass 1's partials (fixed order) and forms the step's scalars:
+//   scal[0] (p, Ap) (the previous direction's on entry)   scal[1] beta
+//   scal[2] alpha   scal[3] (p, r)
+__global__ void direction_finish_kernel(const double* __restrict__ part, int blocks, const int* __restrict__ flags,
+                                        double* __restrict__ scal) {
+    __shared__ double shared[4][32];
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int b = threadIdx.x; b < blocks; b += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] += part[4 * (int64_t)b + k];
+    block_sums<4>(v, shared);
+    if (threadIdx.x != 0) return;
+    const double zz = v[0], zq = v[1], zr = v[2], pr = v[3];
+    const bool first = flags[0] != 0;
+    const double pap_prev = scal[0];
+    const double beta = first || !(pap_prev > 0.0) ? 0.0 : zq / pap_prev;
+    const double pap = first ? zz : zz - 2.0 * beta * zq + beta * beta * pap_prev;
+    const double prn = first ? zr : zr - beta * pr;
+    scal[0] = pap;
+    scal[1] = beta;
+    scal[2] = pap > 0.0 ? prn / pap : 0.0;
+    scal[3] = prn;
+}
+
+// Pass 2: p_new = z - beta p_prev, x_new = x + alpha p_new, r = b - A x_new
+// (neighbour values of x_new formed on the fly), r32 = (float) r, per-block
+// ||r||^2.  Buffers by parity: p_prev = p[it & 1] -> p_new = p[(it+1) & 1],
+// x = x[it & 1] -> x_new = x[(it+1) & 1].
+__global__ void __launch_bounds__(kThreads) update_residual_kernel(
+    const float* __restrict__ z, Pad g, double* p0, double* p1, double* x0, double* x1, const double* __restrict__ b,
+    const double* __restrict__ screen, double pw, const double* __restrict__ scal, const int* __restrict__ flags,
+    float* __restrict__ r32, double* __restrict__ part) {
+    __shared__ double shared[1][32];
+    const int n = g.n;
+    const int x = blockIdx.x * kTX + threadIdx.x, y = blockIdx.y * kTY + threadIdx.y;
+    const int z0 = blockIdx.z * kTZ, z1 = min(n, z0 + kTZ);
+    const double h = (double)(n - 1), h2 = h * h;
+    const int odd = flags[1] & 1;
+    const bool first = flags[0] != 0;
+    const double* __restrict__ pp = odd ? p1 : p0;
+    double* __restrict__ pn = odd ? p0 : p1;
+    const double* __restrict__ xc = odd ? x1 : x0;
+    double* __restrict__ xn = odd ? x0 : x1;
+    const double beta = first ? 0.0 : scal[1], alpha = scal[2];
     const int64_t nn = (int64_t)n * n;
-    double v[2] = {0.0, 0.0};
+    double v[1] = {0.0};
     if (x < n && y < n) {
         const int degxy = (x > 0) + (x + 1 < n) + (y > 0) + (y + 1 < n);
         for (int k = z0; k < z1; ++k) {
             const int64_t i = (int64_t)k * nn + (int64_t)y * n + x;
             const int64_t c = g.at(x, y, k);
-            auto pv = [&](int64_t di, int64_t dc) -> double {
-                double val = (double)zc[c + dc];
-                if (!FIRST) val -= beta * p_prev[i + di];
+            auto dir = [&](int64_t di, int64_t dc) -> double {
+                double val = (double)z[c + dc];
+                if (!first) val -= beta * pp[i + di];
                 return val;
             };
+            auto xnew = [&](int64_t di, int64_t dc) -> double { return xc[i + di] + alpha * dir(di, dc); };
             double s = 0.0;
-            if (x > 0) s += pv(-1, -1);
-            if (x + 1 < n) s += pv(1, 1);
-            if (y > 0) s += pv(-n, -g.P);
-            if (y + 1 < n) s += pv(n, g.P);
-            if (k > 0) s += pv(-nn, -g.plane);
-            if (k + 1 < n) s += pv(nn, g.plane);
+            if (x > 0) s += xnew(-1, -1);
+            if (x + 1 < n) s += xnew(1, 1);
+            if (y > 0) s += xnew(-n, -g.P);
+            if (y + 1 < n) s += xnew(n, g.P);
+            if (k > 0) s += xnew(-nn, -g.plane);
+            if (k + 1 < n) s += xnew(nn, g.plane);
             const int deg = degxy + (k > 0) + (k + 1 < n);
-            const double pc = pv(0, 0);
-            const double qc = ((double)deg * h2 + pw * screen[i] * h2) * pc - s * h2;
-            p[i] = pc;
-            q[i] = qc;
-            v[0] += pc * qc;
-            v[1] += pc * r[i];
+            const double pc = dir(0, 0);
+            const double xv = xc[i] + alpha * pc;
+            pn[i] = pc;
+            xn[i] = xv;
+            const double r = b[i] - (((double)deg * h2 + pw * screen[i] * h2) * xv - s * h2);
+            r32[c] = (float)r;
+            v[0] += r * r;
         }
     }
-    block_sums<2>(v, shared);
-    if (lin_tid() == 0) {
-        part[2 * block_index()] = v[0];
-        part[2 * block_index() + 1] = v[1];
-    }
-}
-
-// x += alpha p, r -= alpha q (alpha = scal[3] / scal[2]), r32 = (float) r, per-block ||r||^2.
-__global__ void __launch_bounds__(kThreads) update_kernel(double* __restrict__ x, double* __restrict__ r,
-                                                          const double* __restrict__ p,
-                                                          const double* __restrict__ q,
-                                                          const double* __restrict__ scal, float* __restrict__ r32,
-                                                          Pad g, double* __restrict__ part) {
-    __shared__ double shared[1][32];
-    const int n = g.n;
-    const int xx = blockIdx.x * kTX + threadIdx.x, y = blockIdx.y * kTY + threadIdx.y;
-    const int z0 = blockIdx.z * kTZ, z1 = min(n, z0 + kTZ);
-    const double alpha = scal[3] / scal[2];  // (p, r) / (p, q)
-    double v[1] = {0.0};
-    if (xx < n && y < n)
-        for (int k = z0; k < z1; ++k) {
-            const int64_t i = ((int64_t)k * n + y) * n + xx;
-            x[i] += alpha * p[i];
-            const double rn = r[i] - alpha * q[i];
-            r[i] = rn;
-            r32[g.at(xx, y, k)] = (float)rn;
-            v[0] += rn * rn;
-        }
     block_sums<1>(v, shared);
     if (lin_tid() == 0) part[block_index()] = v[0];
 }
 
-// out[k] = sum over blocks of part[stride * b + k], k < count (fixed order).
-__global__ void finish_kernel(const double* __restrict__ part, int blocks, int stride, int count,
-                              double* __restrict__ out) {
-    __shared__ double shared[3][32];
-    double v[3] = {0.0, 0.0, 0.0};
-    for (int b = threadIdx.x; b < blocks; b += blockDim.x)
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-            if (k < count) v[k] += part[(int64_t)stride * b + k];
-    block_sums<3>(v, shared);
-    if (threadIdx.x == 0)
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-            if (k < count) out[k] = v[k];
-}
-
-// ---- graph-friendly form: one iteration touches the same buffers every time ----
-// p = first ? z : z - beta p, in place (pointwise), beta = scal[0] / scal[2];
-// flags[0] != 0 marks the first step.
-__global__ void __launch_bounds__(kThreads) newdir_kernel(const float* __restrict__ zc, Pad g,
-                                                          double* __restrict__ p, const double* __restrict__ scal,
-                                                          const int* __restrict__ flags) {
-    const int n = g.n;
-    const int x = blockIdx.x * kTX + threadIdx.x, y = blockIdx.y * kTY + threadIdx.y;
-    if (x >= n || y >= n) return;
-    const int z0 = blockIdx.z * kTZ, z1 = min(n, z0 + kTZ);
-    const bool first = flags[0] != 0;
-    const double beta = first ? 0.0 : scal[0] / scal[2];
-    for (int k = z0; k < z1; ++k) {
-        const int64_t i = ((int64_t)k * n + y) * n + x;
-        const double zv = (double)zc[g.at(x, y, k)];
-        p[i] = first ? zv : zv - beta * p[i];
-    }
-}
-
-// q = A p and per-block (p, q), (p, r).
-__global__ void __launch_bounds__(kThreads) matvec_kernel(const double* __restrict__ p, int n,
-                                                          const double* __restrict__ screen,
-                                                          const double* __restrict__ r, double pw,
-                                                          double* __restrict__ q, double* __restrict__ part) {
-    __shared__ double shared[2][32];
-    const int x = blockIdx.x * kTX + threadIdx.x, y = blockIdx.y * kTY + threadIdx.y;
-    const int z0 = blockIdx.z * kTZ, z1 = min(n, z0 + kTZ);
-    const double h = (double)(n - 1), h2 = h * h;
-    const int64_t nn = (int64_t)n * n;
-    double v[2] = {0.0, 0.0};
-    if (x < n && y < n) {
-        const int degxy = (x > 0) + (x + 1 < n) + (y > 0) + (y + 1 < n);
-        for (int k = z0; k < z1; ++k) {
-            const int64_t i = (int64_t)k * nn + (int64_t)y * n + x;
-            double s = 0.0;
-            if (x > 0) s += p[i - 1];
-            if (x + 1 < n) s += p[i + 1];
-            if (y > 0) s += p[i - n];
-            if (y + 1 < n) s += p[i + n];
-            if (k > 0) s += p[i - nn];
-            if (k + 1 < n) s += p[i + nn];
-            const int deg = degxy + (k > 0) + (k + 1 < n);
-            const double pc = p[i];
-            const double qc = ((double)deg * h2 + pw * screen[i] * h2) * pc - s * h2;
-            q[i] = qc;
-            v[0] += pc * qc;
-            v[1] += pc * r[i];
-        }
-    }
-    block_sums<2>(v, shared);
-    if (lin_tid() == 0) {
-        part[2 * block_index()] = v[0];
-        part[2 * block_index() + 1] = v[1];
-    }
+// out[0] = sum over blocks of part[b] (fixed order).
+__global__ void sum_kernel(const double* __restrict__ part, int blocks, double* __restrict__ out) {
+    __shared__ double shared[1][32];
+    double v[1] = {0.0};
+    for (int b = threadIdx.x; b < blocks; b += blockDim.x) v[0] += part[b];
+    block_sums<1>(v, shared);
+    if (threadIdx.x == 0) out[0] = v[0];
 }
 
 // End of one iteration: record ||r||^2, count it, clear the first-step flag
@@ -259,78 +230,54 @@ using namespace pb;
 
 extern "C" size_t pb_fcg_workspace_size(int64_t n) {
     if (n < 2) n = 2;
-    return (size_t)fcg::blocks_of((int)n) * 2 * sizeof(double) + 256;
+    return (size_t)fcg::blocks_of((int)n) * 4 * sizeof(double) + 256;
 }
 
-// One FCG(1) step after the preconditioner produced z (padded FP32):
-//   scal (device, 5 doubles): [0] (z, q_prev)  [2] (p, q)  [3] (p, r)
-//                             [4] ||r||^2 after the step  ([1] unused)
-// p_prev -> p and q are dense FP64; on the first step p_prev may be NULL.
-// Writes x, r (FP64), r32 (padded FP32 copy of r) and scal[0..4]; p_prev and p
-// must differ (the direction is formed from neighbours of p_prev).
-extern "C" int pb_fcg_step_f64(const float* z, const double* p_prev, double* p, double* q, double* x, double* r,
-                               float* r32, const double* screen, int64_t n, double point_weight, double* scal,
-                               int64_t first, void* workspace, size_t workspace_bytes, void* stream) {
-    using namespace pb::fcg;
-    if (n < 2 || n > 4097 || !z || !p || !q || !x || !r || !r32 || !screen || !scal || (!first && !p_prev))
-        return fail(PB_ERR_INVALID, "fcg step: bad args");
-    if (p == p_prev) return fail(PB_ERR_INVALID, "fcg step: p must not alias p_prev");
-    const unsigned blocks = blocks_of((int)n);
-    if (!workspace || workspace_bytes < (size_t)blocks * 2 * sizeof(double))
-        return fail(PB_ERR_WORKSPACE, "fcg step: workspace needs %zu bytes", pb_fcg_workspace_size(n));
-    double* part = (double*)workspace;
-    cudaStream_t s = (cudaStream_t)stream;
-    const dim3 grid = grid_of((int)n), block(kTX, kTY);
-    const Pad g = pad_of((int)n);
-    if (!first) {
-        dot_zq_kernel<<<grid, block, 0, s>>>(z, g, q, part);  // q still holds q_prev here
-        PB_CHECK_LAUNCH("fcg dot_zq_kernel");
-        finish_kernel<<<1, 1024, 0, s>>>(part, (int)blocks, 1, 1, scal + 0);
-        PB_CHECK_LAUNCH("fcg finish_kernel");
-        direction_kernel<false><<<grid, block, 0, s>>>(z, g, p_prev, scal, screen, r, point_weight, p, q, part);
-    } else {
-        direction_kernel<true><<<grid, block, 0, s>>>(z, g, nullptr, scal, screen, r, point_weight, p, q, part);
-    }
-    PB_CHECK_LAUNCH("fcg direction_kernel");
-    finish_kernel<<<1, 1024, 0, s>>>(part, (int)blocks, 2, 2, scal + 2);
-    PB_CHECK_LAUNCH("fcg finish_kernel");
-    update_kernel<<<grid, block, 0, s>>>(x, r, p, q, scal, r32, g, part);
-    PB_CHECK_LAUNCH("fcg update_kernel");
-    finish_kernel<<<1, 1024, 0, s>>>(part, (int)blocks, 1, 1, scal + 4);
-    PB_CHECK_LAUNCH("fcg finish_kernel");
+static int fcg_check(int64_t n, size_t workspace_bytes, const void* workspace) {
+    if (!workspace || workspace_bytes < (size_t)pb::fcg::blocks_of((int)n) * 4 * sizeof(double))
+        return fail(PB_ERR_WORKSPACE, "fcg: workspace needs %zu bytes", pb_fcg_workspace_size(n));
     return PB_OK;
 }
 
-// Graph-friendly FCG(1) step: the direction is updated in place (pointwise),
-// then q = A p, alpha, and the x / r update; flags[0] selects the first step.
-// Every call touches the same buffers, so the step can be captured in a graph.
-extern "C" int pb_fcg_step_inplace_f64(const float* z, double* p, double* q, double* x, double* r, float* r32,
-                                       const double* screen, int64_t n, double point_weight, double* scal,
-                                       const int* flags, void* workspace, size_t workspace_bytes, void* stream) {
+// FCG(1) pass 1 after the preconditioner produced z (padded FP32): the step's
+// scalars into scal[0..3] (scal[0] holds the previous (p, Ap) on entry).
+// p0/p1: the two dense FP64 direction buffers, p_prev = p[flags[1] & 1];
+// r32: the padded FP32 residual the preconditioner read.
+extern "C" int pb_fcg_direction_f64(const float* z, const double* p0, const double* p1, const float* r32,
+                                    const double* screen, int64_t n, double point_weight, double* scal,
+                                    const int* flags, void* workspace, size_t workspace_bytes, void* stream) {
     using namespace pb::fcg;
-    if (n < 2 || n > 4097 || !z || !p || !q || !x || !r || !r32 || !screen || !scal || !flags)
-        return fail(PB_ERR_INVALID, "fcg step: bad args");
-    const unsigned blocks = blocks_of((int)n);
-    if (!workspace || workspace_bytes < (size_t)blocks * 2 * sizeof(double))
-        return fail(PB_ERR_WORKSPACE, "fcg step: workspace needs %zu bytes", pb_fcg_workspace_size(n));
+    if (n < 2 || n > 4097 || !z || !p0 || !p1 || p0 == p1 || !r32 || !screen || !scal || !flags)
+        return fail(PB_ERR_INVALID, "fcg direction: bad args");
+    PB_TRY(fcg_check(n, workspace_bytes, workspace));
     double* part = (double*)workspace;
     cudaStream_t s = (cudaStream_t)stream;
-    const dim3 grid = grid_of((int)n), block(kTX, kTY);
-    const Pad g = pad_of((int)n);
-    dot_zq_kernel<<<grid, block, 0, s>>>(z, g, q, part);  // q holds q_prev (ignored on the first step)
-    PB_CHECK_LAUNCH("fcg dot_zq_kernel");
-    finish_kernel<<<1, 1024, 0, s>>>(part, (int)blocks, 1, 1, scal + 0);
-    PB_CHECK_LAUNCH("fcg finish_kernel");
-    newdir_kernel<<<grid, block, 0, s>>>(z, g, p, scal, flags);
-    PB_CHECK_LAUNCH("fcg newdir_kernel");
-    matvec_kernel<<<grid, block, 0, s>>>(p, (int)n, screen, r, point_weight, q, part);
-    PB_CHECK_LAUNCH("fcg matvec_kernel");
-    finish_kernel<<<1, 1024, 0, s>>>(part, (int)blocks, 2, 2, scal + 2);
-    PB_CHECK_LAUNCH("fcg finish_kernel");
-    update_kernel<<<grid, block, 0, s>>>(x, r, p, q, scal, r32, g, part);
-    PB_CHECK_LAUNCH("fcg update_kernel");
-    finish_kernel<<<1, 1024, 0, s>>>(part, (int)blocks, 1, 1, scal + 4);
-    PB_CHECK_LAUNCH("fcg finish_kernel");
+    direction_sums_kernel<<<grid_of((int)n), dim3(kTX, kTY), 0, s>>>(z, pad_of((int)n), p0, p1, r32, screen,
+                                                                     point_weight, flags, part);
+    PB_CHECK_LAUNCH("fcg direction_sums_kernel");
+    direction_finish_kernel<<<1, 1024, 0, s>>>(part, (int)blocks_of((int)n), flags, scal);
+    PB_CHECK_LAUNCH("fcg direction_finish_kernel");
+    return PB_OK;
+}
+
+// FCG(1) pass 2: p_new, x_new = x + alpha p_new and the true residual
+// r = b - A x_new into r32, scal[4] = ||r||^2.  Iterate and direction buffers
+// alternate by parity of flags[1]: x[it & 1] -> x[(it+1) & 1].
+extern "C" int pb_fcg_update_f64(const float* z, double* p0, double* p1, double* x0, double* x1, const double* b,
+                                 const double* screen, float* r32, int64_t n, double point_weight, double* scal,
+                                 const int* flags, void* workspace, size_t workspace_bytes, void* stream) {
+    using namespace pb::fcg;
+    if (n < 2 || n > 4097 || !z || !p0 || !p1 || p0 == p1 || !x0 || !x1 || x0 == x1 || !b || !screen || !r32 ||
+        !scal || !flags)
+        return fail(PB_ERR_INVALID, "fcg update: bad args");
+    PB_TRY(fcg_check(n, workspace_bytes, workspace));
+    double* part = (double*)workspace;
+    cudaStream_t s = (cudaStream_t)stream;
+    update_residual_kernel<<<grid_of((int)n), dim3(kTX, kTY), 0, s>>>(z, pad_of((int)n), p0, p1, x0, x1, b, screen,
+                                                                      point_weight, scal, flags, r32, part);
+    PB_CHECK_LAUNCH("fcg update_residual_kernel");
+    sum_kernel<<<1, 1024, 0, s>>>(part, (int)blocks_of((int)n), scal + 4);
+    PB_CHECK_LAUNCH("fcg sum_kernel");
     return PB_OK;
 }
 

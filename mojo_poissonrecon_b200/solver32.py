@@ -7,7 +7,8 @@ flexible conjugate gradients:
     r = b - A x                              FP64 (pb_defect_f64)
     while ||r|| > tol * ||b||:               evaluated on the device
         z = V-cycle on A e = r, e = 0        FP32
-        p = z - beta p;  q = A p;  x += alpha p;  r -= alpha q      FP64 (pb_fcg_step_inplace_f64)
+        p = z - beta p;  x += alpha p;  r = b - A x                 FP64 (pb_fcg_direction_f64,
+                                                                         pb_fcg_update_f64)
 
 One iteration touches the same buffers every time, so the engine captures it
 once as the body of a CUDA graph WHILE node whose condition a device kernel
@@ -218,7 +219,9 @@ class RefinedEngine:
     def _allocate(self, n: int, device: torch.device) -> None:
         self.h = Hierarchy32(n, device)
         f64 = lambda: torch.empty((n, n, n), dtype=torch.float64, device=device)
-        self.screen, self.x, self.r, self.p, self.q = f64(), f64(), f64(), f64(), f64()
+        self.screen, self.b = f64(), f64()
+        self.xs = (f64(), f64())  # iterate, alternating by iteration parity
+        self.ps = (f64(), f64())  # search direction, alternating by iteration parity
         self.scal = torch.zeros(8, dtype=torch.float64, device=device)
         self.ctrl = torch.zeros(2, dtype=torch.float64, device=device)
         self.flags = torch.zeros(4, dtype=torch.int32, device=device)
@@ -242,16 +245,21 @@ class RefinedEngine:
             pass
 
     def nbytes(self) -> int:
-        return sum(t.numel() * t.element_size() for t in (self.screen, self.x, self.r, self.p, self.q)) + \
+        return sum(t.numel() * t.element_size() for t in (self.screen, self.b) + self.xs + self.ps) + \
             self.h.nbytes()
 
     def _iteration(self, handle: int) -> None:
         L, s = self.lib, nat.stream_handle()
         z = self.h.v_cycle(0)
-        nat.check(L.pb_fcg_step_inplace_f64(z.data_ptr(), self.p.data_ptr(), self.q.data_ptr(), self.x.data_ptr(),
-                                            self.r.data_ptr(), self.h.levels[0].rhs.data_ptr(),
-                                            self.screen.data_ptr(), self.n, self.pw, self.scal.data_ptr(),
-                                            self.flags.data_ptr(), self.ws_ptr, self.ws_size, s), "fcg step")
+        r32 = self.h.levels[0].rhs
+        p0, p1 = (t.data_ptr() for t in self.ps)
+        x0, x1 = (t.data_ptr() for t in self.xs)
+        nat.check(L.pb_fcg_direction_f64(z.data_ptr(), p0, p1, r32.data_ptr(), self.screen.data_ptr(), self.n,
+                                         self.pw, self.scal.data_ptr(), self.flags.data_ptr(), self.ws_ptr,
+                                         self.ws_size, s), "fcg direction")
+        nat.check(L.pb_fcg_update_f64(z.data_ptr(), p0, p1, x0, x1, self.b.data_ptr(), self.screen.data_ptr(),
+                                      r32.data_ptr(), self.n, self.pw, self.scal.data_ptr(), self.flags.data_ptr(),
+                                      self.ws_ptr, self.ws_size, s), "fcg update")
         nat.check(L.pb_loop_condition(handle, self.scal.data_ptr(), self.ctrl.data_ptr(), self.flags.data_ptr(),
                                       MAX_ITER, self.history.data_ptr(), s), "loop condition")
 
@@ -272,13 +280,17 @@ class RefinedEngine:
         nat.check(L.pb_loop_capture_end(s, self.graph, ctypes.byref(self.exec)), "loop capture end")
         self.body_launches = L.pb_launch_count() - before
 
-    def _start(self, rhs: torch.Tensor) -> None:
-        """x = 0.5, r = b - A x (FP64 and its FP32 copy), ||r||^2."""
+    def _start(self) -> None:
+        """x[0] = 0.5, r = b - A x (its FP32 copy for the first V-cycle), ||r||^2;
+        iteration counter and first-step flag reset."""
         L, s = self.lib, nat.stream_handle()
-        nat.check(L.pb_fill_f64(self.x.data_ptr(), self.x.numel(), 0.5, s), "fill")  # core.py:270
-        nat.check(L.pb_defect_f64(self.x.data_ptr(), None, None, rhs.data_ptr(), self.screen.data_ptr(), self.n,
-                                  self.pw, self.h.levels[0].rhs.data_ptr(), self.r.data_ptr(),
-                                  self.norm2.data_ptr(), self.ws_ptr, self.ws_size, s), "defect")
+        x0 = self.xs[0]
+        nat.check(L.pb_fill_f64(x0.data_ptr(), x0.numel(), 0.5, s), "fill")  # core.py:270
+        nat.check(L.pb_defect_f64(x0.data_ptr(), None, None, self.b.data_ptr(), self.screen.data_ptr(), self.n,
+                                  self.pw, self.h.levels[0].rhs.data_ptr(), None, self.norm2.data_ptr(),
+                                  self.ws_ptr, self.ws_size, s), "defect")
+        self.flags.zero_()
+        self.flags[0] = 1
 
     def solve(self, rhs: torch.Tensor, screen: torch.Tensor, tol: float,
               max_cycles: int) -> tuple[torch.Tensor, SolveStats]:
@@ -287,46 +299,44 @@ class RefinedEngine:
         caller = torch.cuda.current_stream(self.device)
         self.stream.wait_stream(caller)
         with torch.cuda.stream(self.stream):
-            stats = self._solve(rhs, screen, tol, max_cycles)
+            x, stats = self._solve(rhs, screen, tol, max_cycles)
+            x = x.clone()
         caller.wait_stream(self.stream)
-        return self.x.clone(), stats
+        return x, stats
 
-    def _solve(self, rhs: torch.Tensor, screen: torch.Tensor, tol: float, max_cycles: int) -> SolveStats:
+    def _solve(self, rhs: torch.Tensor, screen: torch.Tensor, tol: float, max_cycles: int):
         L, s = self.lib, nat.stream_handle()
         stats = SolveStats()
         self.screen.copy_(screen)
+        self.b.copy_(rhs)
         self.h.setup(self.screen, self.pw)
-        self._start(rhs)
-        norm(rhs, self.norm_ws, self.bnorm)
+        self._start()
+        norm(self.b, self.norm_ws, self.bnorm)
         both = torch.cat([self.norm2, self.bnorm]).cpu()
         stats.rhs_norm = float(both[1])
         r = math.sqrt(max(float(both[0]), 0.0))
         stats.history.append(r)
+        stats.residual_norm = r
         target = tol * stats.rhs_norm
+        it = 0
         if r > target and max_cycles > 0:
             self.ctrl.copy_(torch.tensor([target * target, float(max_cycles)], dtype=torch.float64))
             if not self.exec.value:
                 # one eager iteration first sets kernel attributes outside the
                 # capture; its effect is discarded by restarting below
-                self.flags.zero_()
-                self.flags[0] = 1
                 self._iteration(0)
-                self._start(rhs)
+                self._start()
                 self._capture()
-            self.flags.zero_()
-            self.flags[0] = 1
             nat.check(L.pb_graph_launch(self.exec, s), "graph launch")
-            it = int(self.flags[1].item())
+            tail = torch.cat([self.flags[1:2].to(torch.float64), self.scal[4:5]]).cpu()
+            it = int(tail[0])
             L.pb_note_launches(it * self.body_launches)
             stats.cycles = it
             stats.history.extend(math.sqrt(max(v, 0.0)) for v in self.history[:it].cpu().tolist())
-        # the recurrence r -= alpha q drifts from b - A x by rounding; report the true residual
-        nat.check(L.pb_defect_f64(self.x.data_ptr(), None, None, rhs.data_ptr(), self.screen.data_ptr(), self.n,
-                                  self.pw, self.h.levels[0].rhs.data_ptr(), None, self.norm2.data_ptr(),
-                                  self.ws_ptr, self.ws_size, s), "defect")
-        stats.residual_norm = math.sqrt(max(float(self.norm2.item()), 0.0))
+            # pass 2 computes the true residual b - A x of every iterate
+            stats.residual_norm = math.sqrt(max(float(tail[1]), 0.0))
         self.h.check_status()
-        return stats
+        return self.xs[it & 1], stats
 
 
 _ENGINES: "collections.OrderedDict[tuple, RefinedEngine]" = collections.OrderedDict()
