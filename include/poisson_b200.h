@@ -240,6 +240,21 @@ int pb_graph_destroy(void *exec, void *graph);
 /* Adds launches that ran inside graphs to pb_launch_count(). */
 int pb_note_launches(long long count);
 
+/* Extraction for reconstruct(): the mesh pb_dual_vertices_f64 +
+ * pb_dual_faces_f64 give (same vertices, densities and faces, same order,
+ * bit-identical), from sign bits and rank structures instead of a dense cell
+ * map (no counterpart in the reference, whose extraction is
+ * capi.mojo:798-1129).  Count first (counts[0] = vertices, counts[1] =
+ * triangles, device int64), then emit with the same field, side, iso and
+ * workspace; emit's vertices (with vertex_density) or faces may be NULL when
+ * their count is 0 and are then not written.  Sides 2..1025. */
+size_t pb_extract_workspace_size(int64_t n);
+int pb_extract_count_f64(const double *field, int64_t n, const double *iso, int64_t *counts, void *workspace,
+                         size_t workspace_bytes, void *stream);
+int pb_extract_emit_f64(const double *field, const double *density, int64_t n, const double *iso, double *vertices,
+                        double *vertex_density, int64_t *faces, void *workspace, size_t workspace_bytes,
+                        void *stream);
+
 /* ---- FP32 preconditioner levels (no counterpart in the reference) ----------
  * The reference's V-cycle (core.py:141-193) rediscretises coarse levels; the
  * FP32 preconditioner of the refined solvers uses Galerkin coarse levels

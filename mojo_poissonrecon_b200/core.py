@@ -307,10 +307,31 @@ def solve_screened_poisson(
 
 # ---- extraction (core.py:309-374) --------------------------------------------
 
+EXTRACT_FAST_MAX_SIDE = 1025
+
+
 def _extract_device(ctx: _Context, field: torch.Tensor, density: torch.Tensor, iso: torch.Tensor):
-    """Two-pass dual contouring on device tensors; returns (vertices, faces, vdens)."""
+    """Dual contouring on device tensors; returns (vertices, faces, vdens).
+
+    Sides up to 1025 use the bit-array extraction (count, one host read of the
+    two counts, emit); larger ones the reference-shaped two-pass entry points.
+    Both give the reference's mesh (capi.mojo:798-1129) bit for bit."""
     L = ctx.lib
     n = field.shape[0]
+    if n <= EXTRACT_FAST_MAX_SIDE:
+        ptr, size = ctx.ws.get(L.pb_extract_workspace_size(n))
+        counts = torch.empty(2, dtype=torch.int64, device=ctx.device)
+        ctx.check(L.pb_extract_count_f64(field.data_ptr(), n, iso.data_ptr(), counts.data_ptr(), ptr, size,
+                                         ctx.stream), "extract count")
+        nv, nf = (int(v) for v in counts.cpu())
+        vertices = torch.empty((nv, 3), dtype=torch.float64, device=ctx.device)
+        vdens = torch.empty(nv, dtype=torch.float64, device=ctx.device)
+        faces = torch.empty((nf, 3), dtype=torch.int64, device=ctx.device)
+        if nv:
+            ctx.check(L.pb_extract_emit_f64(field.data_ptr(), density.data_ptr(), n, iso.data_ptr(),
+                                            vertices.data_ptr(), vdens.data_ptr(), faces.data_ptr() if nf else None,
+                                            ptr, size, ctx.stream), "extract emit")
+        return vertices, faces, vdens
     cells = n - 1
     ptr, size = ctx.ws.get(L.pb_dual_workspace_size(n))
     count = torch.zeros(1, dtype=torch.int64, device=ctx.device)

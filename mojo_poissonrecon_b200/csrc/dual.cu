@@ -65,6 +65,50 @@ __device__ __forceinline__ int edge_root(double v0, double v1, double iso, doubl
     return 1;
 }
 
+// Vertex of active cell (x, y, z): the mean of its edge roots (capi.mojo:964-1033),
+// and the mean density of its corners.
+__device__ __forceinline__ void cell_vertex(const double* __restrict__ field, const double* __restrict__ density,
+                                            int64_t n, int64_t x, int64_t y, int64_t z, double iso, double cells_d,
+                                            double* __restrict__ out, double* __restrict__ dens) {
+    double v[8];
+#pragma unroll
+    for (int corner = 0; corner < 8; ++corner)
+        v[corner] = field[grid_index(x + (corner & 1), y + ((corner >> 1) & 1), z + ((corner >> 2) & 1), n)];
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    int roots = 0;
+    // x-edges, y-edges, z-edges; within each, (a, b) in row-major order (capi.mojo:968-1023).
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const int c0 = 2 * a + 4 * b;
+            roots += edge_root(v[c0], v[c0 + 1], iso, 0.0, (double)a, (double)b, 1.0, (double)a, (double)b, sx, sy, sz);
+        }
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const int c0 = a + 4 * b;
+            roots += edge_root(v[c0], v[c0 + 2], iso, (double)a, 0.0, (double)b, (double)a, 1.0, (double)b, sx, sy, sz);
+        }
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const int c0 = a + 2 * b;
+            roots += edge_root(v[c0], v[c0 + 4], iso, (double)a, (double)b, 0.0, (double)a, (double)b, 1.0, sx, sy, sz);
+        }
+    const double inv_roots = 1.0 / (double)roots;
+    out[0] = ((double)x + sx * inv_roots) / cells_d;
+    out[1] = ((double)y + sy * inv_roots) / cells_d;
+    out[2] = ((double)z + sz * inv_roots) / cells_d;
+    double dsum = 0.0;
+#pragma unroll
+    for (int corner = 0; corner < 8; ++corner)
+        dsum += density[grid_index(x + (corner & 1), y + ((corner >> 1) & 1), z + ((corner >> 2) & 1), n)];
+    *dens = dsum * 0.125;
+}
+
 __global__ void __launch_bounds__(kDualThreads) vertex_emit_kernel(const double* __restrict__ field,
                                                                    const double* __restrict__ density, int64_t n,
                                                                    IsoArg iso_arg,
@@ -106,43 +150,7 @@ __global__ void __launch_bounds__(kDualThreads) vertex_emit_kernel(const double*
             continue;
         }
         const int64_t x = i % cells, y = (i / cells) % cells, z = i / (cells * cells);
-        double v[8];
-#pragma unroll
-        for (int corner = 0; corner < 8; ++corner)
-            v[corner] = field[grid_index(x + (corner & 1), y + ((corner >> 1) & 1), z + ((corner >> 2) & 1), n)];
-        double sx = 0.0, sy = 0.0, sz = 0.0;
-        int roots = 0;
-        // x-edges, y-edges, z-edges; within each, (a, b) in row-major order (capi.mojo:968-1023).
-#pragma unroll
-        for (int a = 0; a < 2; ++a)
-#pragma unroll
-            for (int b = 0; b < 2; ++b) {
-                const int c0 = 2 * a + 4 * b;
-                roots += edge_root(v[c0], v[c0 + 1], iso, 0.0, (double)a, (double)b, 1.0, (double)a, (double)b, sx, sy, sz);
-            }
-#pragma unroll
-        for (int a = 0; a < 2; ++a)
-#pragma unroll
-            for (int b = 0; b < 2; ++b) {
-                const int c0 = a + 4 * b;
-                roots += edge_root(v[c0], v[c0 + 2], iso, (double)a, 0.0, (double)b, (double)a, 1.0, (double)b, sx, sy, sz);
-            }
-#pragma unroll
-        for (int a = 0; a < 2; ++a)
-#pragma unroll
-            for (int b = 0; b < 2; ++b) {
-                const int c0 = a + 2 * b;
-                roots += edge_root(v[c0], v[c0 + 4], iso, (double)a, (double)b, 0.0, (double)a, (double)b, 1.0, sx, sy, sz);
-            }
-        const double inv_roots = 1.0 / (double)roots;
-        vertices[3 * id] = ((double)x + sx * inv_roots) / cells_d;
-        vertices[3 * id + 1] = ((double)y + sy * inv_roots) / cells_d;
-        vertices[3 * id + 2] = ((double)z + sz * inv_roots) / cells_d;
-        double dsum = 0.0;
-#pragma unroll
-        for (int corner = 0; corner < 8; ++corner)
-            dsum += density[grid_index(x + (corner & 1), y + ((corner >> 1) & 1), z + ((corner >> 2) & 1), n)];
-        vertex_density[id] = dsum * 0.125;
+        cell_vertex(field, density, n, x, y, z, iso, cells_d, vertices + 3 * id, vertex_density + id);
         cell_map[i] = id;
         ++id;
     }
@@ -335,6 +343,260 @@ static int dual_faces(const double* field, int64_t n, IsoArg iso, const int64_t*
     return PB_OK;
 }
 
+
+// ---- extraction for reconstruct(): sign bits and rank structures ----------------
+// Same output, order and arithmetic as the two-pass kernels above, but the
+// passes over all cells and edges read a bit per node (field < iso) instead of
+// the FP64 field, and vertex ids are ranks in a bit array of active cells
+// (prefix sum per 32-cell word + popcount) instead of a dense cell map.  Only
+// active cells read field and density values.  Sides up to 1025 (32-bit
+// node, cell and per-sweep edge indices).
+namespace fast {
+
+constexpr int kT = 256;
+constexpr int64_t kMaxSide = 1025;
+
+__device__ __forceinline__ uint32_t bit_at(const uint32_t* __restrict__ bits, uint32_t i) {
+    return (bits[i >> 5] >> (i & 31)) & 1u;
+}
+__device__ __forceinline__ uint32_t lanes_below(uint32_t word, uint32_t b) { return __popc(word & ((1u << b) - 1u)); }
+
+// bits: bit b of word w = (field[32w + b] < iso).
+__global__ void __launch_bounds__(kT) sign_bits_kernel(const double* __restrict__ field, uint32_t nodes, IsoArg iso_arg,
+                                                       uint32_t* __restrict__ bits) {
+    const double iso = iso_arg.get();
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i - lane < nodes; i += stride) {
+        const uint32_t m = __ballot_sync(0xffffffffu, i < nodes && field[i] < iso);
+        if (lane == 0) bits[i >> 5] = m;
+    }
+}
+
+// active cells (corners on both sides, capi.mojo:946-960) as bits, and the
+// popcount of each 32-cell word (scanned in place into the word's first id).
+__global__ void __launch_bounds__(kT) cell_words_kernel(const uint32_t* __restrict__ bits, uint32_t n,
+                                                        uint32_t cells3, uint32_t* __restrict__ active,
+                                                        uint32_t* __restrict__ counts) {
+    const uint32_t c = n - 1, nn = n * n, lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i - lane < cells3; i += stride) {
+        bool a = false;
+        if (i < cells3) {
+            const uint32_t ci = (uint32_t)i, x = ci % c, t = ci / c, y = t % c, z = t / c;
+            const uint32_t i0 = (z * n + y) * n + x;
+            const uint32_t below = bit_at(bits, i0) + bit_at(bits, i0 + 1) + bit_at(bits, i0 + n) +
+                                   bit_at(bits, i0 + n + 1) + bit_at(bits, i0 + nn) + bit_at(bits, i0 + nn + 1) +
+                                   bit_at(bits, i0 + nn + n) + bit_at(bits, i0 + nn + n + 1);
+            a = below != 0 && below != 8;
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, a);
+        if (lane == 0) {
+            active[i >> 5] = m;
+            counts[i >> 5] = __popc(m);
+        }
+    }
+}
+
+// Edge `local` of sweep s (capi.mojo:1090-1128): its lower node; sweep order z, y, x.
+__device__ __forceinline__ void sweep_edge(int s, uint32_t local, uint32_t c, uint32_t& x, uint32_t& y, uint32_t& z) {
+    const uint32_t cm1 = c - 1;
+    if (s == 0) {  // x-edges: z, y in [1, c), x in [0, c)
+        x = local % c;
+        const uint32_t t = local / c;
+        y = 1 + t % cm1;
+        z = 1 + t / cm1;
+    } else if (s == 1) {  // y-edges: z in [1, c), y in [0, c), x in [1, c)
+        x = 1 + local % cm1;
+        const uint32_t t = local / cm1;
+        y = t % c;
+        z = 1 + t / c;
+    } else {  // z-edges: z in [0, c), y, x in [1, c)
+        x = 1 + local % cm1;
+        const uint32_t t = local / cm1;
+        y = 1 + t % cm1;
+        z = t / cm1;
+    }
+}
+
+// Sign-changing edges of the three sweeps as bits (word w of sweep s at
+// s * words + w) and per-word popcounts.  An interior edge that changes sign
+// lies on four active cells, so it always yields a quad.
+__global__ void __launch_bounds__(kT) edge_words_kernel(const uint32_t* __restrict__ bits, uint32_t n,
+                                                        uint32_t per_sweep, uint32_t words,
+                                                        uint32_t* __restrict__ fwords, uint32_t* __restrict__ counts) {
+    const int s = blockIdx.y;
+    const uint32_t c = n - 1, lane = threadIdx.x & 31;
+    const uint32_t step = s == 0 ? 1u : (s == 1 ? n : n * n);
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e - lane < per_sweep; e += stride) {
+        bool a = false;
+        if (e < per_sweep) {
+            uint32_t x, y, z;
+            sweep_edge(s, (uint32_t)e, c, x, y, z);
+            const uint32_t i0 = (z * n + y) * n + x;
+            a = bit_at(bits, i0) != bit_at(bits, i0 + step);
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, a);
+        if (lane == 0) {
+            fwords[(uint64_t)s * words + (e >> 5)] = m;
+            counts[(uint64_t)s * words + (e >> 5)] = __popc(m);
+        }
+    }
+}
+
+__global__ void store_counts_kernel(const uint32_t* __restrict__ totals, int64_t* __restrict__ counts) {
+    counts[0] = totals[0];
+    counts[1] = 2 * (int64_t)totals[1];  // two triangles per quad
+}
+
+// One thread per 32-cell word: each active cell's vertex at id = its rank.
+__global__ void __launch_bounds__(kT) vertex_words_kernel(const double* __restrict__ field,
+                                                          const double* __restrict__ density, uint32_t n,
+                                                          IsoArg iso_arg, const uint32_t* __restrict__ active,
+                                                          const uint32_t* __restrict__ first, uint32_t cell_words,
+                                                          double* __restrict__ vertices,
+                                                          double* __restrict__ vertex_density) {
+    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= cell_words) return;
+    uint32_t m = active[w];
+    if (!m) return;
+    const double iso = iso_arg.get();
+    const uint32_t c = n - 1;
+    const double cells_d = (double)c;
+    uint32_t id = first[w];
+    while (m) {
+        const uint32_t b = __ffs(m) - 1;
+        m &= m - 1;
+        const uint32_t ci = 32 * w + b, x = ci % c, t = ci / c, y = t % c, z = t / c;
+        cell_vertex(field, density, n, x, y, z, iso, cells_d, vertices + 3 * (int64_t)id, vertex_density + id);
+        ++id;
+    }
+}
+
+__device__ __forceinline__ int64_t cell_id(const uint32_t* __restrict__ active, const uint32_t* __restrict__ first,
+                                           uint32_t ci) {
+    return (int64_t)first[ci >> 5] + lanes_below(active[ci >> 5], ci & 31);
+}
+
+// One thread per 32-edge word: each sign-changing edge's two triangles at
+// quad = its rank (capi.mojo:1040-1071).
+__global__ void __launch_bounds__(kT) face_words_kernel(const uint32_t* __restrict__ bits, uint32_t n,
+                                                        uint32_t words, const uint32_t* __restrict__ fwords,
+                                                        const uint32_t* __restrict__ ffirst,
+                                                        const uint32_t* __restrict__ active,
+                                                        const uint32_t* __restrict__ first,
+                                                        int64_t* __restrict__ faces) {
+    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= words) return;
+    const int s = blockIdx.y;
+    uint32_t m = fwords[(uint64_t)s * words + w];
+    if (!m) return;
+    const uint32_t c = n - 1;
+    int64_t quad = ffirst[(uint64_t)s * words + w];
+    while (m) {
+        const uint32_t b = __ffs(m) - 1;
+        m &= m - 1;
+        uint32_t x, y, z;
+        sweep_edge(s, 32 * w + b, c, x, y, z);
+        const bool reverse = bit_at(bits, (z * n + y) * n + x) != 0;
+        uint32_t q[4];
+        if (s == 0) {
+            q[0] = (uint32_t)grid_index(x, y - 1, z - 1, c);
+            q[1] = (uint32_t)grid_index(x, y, z - 1, c);
+            q[2] = (uint32_t)grid_index(x, y, z, c);
+            q[3] = (uint32_t)grid_index(x, y - 1, z, c);
+        } else if (s == 1) {
+            q[0] = (uint32_t)grid_index(x - 1, y, z - 1, c);
+            q[1] = (uint32_t)grid_index(x - 1, y, z, c);
+            q[2] = (uint32_t)grid_index(x, y, z, c);
+            q[3] = (uint32_t)grid_index(x, y, z - 1, c);
+        } else {
+            q[0] = (uint32_t)grid_index(x - 1, y - 1, z, c);
+            q[1] = (uint32_t)grid_index(x, y - 1, z, c);
+            q[2] = (uint32_t)grid_index(x, y, z, c);
+            q[3] = (uint32_t)grid_index(x - 1, y, z, c);
+        }
+        const int64_t a = cell_id(active, first, q[0]), bb = cell_id(active, first, q[1]);
+        const int64_t cc = cell_id(active, first, q[2]), d = cell_id(active, first, q[3]);
+        int64_t* out = faces + 6 * quad;
+        if (reverse) {
+            out[0] = a; out[1] = d; out[2] = cc; out[3] = a; out[4] = cc; out[5] = bb;
+        } else {
+            out[0] = a; out[1] = bb; out[2] = cc; out[3] = a; out[4] = cc; out[5] = d;
+        }
+        ++quad;
+    }
+}
+
+inline uint64_t words_of(uint64_t items) { return (items + 31) / 32; }
+
+// Arrays carved from the workspace, identically in count and emit.
+struct Layout {
+    uint32_t n, c, nodes, cells3, cell_words, per_sweep, words;
+    uint32_t *bits, *active, *first, *fwords, *ffirst, *totals;
+    void* base;
+    size_t bytes, used;
+    Workspace scratch() const {  // the scan scratch after the arrays
+        Workspace w(base, bytes);
+        w.used = used;
+        return w;
+    }
+};
+
+template <class W>
+void carve(W& w, uint64_t nodes, uint64_t cell_words, uint64_t words, uint32_t** out) {
+    out[0] = w.template take<uint32_t>(words_of(nodes));
+    out[1] = w.template take<uint32_t>(cell_words);
+    out[2] = w.template take<uint32_t>(cell_words + 1);
+    out[3] = w.template take<uint32_t>(3 * words + 1);
+    out[4] = w.template take<uint32_t>(3 * words + 1);
+    out[5] = w.template take<uint32_t>(2);
+}
+
+inline Layout layout(int64_t n, void* base, size_t bytes) {
+    Layout L{};
+    L.n = (uint32_t)n;
+    L.c = (uint32_t)(n - 1);
+    L.nodes = (uint32_t)(n * n * n);
+    L.cells3 = L.c * L.c * L.c;
+    L.cell_words = (uint32_t)words_of(L.cells3);
+    L.per_sweep = L.c == 0 ? 0 : L.c * (L.c - 1) * (L.c - 1);
+    L.words = (uint32_t)words_of(L.per_sweep);
+    Workspace w(base, bytes);
+    uint32_t* p[6];
+    carve(w, L.nodes, L.cell_words, L.words, p);
+    L.bits = p[0];
+    L.active = p[1];
+    L.first = p[2];
+    L.fwords = p[3];
+    L.ffirst = p[4];
+    L.totals = p[5];
+    L.base = base;
+    L.bytes = bytes;
+    L.used = w.used;
+    return L;
+}
+
+inline size_t workspace_bytes(int64_t n) {
+    return measure([&](Workspace& w) {
+        const uint64_t c = n - 1, nodes = (uint64_t)n * n * n, cells3 = c * c * c;
+        const uint64_t per_sweep = c == 0 ? 0 : c * (c - 1) * (c - 1);
+        const uint64_t cw = words_of(cells3), fw = words_of(per_sweep);
+        uint32_t* p[6];
+        carve(w, nodes, cw, fw, p);
+        scan_carve<uint32_t>(w, (int64_t)(cw > 3 * fw ? cw : 3 * fw));
+    });
+}
+
+inline unsigned grid_for(uint64_t items) {
+    uint64_t b = (items + kT - 1) / kT;
+    const uint64_t cap = (uint64_t)kSMs * 16;
+    return (unsigned)(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+}  // namespace fast
+
 }  // namespace pb
 
 using namespace pb;
@@ -370,4 +632,67 @@ extern "C" int pb_dual_faces_f64_isoptr(const double* field, int64_t n, const do
     if (!iso) return fail(PB_ERR_INVALID, "dual faces: null iso pointer");
     return dual_faces(field, n, IsoArg{0.0, iso}, cell_map, faces, capacity, count, workspace, workspace_bytes,
                       (cudaStream_t)stream);
+}
+
+// ---- extraction for reconstruct() (no counterpart in the reference's C API) ----
+extern "C" size_t pb_extract_workspace_size(int64_t n) { return fast::workspace_bytes(n < 2 ? 2 : n); }
+
+// Counts of the mesh extract_isosurface(field, iso) would give (capi.mojo:
+// 798-1129): counts[0] = vertices, counts[1] = triangles (device int64[2]).
+// Leaves in the workspace the state pb_extract_emit_f64 needs: call emit next
+// with the same field, side, iso and workspace.  Sides 2..1025.
+extern "C" int pb_extract_count_f64(const double* field, int64_t n, const double* iso, int64_t* counts,
+                                    void* workspace, size_t workspace_bytes, void* stream) {
+    if (n < 2 || n > fast::kMaxSide || !field || !iso || !counts) return fail(PB_ERR_INVALID, "extract count: bad args");
+    if (!workspace || workspace_bytes < fast::workspace_bytes(n))
+        return fail(PB_ERR_WORKSPACE, "extract: workspace needs %zu bytes", fast::workspace_bytes(n));
+    cudaStream_t s = (cudaStream_t)stream;
+    fast::Layout L = fast::layout(n, workspace, workspace_bytes);
+    const IsoArg ia{0.0, iso};
+    fast::sign_bits_kernel<<<fast::grid_for(L.nodes), fast::kT, 0, s>>>(field, L.nodes, ia, L.bits);
+    PB_CHECK_LAUNCH("sign_bits_kernel");
+    fast::cell_words_kernel<<<fast::grid_for(L.cells3), fast::kT, 0, s>>>(L.bits, L.n, L.cells3, L.active, L.first);
+    PB_CHECK_LAUNCH("cell_words_kernel");
+    Workspace scan_ws = L.scratch();
+    PB_TRY(exclusive_scan<uint32_t>(L.first, L.first, L.cell_words, L.totals, scan_ws, s));
+    if (L.per_sweep) {
+        fast::edge_words_kernel<<<dim3(fast::grid_for(L.per_sweep), 3), fast::kT, 0, s>>>(L.bits, L.n, L.per_sweep,
+                                                                                           L.words, L.fwords, L.ffirst);
+        PB_CHECK_LAUNCH("edge_words_kernel");
+        Workspace scan_ws2 = L.scratch();
+        PB_TRY(exclusive_scan<uint32_t>(L.ffirst, L.ffirst, 3 * (int64_t)L.words, L.totals + 1, scan_ws2, s));
+    } else {
+        PB_CHECK_CUDA(cudaMemsetAsync(L.totals + 1, 0, sizeof(uint32_t), s), "extract face total");
+    }
+    fast::store_counts_kernel<<<1, 1, 0, s>>>(L.totals, counts);
+    PB_CHECK_LAUNCH("store_counts_kernel");
+    return PB_OK;
+}
+
+// Emits the counted mesh: vertices (counts[0] x 3), vertex_density
+// (counts[0]), faces (counts[1] x 3), in the reference's order, bit-identical
+// to pb_dual_vertices_f64 / pb_dual_faces_f64.  vertices (with
+// vertex_density) or faces may be NULL when their count is 0; they are then
+// not written.
+extern "C" int pb_extract_emit_f64(const double* field, const double* density, int64_t n, const double* iso,
+                                   double* vertices, double* vertex_density, int64_t* faces, void* workspace,
+                                   size_t workspace_bytes, void* stream) {
+    if (n < 2 || n > fast::kMaxSide || !field || !iso || (vertices && (!density || !vertex_density)))
+        return fail(PB_ERR_INVALID, "extract emit: bad args");
+    if (!workspace || workspace_bytes < fast::workspace_bytes(n))
+        return fail(PB_ERR_WORKSPACE, "extract: workspace needs %zu bytes", fast::workspace_bytes(n));
+    cudaStream_t s = (cudaStream_t)stream;
+    fast::Layout L = fast::layout(n, workspace, workspace_bytes);
+    const IsoArg ia{0.0, iso};
+    if (vertices) {
+        fast::vertex_words_kernel<<<(L.cell_words + fast::kT - 1) / fast::kT, fast::kT, 0, s>>>(
+            field, density, L.n, ia, L.active, L.first, L.cell_words, vertices, vertex_density);
+        PB_CHECK_LAUNCH("vertex_words_kernel");
+    }
+    if (faces && L.per_sweep) {
+        fast::face_words_kernel<<<dim3((L.words + fast::kT - 1) / fast::kT, 3), fast::kT, 0, s>>>(
+            L.bits, L.n, L.words, L.fwords, L.ffirst, L.active, L.first, faces);
+        PB_CHECK_LAUNCH("face_words_kernel");
+    }
+    return PB_OK;
 }
