@@ -57,6 +57,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="only the FP32-refined arm (the command the ncu captures run)")
+    ap.add_argument("--eager", action="store_true",
+                    help="with --profile: run the solver's iterations as eager launches (no graph), so that ncu "
+                         "sees every kernel")
     ap.add_argument("--workload", choices=("torus", "batch", "serving", "deep"), default="torus",
                     help="torus: the default line; batch: 256 uneven clouds; serving: Poisson arrivals; "
                          "deep: depth 10")
@@ -137,6 +140,10 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     import mojo_poissonrecon_b200 as mpr
     from mojo_poissonrecon_b200 import _native, solver32
 
+    if args.eager:
+        if not args.profile:
+            raise SystemExit("--eager is a profiling aid: use it with --profile")
+        solver32.EAGER_LOOP = True
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -274,7 +281,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         avg_ms = statistics.mean(sweep_ms)
         algorithmic = 16.0 * n**3  # read e, rhs, 1/D and write e, FP32, per launch
         achieved = algorithmic / (avg_ms / 1e3) / 1e9
-        roofline = {"kernel": "pb::tma::sweep_kernel<false> (fused red-black sweep, level 0, 257^3)",
+        roofline = {"kernel": "pb::tma::sweep_kernel<0, 5> (fused red-black sweep, level 0, 257^3)",
                     "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                     "frac": round(achieved / peak, 4), "peak_source": peak_src,
                     "avg_launch_ms": round(avg_ms, 4), "launches_timed": len(sweep_ms),

@@ -45,6 +45,11 @@ COARSE_N = 17  # levels of this side or smaller: one single-block launch
 COARSE_SWEEPS = 2  # pre- and post-smoothing sweeps on every level below level 0
 MAX_ITER = 512  # capacity of the device iteration history (and hard cap)
 
+# When true, RefinedEngine runs its iterations as eager launches with a host
+# read of the residual after each (the same kernels as the captured loop), for
+# profilers that do not follow kernels inside a graph's conditional node.
+EAGER_LOOP = False
+
 # When set to a list, every finest-level sweep launched eagerly appends
 # (start, end, mode) CUDA events recorded on the launching stream around it.
 PROBE: list | None = None
@@ -321,16 +326,25 @@ class RefinedEngine:
         it = 0
         if r > target and max_cycles > 0:
             self.ctrl.copy_(torch.tensor([target * target, float(max_cycles)], dtype=torch.float64))
-            if not self.exec.value:
-                # one eager iteration first sets kernel attributes outside the
-                # capture; its effect is discarded by restarting below
-                self._iteration(0)
-                self._start()
-                self._capture()
-            nat.check(L.pb_graph_launch(self.exec, s), "graph launch")
+            if EAGER_LOOP:
+                while True:
+                    self._iteration(0)
+                    done = int(self.flags[1].item())
+                    r2 = float(self.scal[4].item())
+                    if not (r2 > target * target and done < min(MAX_ITER, max_cycles)):
+                        break
+            else:
+                if not self.exec.value:
+                    # one eager iteration first sets kernel attributes outside the
+                    # capture; its effect is discarded by restarting below
+                    self._iteration(0)
+                    self._start()
+                    self._capture()
+                nat.check(L.pb_graph_launch(self.exec, s), "graph launch")
             tail = torch.cat([self.flags[1:2].to(torch.float64), self.scal[4:5]]).cpu()
             it = int(tail[0])
-            L.pb_note_launches(it * self.body_launches)
+            if not EAGER_LOOP:
+                L.pb_note_launches(it * self.body_launches)
             stats.cycles = it
             stats.history.extend(math.sqrt(max(v, 0.0)) for v in self.history[:it].cpu().tolist())
             # pass 2 computes the true residual b - A x of every iterate
