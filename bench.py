@@ -483,12 +483,15 @@ def run_deep(args) -> dict:
     import torch
 
     import mojo_poissonrecon_b200 as mpr
-    from mojo_poissonrecon_b200 import workloads
+    from mojo_poissonrecon_b200 import solver32, workloads
 
     pts, nrm = workloads.sphere_union(20_000_000, spheres=64, seed=2)
     dp, dn = torch.from_numpy(pts).cuda(), torch.from_numpy(nrm).cuda()
     out = {}
     for prec in ("fp32_refined", "fp64"):
+        solver32.clear_engines()  # the refined engine (~100 GB at 1025^3) must not outlive its run
+        torch.cuda.empty_cache()
+        torch.cuda.reset_peak_memory_stats()
         mpr.reconstruct(dp[:200_000], dn[:200_000], depth=10, precision=prec, tol=TOL, device_out=True)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -497,11 +500,11 @@ def run_deep(args) -> dict:
         e1.record()
         torch.cuda.synchronize()
         out[prec] = {"ms": round(e0.elapsed_time(e1), 1), "vertices": int(mesh.vertices.shape[0]),
-                     "faces": int(mesh.faces.shape[0]), "residual_norm": mesh.residual_norm}
+                     "faces": int(mesh.faces.shape[0]), "residual_norm": mesh.residual_norm,
+                     "peak_memory_gib": round(torch.cuda.max_memory_allocated() / 2**30, 1)}
     return {"metric": METRIC, "workload": "deep: 20M points on 64 spheres, depth 10 (1025^3), solve to 1e-8, "
                                           "dual contour", "value": round(1e3 / out["fp32_refined"]["ms"], 4),
             "unit": "recons/s", "n_gpus": 1, "fp32_refined": out["fp32_refined"], "fp64": out["fp64"],
-            "peak_memory_gib": round(torch.cuda.max_memory_allocated() / 2**30, 1),
             "data": "synthetic (workloads.sphere_union, seed 2)"}
 
 

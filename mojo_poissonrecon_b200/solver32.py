@@ -58,10 +58,11 @@ PROBE: list | None = None
 class Level32:
     """Padded FP32 arrays of one level (zero-filled so the ghosts stay zero).
 
-    Every level has work arrays (rhs, res, ea, eb), 1/diagonal (invD) and its
+    Every level has work arrays (rhs, ea, eb), 1/diagonal (invD) and its
     prolongation weights (weights).  Level 0 also keeps the reference's
     7-point operator as its diagonal D.  Levels that run the 27-point kernels
-    (all but a level 0 of side >= 33) hold their operator as 14 planes `coef`."""
+    (all but a level 0 of side >= 33) hold their operator as 14 planes `coef`
+    and a residual array `res`."""
 
     def __init__(self, n: int, device: torch.device, lib, first: bool):
         self.n = n
@@ -72,8 +73,10 @@ class Level32:
         def zeros(*lead):
             return torch.zeros(*lead, self.count, dtype=torch.float32, device=device)
 
-        self.invD, self.rhs, self.res, self.ea, self.eb, self.weights = (zeros() for _ in range(6))
         self.seven = first and n > COARSE_N
+        self.invD, self.rhs, self.ea, self.eb, self.weights = (zeros() for _ in range(5))
+        # level 0's residual is fused into its restriction; 27-point levels store theirs
+        self.res = None if self.seven else zeros()
         self.D = zeros() if first else None
         self.coef = None if self.seven else zeros(14)
 
