@@ -268,12 +268,9 @@ __global__ void __launch_bounds__(32) coarse_inverse_kernel(const float* __restr
     }
     __syncwarp();
     for (int k = 0; k < kInvN; ++k) {
-        const double piv = a[k][k];
+        const double inv_piv = 1.0 / a[k][k];
         __syncwarp();
-        if (lane == k) {
-            a[k][k] = 1.0;
-            for (int j = 0; j < kInvN; ++j) a[k][j] /= piv;
-        }
+        if (lane < kInvN) a[k][lane] = lane == k ? inv_piv : a[k][lane] * inv_piv;  // row k / pivot, in parallel
         __syncwarp();
         if (lane < kInvN && lane != k) {
             const double f = a[lane][k];

@@ -118,7 +118,10 @@ __global__ void sum_partials_kernel(const double* __restrict__ partial, int coun
 // ring in shared memory, plane 2zc+1 being reused as plane 2(zc+1)-1 of the
 // next coarse plane.  Out-of-grid ring entries are zero, so the restriction
 // sums all 27 entries with weights (1,2,1)^3 / 64.
-constexpr int kRrCX = 32, kRrCY = 4, kRrCZ = 8;
+#ifndef PB_RR_CZ
+#define PB_RR_CZ 8  // coarse planes per block
+#endif
+constexpr int kRrCX = 32, kRrCY = 4, kRrCZ = PB_RR_CZ;
 constexpr int kRrFX = 2 * kRrCX + 1, kRrFY = 2 * kRrCY + 1;  // 65 x 9 fine nodes
 constexpr int kRrThreads = 256;
 

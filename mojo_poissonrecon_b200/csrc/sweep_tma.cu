@@ -282,7 +282,10 @@ static int make_map(CUtensorMap* map, const float* base, int n, int P, int rows)
 // coordinates come from the launch shape, rows are read and written
 // coalesced, and the coarse values (one coarse node per 2 x 2 x 2 fine nodes)
 // stay in L1/L2 across the fine planes that share them.
-constexpr int kProTX = 64, kProTY = 4, kProTZ = 16;
+#ifndef PB_PROLONG_TZ
+#define PB_PROLONG_TZ 16  // fine planes per block
+#endif
+constexpr int kProTX = 64, kProTY = 4, kProTZ = PB_PROLONG_TZ;
 
 __global__ void __launch_bounds__(kProTX* kProTY) prolong_add32_kernel(const float* __restrict__ c,
                                                                        float* __restrict__ f,

@@ -24,7 +24,7 @@ Gauss-Seidel smoother, 3 sweeps each way (core.py:141-193); the coarser
 levels are Galerkin operators with screening-scaled transfers (mg27.cu),
 smoothed by COARSE_SWEEPS sweeps each way, which cut the cycles needed for a
 given residual 2-4x against the reference's rediscretised hierarchy.  Levels
-of side <= 17 run in a single launch, the 3^3 level solved exactly with its
+of side <= 9 run in a single launch, the 3^3 level solved exactly with its
 inverse (built once per set-up).  Convergence is always measured with the
 reference's FP64 operator.
 """
@@ -41,7 +41,8 @@ import torch
 from . import _native as nat
 from .solver import SolveStats, level_sizes, norm
 
-COARSE_N = 17  # levels of this side or smaller: one single-block launch
+COARSE_N = 9  # levels of this side or smaller: one single-block launch
+TMA_MIN_N = 33  # smallest side the TMA sweep takes (level 0 below it is a 27-point level)
 COARSE_SWEEPS = 2  # pre- and post-smoothing sweeps on every level below level 0
 MAX_ITER = 512  # capacity of the device iteration history (and hard cap)
 
@@ -61,8 +62,8 @@ class Level32:
     Every level has work arrays (rhs, ea, eb), 1/diagonal (invD) and its
     prolongation weights (weights).  Level 0 also keeps the reference's
     7-point operator as its diagonal D.  Levels that run the 27-point kernels
-    (all but a level 0 of side >= 33) hold their operator as 14 planes `coef`
-    and a residual array `res`."""
+    (all but a level 0 of side >= TMA_MIN_N) hold their operator as 14 planes
+    `coef` and a residual array `res`."""
 
     def __init__(self, n: int, device: torch.device, lib, first: bool):
         self.n = n
@@ -73,7 +74,7 @@ class Level32:
         def zeros(*lead):
             return torch.zeros(*lead, self.count, dtype=torch.float32, device=device)
 
-        self.seven = first and n > COARSE_N
+        self.seven = first and n >= TMA_MIN_N
         self.invD, self.rhs, self.ea, self.eb, self.weights = (zeros() for _ in range(5))
         # level 0's residual is fused into its restriction; 27-point levels store theirs
         self.res = None if self.seven else zeros()
