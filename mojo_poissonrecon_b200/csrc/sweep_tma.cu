@@ -278,40 +278,61 @@ static int make_map(CUtensorMap* map, const float* base, int n, int P, int rows)
 // ---- scaled prolongation add on the padded layout -------------------------------
 // fine += s * trilinear(coarse) (the P_s of mg27.cu; trilinear as in
 // capi.mojo:677-742), s the fine level's prolongation weights.
-// Tiled: a block owns a 64 x 4 (x, y) fine tile and 16 fine planes; the fine
-// coordinates come from the launch shape, rows are read and written
-// coalesced, and the coarse values (one coarse node per 2 x 2 x 2 fine nodes)
-// stay in L1/L2 across the fine planes that share them.
+// A thread owns four consecutive fine x (one float4 of e and of s; x offset 4
+// keeps them 16-byte aligned), a block a 128 x 8 (x, y) tile and kProTZ fine
+// planes.  The four fine nodes of a thread share three coarse values per
+// coarse row: fine x = 4k + j lies on coarse 2k + j/2 (even j) or between
+// 2k + j/2 and the next (odd j).  Fine x >= n (ghost and padding) is never
+// written.
 #ifndef PB_PROLONG_TZ
 #define PB_PROLONG_TZ 16  // fine planes per block
 #endif
-constexpr int kProTX = 64, kProTY = 4, kProTZ = PB_PROLONG_TZ;
+constexpr int kProTX = 32, kProTY = 8, kProTZ = PB_PROLONG_TZ;
 
 __global__ void __launch_bounds__(kProTX* kProTY) prolong_add32_kernel(const float* __restrict__ c,
                                                                        float* __restrict__ f,
                                                                        const float* __restrict__ w, int n, int P,
                                                                        int cn, int cP) {
-    const int x = blockIdx.x * kProTX + threadIdx.x, y = blockIdx.y * kProTY + threadIdx.y;
+    const int k = blockIdx.x * kProTX + threadIdx.x, y = blockIdx.y * kProTY + threadIdx.y;
+    const int x = 4 * k;
     if (x >= n || y >= n) return;
     const int z0 = blockIdx.z * kProTZ, z1 = min(n, z0 + kProTZ);
-    const int xa = x >> 1, ya = y >> 1;
-    const int xb = min(xa + 1, cn - 1), yb = min(ya + 1, cn - 1);
-    const float tx = (x & 1) ? 0.5f : 0.f, ty = (y & 1) ? 0.5f : 0.f;
+    const int ya = y >> 1, yb = min(ya + 1, cn - 1);
+    const float ty = (y & 1) ? 0.5f : 0.f;
     const int64_t cplane = (int64_t)(cn + 2) * cP;
-    const float* ca = c + (int64_t)(ya + 1) * cP + (xa + 4);  // coarse row ya at plane -1 + 1
-    const int64_t dx = xb - xa, dy = (int64_t)(yb - ya) * cP;
+    // coarse row ya, columns 2k .. 2k+2 (offset 4); column 2k+2 <= cn + 1 stays inside the padded row
+    const float* ca = c + (int64_t)(ya + 1) * cP + (2 * k + 4);
+    const int64_t dy = (int64_t)(yb - ya) * cP;
+    const int valid = min(4, n - x);
     for (int z = z0; z < z1; ++z) {
         const int za = z >> 1, zb = min(za + 1, cn - 1);
         const float tz = (z & 1) ? 0.5f : 0.f;
         const float* c0 = ca + (int64_t)(za + 1) * cplane;
         const float* c1 = ca + (int64_t)(zb + 1) * cplane;
-        const float c00 = c0[0] * (1.f - tx) + c0[dx] * tx;
-        const float c10 = c0[dy] * (1.f - tx) + c0[dy + dx] * tx;
-        const float c01 = c1[0] * (1.f - tx) + c1[dx] * tx;
-        const float c11 = c1[dy] * (1.f - tx) + c1[dy + dx] * tx;
-        const float v = (c00 * (1.f - ty) + c10 * ty) * (1.f - tz) + (c01 * (1.f - ty) + c11 * ty) * tz;
+        float q[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const float a0 = c0[i] * (1.f - ty) + c0[dy + i] * ty;
+            const float a1 = c1[i] * (1.f - ty) + c1[dy + i] * ty;
+            q[i] = a0 * (1.f - tz) + a1 * tz;
+        }
+        // x interpolation: t = 0 on even x, 1/2 on odd x (coarse 2k + 2 only weighs odd x < n - 1)
+        const float v0 = q[0], v1 = q[0] * 0.5f + q[1] * 0.5f, v2 = q[1], v3 = q[1] * 0.5f + q[2] * 0.5f;
         const int64_t p = ((int64_t)(z + 1) * (n + 2) + (y + 1)) * P + (x + 4);
-        f[p] += w[p] * v;
+        if (valid == 4) {
+            float4 e = *reinterpret_cast<const float4*>(f + p);
+            const float4 s = *reinterpret_cast<const float4*>(w + p);
+            e.x += s.x * v0;
+            e.y += s.y * v1;
+            e.z += s.z * v2;
+            e.w += s.w * v3;
+            *reinterpret_cast<float4*>(f + p) = e;
+        } else {
+            const float v[4] = {v0, v1, v2, v3};
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                if (j < valid) f[p + j] += w[p + j] * v[j];
+        }
     }
 }
 
@@ -377,7 +398,8 @@ extern "C" int pb_prolong_fac_f32(const float* coarse, float* fine, const float*
                                   void* stream) {
     if (fine_n < 3 || fine_n > 4097 || !coarse || !fine || !weights) return fail(PB_ERR_INVALID, "prolong32: bad args");
     const int n = (int)fine_n, cn = (n + 1) / 2;
-    const dim3 grid((n + kProTX - 1) / kProTX, (n + kProTY - 1) / kProTY, (n + kProTZ - 1) / kProTZ);
+    const int groups = (n + 3) / 4;
+    const dim3 grid((groups + kProTX - 1) / kProTX, (n + kProTY - 1) / kProTY, (n + kProTZ - 1) / kProTZ);
     prolong_add32_kernel<<<grid, dim3(kProTX, kProTY), 0, (cudaStream_t)stream>>>(coarse, fine, weights, n,
                                                                                    pitch_for(n), cn, pitch_for(cn));
     PB_CHECK_LAUNCH("prolong_add32_kernel");
