@@ -85,8 +85,11 @@ __device__ __forceinline__ void scatter14(float v, int dx, int dy, int dz, float
 // FINE7: `fc` is the level-0 diagonal D (couplings -h2 to in-grid face
 // neighbours); otherwise `fc` holds the fine level's 14 planes.  S: the fine
 // level's prolongation weights.
+#ifndef PB_GALERKIN_MIN_BLOCKS
+#define PB_GALERKIN_MIN_BLOCKS 4  // 128 registers: the 27-point gather runs 1.5x faster at 4 blocks per SM
+#endif
 template <bool FINE7>
-__global__ void __launch_bounds__(128) galerkin_kernel(const float* __restrict__ fc, int64_t fs,
+__global__ void __launch_bounds__(128, PB_GALERKIN_MIN_BLOCKS) galerkin_kernel(const float* __restrict__ fc, int64_t fs,
                                                        const float* __restrict__ S, Geom gf, float h2,
                                                        float* __restrict__ cc, int64_t cs, Geom gc) {
     const int xc = blockIdx.x * blockDim.x + threadIdx.x, yc = blockIdx.y * blockDim.y + threadIdx.y;

@@ -112,17 +112,20 @@ __global__ void sum_partials_kernel(const double* __restrict__ partial, int coun
 
 // ---- level-0 residual fused with the scaled restriction -------------------------
 // coarse_rhs = P^T (s (rhs - A e)) / 8 (mg27.cu) without writing the fine
-// residual.  A block owns a 32 x 4 tile of coarse (x, y) and marches coarse z;
-// fine residual planes of the tile plus a halo of one (65 x 9 nodes), already
-// multiplied by the prolongation weight s, are computed into a three-plane
-// ring in shared memory, plane 2zc+1 being reused as plane 2(zc+1)-1 of the
-// next coarse plane.  Out-of-grid ring entries are zero, so the restriction
-// sums all 27 entries with weights (1,2,1)^3 / 64.
+// residual.  A block owns a 64 x 4 tile of coarse (x, y) and marches coarse z.
+// The fine residual of the tile's region (fine x from 2 xc0 - 4, 136 columns;
+// fine y from 2 yc0 - 1, 9 rows), already multiplied by the prolongation weight
+// s, is computed four x at a time (float4 loads of e, rhs, D and s; the row
+// starts stay 16-byte aligned) into a three-plane ring in shared memory, plane
+// 2zc+1 being reused as plane 2(zc+1)-1 of the next coarse plane.  Out-of-grid
+// ring entries are zero, so the restriction sums all 27 entries with weights
+// (1,2,1)^3 / 64.
 #ifndef PB_RR_CZ
 #define PB_RR_CZ 8  // coarse planes per block
 #endif
-constexpr int kRrCX = 32, kRrCY = 4, kRrCZ = PB_RR_CZ;
-constexpr int kRrFX = 2 * kRrCX + 1, kRrFY = 2 * kRrCY + 1;  // 65 x 9 fine nodes
+constexpr int kRrCX = 64, kRrCY = 4, kRrCZ = PB_RR_CZ;
+constexpr int kRrFX = 2 * kRrCX + 8, kRrFY = 2 * kRrCY + 1;  // 136 x 9 fine nodes
+constexpr int kRrGroups = kRrFX / 4;                            // float4 groups per ring row
 constexpr int kRrThreads = 256;
 
 __global__ void __launch_bounds__(kRrThreads) residual_restrict32_kernel(const float* __restrict__ e,
@@ -131,24 +134,40 @@ __global__ void __launch_bounds__(kRrThreads) residual_restrict32_kernel(const f
                                                                           const float* __restrict__ w, Geom gf,
                                                                           float h2, float* __restrict__ coarse,
                                                                           Geom gc) {
-    __shared__ float ring[3][kRrFY][kRrFX + 3];
+    __shared__ __align__(16) float ring[3][kRrFY][kRrFX];
     const int fn = gf.n, cn = gc.n;
     const int xc0 = blockIdx.x * kRrCX, yc0 = blockIdx.y * kRrCY;
     const int zc0 = blockIdx.z * kRrCZ, zc1 = min(cn, zc0 + kRrCZ);
-    const int fx0 = 2 * xc0 - 1, fy0 = 2 * yc0 - 1;
+    const int fx0 = 2 * xc0 - 4, fy0 = 2 * yc0 - 1;
     const int tid = threadIdx.x;
-    auto fine_plane = [&](int f) {  // residual of fine plane f over the tile region
-        float(*dst)[kRrFX + 3] = ring[(f + 3) % 3];
-        for (int i = tid; i < kRrFY * kRrFX; i += kRrThreads) {
-            const int ly = i / kRrFX, lx = i - ly * kRrFX;
-            const int x = fx0 + lx, y = fy0 + ly;
-            float r = 0.0f;
-            if (f >= 0 && f < fn && x >= 0 && x < fn && y >= 0 && y < fn) {
+    auto fine_plane = [&](int f) {  // s-weighted residual of fine plane f over the tile region
+        float(*dst)[kRrFX] = ring[(f + 3) % 3];
+        for (int i = tid; i < kRrFY * kRrGroups; i += kRrThreads) {
+            const int ly = i / kRrGroups, g = i - ly * kRrGroups;
+            const int x = fx0 + 4 * g, y = fy0 + ly;
+            float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (f >= 0 && f < fn && y >= 0 && y < fn && x >= 0 && x < fn) {
                 const int64_t p = gf.at(x, y, f);
-                const float sum = e[p - 1] + e[p + 1] + e[p - gf.P] + e[p + gf.P] + e[p - gf.plane] + e[p + gf.plane];
-                r = w[p] * (rhs[p] - (D[p] * e[p] - sum * h2));
+                const float4 c = *reinterpret_cast<const float4*>(e + p);
+                const float4 ym = *reinterpret_cast<const float4*>(e + p - gf.P);
+                const float4 yp = *reinterpret_cast<const float4*>(e + p + gf.P);
+                const float4 zm = *reinterpret_cast<const float4*>(e + p - gf.plane);
+                const float4 zp = *reinterpret_cast<const float4*>(e + p + gf.plane);
+                const float4 b = *reinterpret_cast<const float4*>(rhs + p);
+                const float4 d = *reinterpret_cast<const float4*>(D + p);
+                const float4 s = *reinterpret_cast<const float4*>(w + p);
+                const float l = e[p - 1], rr = e[p + 4];
+                const float s0 = l + c.y + ym.x + yp.x + zm.x + zp.x;
+                const float s1 = c.x + c.z + ym.y + yp.y + zm.y + zp.y;
+                const float s2 = c.y + c.w + ym.z + yp.z + zm.z + zp.z;
+                const float s3 = c.z + rr + ym.w + yp.w + zm.w + zp.w;
+                // lanes at x >= fn lie on ghosts or padding, where s and D are zero: mask them explicitly
+                r.x = s.x * (b.x - (d.x * c.x - s0 * h2));
+                r.y = x + 1 < fn ? s.y * (b.y - (d.y * c.y - s1 * h2)) : 0.f;
+                r.z = x + 2 < fn ? s.z * (b.z - (d.z * c.z - s2 * h2)) : 0.f;
+                r.w = x + 3 < fn ? s.w * (b.w - (d.w * c.w - s3 * h2)) : 0.f;
             }
-            dst[ly][lx] = r;
+            *reinterpret_cast<float4*>(&dst[ly][4 * g]) = r;
         }
     };
     fine_plane(2 * zc0 - 1);
@@ -156,8 +175,8 @@ __global__ void __launch_bounds__(kRrThreads) residual_restrict32_kernel(const f
         fine_plane(2 * zc);
         fine_plane(2 * zc + 1);
         __syncthreads();
-        if (tid < kRrCX * kRrCY) {
-            const int cy = tid / kRrCX, cx = tid - cy * kRrCX;
+        {
+            const int cy = tid / kRrCX, cx = tid - cy * kRrCX;  // 256 threads = the 64 x 4 coarse tile
             const int xc = xc0 + cx, yc = yc0 + cy;
             if (xc < cn && yc < cn) {
                 float sum = 0.0f;
@@ -169,7 +188,7 @@ __global__ void __launch_bounds__(kRrThreads) residual_restrict32_kernel(const f
                         const float* row = ring[(zz + 3) % 3][2 * cy + 1 + oy];
 #pragma unroll
                         for (int ox = -1; ox <= 1; ++ox)
-                            sum += row[2 * cx + 1 + ox] * (float)((ox ? 1 : 2) * (oy ? 1 : 2) * (oz ? 1 : 2));
+                            sum += row[2 * cx + 4 + ox] * (float)((ox ? 1 : 2) * (oy ? 1 : 2) * (oz ? 1 : 2));
                     }
                 }
                 coarse[gc.at(xc, yc, zc)] = sum * (1.0f / 64.0f);

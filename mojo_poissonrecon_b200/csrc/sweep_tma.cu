@@ -27,7 +27,13 @@ constexpr int kTX = 64;                 // interior tile width (last x tile: 65)
 constexpr int kTY = 16;                 // interior tile height (last y tile: 17)
 constexpr int kBoxX = 72;               // kTX + 1 + halo 2 + 2, rounded to 16 B; x origin = x0 - 4
 constexpr int kBoxY = kTY + 1 + 4;      // 21
-constexpr int kSlots = 5;               // planes t-1 .. t+3
+#ifndef PB_SWEEP_SLOTS
+#define PB_SWEEP_SLOTS 5
+#endif
+#ifndef PB_SWEEP_MIN_BLOCKS
+#define PB_SWEEP_MIN_BLOCKS 2
+#endif
+constexpr int kSlots = PB_SWEEP_SLOTS;  // planes t-1 .. t+3
 constexpr long long kWaitCycles = 2000000000ll;
 
 __device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -105,7 +111,7 @@ __device__ __forceinline__ float4 lds4(const float* p) { return *reinterpret_cas
 constexpr int kThreads = 352;  // 19 box rows x 18 groups = 342 work items, one per thread
 
 template <bool ZERO_IN, int SLOTS>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, PB_SWEEP_MIN_BLOCKS)
     sweep_kernel(const __grid_constant__ CUtensorMap map_e, const __grid_constant__ CUtensorMap map_rhs,
                     const __grid_constant__ CUtensorMap map_invD, Params p) {
     constexpr int TY = kTY;
