@@ -255,6 +255,19 @@ int pb_extract_emit_f64(const double *field, const double *density, int64_t n, c
                         double *vertex_density, int64_t *faces, void *workspace, size_t workspace_bytes,
                         void *stream);
 
+/* oriented_points_from_mesh (core.py:429-451) on the device, bit-identical to
+ * the reference's per-face loop: count first (counts[0] = kept vertices,
+ * counts[1] = 1 if a face index lies outside [0, vertex_count); device
+ * int64[2]), then emit the kept vertices and their unit area-weighted normals
+ * in vertex order with the same arguments and workspace. */
+size_t pb_mesh_normals_workspace_size(int64_t vertex_count, int64_t face_count);
+int pb_mesh_normals_count_f64(const double *vertices, int64_t vertex_count, const int64_t *faces,
+                              int64_t face_count, int64_t *counts, void *workspace, size_t workspace_bytes,
+                              void *stream);
+int pb_mesh_normals_emit_f64(const double *vertices, int64_t vertex_count, const int64_t *faces, int64_t face_count,
+                             double *out_points, double *out_normals, void *workspace, size_t workspace_bytes,
+                             void *stream);
+
 /* ---- FP32 preconditioner levels (no counterpart in the reference) ----------
  * The reference's V-cycle (core.py:141-193) rediscretises coarse levels; the
  * FP32 preconditioner of the refined solvers uses Galerkin coarse levels

@@ -71,6 +71,9 @@ _SIGNATURES = {
     "pb_sweep_tma_f32": ([P, P, P, P, I, I, I, P, P], C),
     "pb_prolong_fac_f32": ([P, P, P, I, P], C),
     "pb_extract_workspace_size": ([I], S),
+    "pb_mesh_normals_workspace_size": ([I, I], S),
+    "pb_mesh_normals_count_f64": ([P, I, P, I, P, P, S, P], C),
+    "pb_mesh_normals_emit_f64": ([P, I, P, I, P, P, P, S, P], C),
     "pb_extract_count_f64": ([P, I, P, P, P, S, P], C),
     "pb_extract_emit_f64": ([P, P, I, P, P, P, P, P, S, P], C),
     "pb_residual_restrict_f32": ([P, P, P, P, P, I, P], C),

@@ -27,7 +27,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
           "--expt-relaxed-constexpr"]
 # Units that restate the reference's FP64 arithmetic exactly.
-EXACT_FP64 = {"octree.cu", "splat.cu", "stencil64.cu", "iso.cu", "dual.cu", "prep.cu"}
+EXACT_FP64 = {"octree.cu", "splat.cu", "stencil64.cu", "iso.cu", "dual.cu", "prep.cu", "mesh.cu"}
 
 
 def nvcc() -> str:

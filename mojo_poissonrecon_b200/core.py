@@ -462,32 +462,46 @@ def reconstruct(
 
 # ---- mesh input (core.py:429-455) -------------------------------------------
 
-def oriented_points_from_mesh(vertices, faces):
-    """Return referenced vertices and area-weighted normals from a triangle mesh."""
-    vertices = np.asarray(_points(vertices.cpu() if isinstance(vertices, torch.Tensor) else vertices))
-    faces = np.asarray(i64(faces.cpu() if isinstance(faces, torch.Tensor) else faces))
+def _oriented_points_device(vertices, faces) -> tuple[torch.Tensor, torch.Tensor]:
+    """core.py:429-451 on the device (csrc/mesh.cu): referenced vertices and their
+    area-weighted unit normals, bit-identical to the reference's per-face loop."""
+    vertices = _points(vertices)
+    faces = i64(faces)
     if faces.ndim != 2 or faces.shape[1] != 3:
         raise ValueError("faces must have shape (m, 3)")
-    if len(faces) and (faces.min() < 0 or faces.max() >= len(vertices)):
+    if isinstance(faces, np.ndarray) and len(faces) and (faces.min() < 0 or faces.max() >= len(vertices)):
+        raise ValueError("face index out of range")  # device inputs are checked by the kernel
+    if len(faces) == 0 or len(vertices) == 0:  # nothing is referenced: no device work
+        empty = torch.empty((0, 3), dtype=torch.float64)
+        return empty, empty.clone()
+    ctx = _Context()
+    dv = _to_device(vertices, ctx.device)
+    df = faces.to(ctx.device).contiguous() if isinstance(faces, torch.Tensor) else \
+        torch.from_numpy(np.ascontiguousarray(faces)).to(ctx.device)
+    nv, nf = dv.shape[0], df.shape[0]
+    L = ctx.lib
+    ptr, size = ctx.ws.get(L.pb_mesh_normals_workspace_size(nv, nf))
+    counts = torch.empty(2, dtype=torch.int64, device=ctx.device)
+    ctx.check(L.pb_mesh_normals_count_f64(dv.data_ptr() if nv else None, nv, df.data_ptr() if nf else None, nf,
+                                          counts.data_ptr(), ptr, size, ctx.stream), "mesh normals count")
+    kept, bad = (int(c) for c in counts.cpu())
+    if bad:
         raise ValueError("face index out of range")
-    normals = np.zeros_like(vertices)
-    referenced = np.zeros(len(vertices), dtype=bool)
-    if len(faces):
-        a, b, c = faces[:, 0], faces[:, 1], faces[:, 2]
-        cross = np.cross(vertices[b] - vertices[a], vertices[c] - vertices[a])
-        good = np.isfinite(cross).all(axis=1) & (np.einsum("ij,ij->i", cross, cross) > 0)
-        tri = faces[good]
-        # np.add.at applies the updates one by one in index order: the same
-        # per-vertex summation order as the reference's per-face loop.
-        order = tri.reshape(-1)
-        np.add.at(normals, order, np.repeat(cross[good], 3, axis=0))
-        referenced[order] = True
-    lengths = np.linalg.norm(normals, axis=1)
-    keep = referenced & (lengths > 0) & np.isfinite(lengths)
-    normals[keep] /= lengths[keep, None]
-    return np.ascontiguousarray(vertices[keep]), np.ascontiguousarray(normals[keep])
+    points = torch.empty((kept, 3), dtype=torch.float64, device=ctx.device)
+    normals = torch.empty((kept, 3), dtype=torch.float64, device=ctx.device)
+    if kept:
+        ctx.check(L.pb_mesh_normals_emit_f64(dv.data_ptr(), nv, df.data_ptr() if nf else None, nf,
+                                             points.data_ptr(), normals.data_ptr(), ptr, size, ctx.stream),
+                  "mesh normals emit")
+    return points, normals
+
+
+def oriented_points_from_mesh(vertices, faces):
+    """Return referenced vertices and area-weighted normals from a triangle mesh."""
+    points, normals = _oriented_points_device(vertices, faces)
+    return points.cpu().numpy(), normals.cpu().numpy()
 
 
 def reconstruct_mesh(vertices, faces, **kwargs) -> Mesh:
-    points, normals = oriented_points_from_mesh(vertices, faces)
+    points, normals = _oriented_points_device(vertices, faces)
     return reconstruct(points, normals, **kwargs)
