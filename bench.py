@@ -437,6 +437,44 @@ def run_batch(args) -> dict:
             "data": "synthetic (workloads.batch_clouds, seed 3)"}
 
 
+def run_batch_sharded(args) -> dict | None:
+    """The 256-cloud batch across the ranks of a torchrun job (one GPU each):
+    greedy partition by HBM footprint, meshes gathered on rank 0, time = the
+    slowest rank's, measured on the device."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from mojo_poissonrecon_b200 import serve, shard, workloads
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        rank, world = dist.get_rank(), dist.get_world_size()
+        clouds = workloads.batch_clouds(256, seed=3)
+        serve.reconstruct_batch(clouds[:8], lanes=args.lanes)  # warm the engines and graphs
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        meshes = shard.reconstruct_sharded(clouds, lanes=args.lanes)
+        e1.record()
+        torch.cuda.synchronize()
+        seconds = shard.max_over_ranks(e0.elapsed_time(e1) / 1e3, torch.device("cuda", local))
+        dist.barrier()
+        if rank != 0:
+            return None
+        return {"metric": METRIC, "workload": "batch: 256 uneven clouds (1k-200k points, depths 5-8, "
+                                              "ellipsoids/tori), sharded by HBM footprint",
+                "value": round(len(clouds) / seconds, 2), "unit": "recons/s", "n_gpus": world, "scaling": "strong",
+                "wall_s": round(seconds, 3), "meshes": sum(m is not None for m in meshes), "lanes": args.lanes,
+                "precision": "fp32_refined", "tol": TOL, "data": "synthetic (workloads.batch_clouds, seed 3)"}
+    finally:
+        dist.destroy_process_group()
+
+
 def run_serving(args) -> dict:
     """Poisson arrivals (rate, duration) of requests with log-normal sizes
     (median 50k, sigma 1, clipped to [1k, 2M]) and depths in {6,7,8,9}.  The
@@ -510,6 +548,11 @@ def run_deep(args) -> dict:
 
 def main():
     args = parse_args()
+    if args.workload == "batch" and args.impl == "ours" and int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        result = run_batch_sharded(args)
+        if result is not None:
+            print(json.dumps(result), flush=True)
+        return
     if args.workload != "torus" and args.impl == "ours":
         runner = {"batch": run_batch, "serving": run_serving, "deep": run_deep}[args.workload]
         if int(os.environ.get("RANK", "0")) == 0:

@@ -16,20 +16,19 @@ namespace pb {
 // ---- level set-up: D, 1/D and the prolongation weights from the FP64 screen ----
 // weights (may be null): s = 1 on nodes of the coarse grid (all coordinates
 // even), else deg (n-1)^2 / D (mg27.cu).
-__global__ void level_setup_kernel(const double* __restrict__ screen, Geom g, double pw, float* __restrict__ D,
-                                   float* __restrict__ invD, float* __restrict__ weights) {
+__global__ void __launch_bounds__(256) level_setup_kernel(const double* __restrict__ screen, Geom g, double pw,
+                                                          float* __restrict__ D, float* __restrict__ invD,
+                                                          float* __restrict__ weights) {
     const int n = g.n;
-    const int64_t total = (int64_t)n * n * n;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    if (x >= n || y >= n) return;
     const double h = (double)(n - 1), h2 = h * h;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % n), y = (int)((i / n) % n), z = (int)(i / ((int64_t)n * n));
-        const int deg = (x > 0) + (x + 1 < n) + (y > 0) + (y + 1 < n) + (z > 0) + (z + 1 < n);
-        const double d = (double)deg * h2 + pw * screen[i] * h2;
-        const int64_t p = g.at(x, y, z);
-        D[p] = (float)d;
-        invD[p] = (float)(1.0 / d);
-        if (weights) weights[p] = ((x | y | z) & 1) ? (float)((double)deg * h2 / d) : 1.0f;
-    }
+    const int deg = (x > 0) + (x + 1 < n) + (y > 0) + (y + 1 < n) + (z > 0) + (z + 1 < n);
+    const double d = (double)deg * h2 + pw * screen[((int64_t)z * n + y) * n + x] * h2;
+    const int64_t p = g.at(x, y, z);
+    D[p] = (float)d;
+    invD[p] = (float)(1.0 / d);
+    if (weights) weights[p] = ((x | y | z) & 1) ? (float)((double)deg * h2 / d) : 1.0f;
 }
 
 // ---- FP64 defect with the fused update x_new = x_old + e ------------------------
@@ -198,12 +197,6 @@ __global__ void __launch_bounds__(kRrThreads) residual_restrict32_kernel(const f
     }
 }
 
-static unsigned stride_grid(int64_t items, int threads, int per_sm = 16) {
-    int64_t b = (items + threads - 1) / threads;
-    const int64_t cap = (int64_t)kSMs * per_sm;
-    if (b > cap) b = cap;
-    return (unsigned)(b < 1 ? 1 : b);
-}
 
 static dim3 defect_grid(int n) {
     return dim3((n + kDefTX - 1) / kDefTX, (n + kDefTY - 1) / kDefTY, (n + kDefZ - 1) / kDefZ);
@@ -228,8 +221,9 @@ extern "C" int pb_level_geometry(int64_t n, int64_t* pitch, int64_t* padded_coun
 extern "C" int pb_level_setup_f32(const double* screen, int64_t n, double point_weight, float* D, float* invD,
                                   float* weights, void* stream) {
     if (n < 2 || n > 4097 || !screen || !D || !invD) return fail(PB_ERR_INVALID, "level setup: bad args");
-    level_setup_kernel<<<stride_grid(n * n * n, 256), 256, 0, (cudaStream_t)stream>>>(screen, geom((int)n),
-                                                                                     point_weight, D, invD, weights);
+    const dim3 block(32, 8), grid(((int)n + 31) / 32, ((int)n + 7) / 8, (int)n);
+    level_setup_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(screen, geom((int)n), point_weight, D, invD,
+                                                                 weights);
     PB_CHECK_LAUNCH("level_setup_kernel");
     return PB_OK;
 }
