@@ -289,13 +289,21 @@ int pb_galerkin_f32(const float *fine, int64_t fine_n, int fine_is_7pt, const fl
 int pb_level27_from7_f32(const float *D, int64_t n, float *coef, void *stream);
 /* invD = 1 / diagonal and the prolongation weights of a 27-point level. */
 int pb_level27_finish_f32(const float *coef, int64_t n, float *invD, float *weights, void *stream);
-/* One red-black ordered sweep e_next <- S(e_prev) on a 27-point level, the
+/* Packed 27-point levels: per colour c, the 26 couplings divided by the
+ * diagonal, -a(J, J+K) / a(J, J), in FP16 (h_c, 26 planes) and 1/a(J, J) in
+ * FP32 (inv_c), over the colour's nodes numbered compactly; sizes in bytes
+ * from pb_packed27_size.  Relaxation and residual of a packed level both use
+ * the rounded couplings. */
+int pb_packed27_size(int64_t n, int64_t *coupling_bytes, int64_t *inverse_bytes);
+int pb_pack27_f32(const float *coef, int64_t n, void *h0, void *h1, float *inv0, float *inv1, void *stream);
+/* One red-black ordered sweep e_next <- S(e_prev) on a packed level, the
  * same-colour couplings from e_prev (e_prev NULL: from zero). */
-int pb_relax27_f32(const float *e_prev, float *e_next, const float *rhs, const float *coef,
-                   const float *invD, int64_t n, void *stream);
-/* res = weights * (rhs - A e) on a 27-point level, then coarse_rhs = P^T res / 8. */
-int pb_residual_restrict27_f32(const float *e, const float *rhs, const float *coef, const float *weights,
-                               int64_t n, float *res, float *coarse_rhs, void *stream);
+int pb_relax27p_f32(const float *e_prev, float *e_next, const float *rhs, const void *h0, const void *h1,
+                    const float *inv0, const float *inv1, int64_t n, void *stream);
+/* res = weights * (rhs - A e) on a packed level, then coarse_rhs = P^T res / 8. */
+int pb_residual_restrict27p_f32(const float *e, const float *rhs, const void *h0, const void *h1,
+                                const float *inv0, const float *inv1, const float *weights, int64_t n,
+                                float *res, float *coarse_rhs, void *stream);
 /* Inverse (27 x 27, FP32 row-major) of the 27-point level of side 3. */
 int pb_coarse_inverse_f32(const float *coef, int64_t n, float *inverse, void *stream);
 /* The V-cycle below a 27-point level of side <= 17 in one block: count

@@ -80,8 +80,10 @@ _SIGNATURES = {
     "pb_galerkin_f32": ([P, I, C, P, P, P], C),
     "pb_level27_from7_f32": ([P, I, P, P], C),
     "pb_level27_finish_f32": ([P, I, P, P, P], C),
-    "pb_relax27_f32": ([P, P, P, P, P, I, P], C),
-    "pb_residual_restrict27_f32": ([P, P, P, P, I, P, P, P], C),
+    "pb_packed27_size": ([I, ctypes.POINTER(I), ctypes.POINTER(I)], C),
+    "pb_pack27_f32": ([P, I, P, P, P, P, P], C),
+    "pb_relax27p_f32": ([P, P, P, P, P, P, P, I, P], C),
+    "pb_residual_restrict27p_f32": ([P, P, P, P, P, P, P, I, P, P, P], C),
     "pb_coarse_inverse_f32": ([P, I, P, P], C),
     "pb_coarse27_cycle_f32": ([I, P, P, P, P, P, P, P, I, I, I, P, P], C),
 }

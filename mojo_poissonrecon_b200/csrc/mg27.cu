@@ -24,13 +24,16 @@
 //
 // Smoothing on 27-point levels: red-black ordered, same-colour couplings
 // taken from the previous iterate (two passes per sweep, e_prev -> e_next,
-// no in-place race).
+// no in-place race); levels of side > 9 with their couplings packed per colour
+// (see "packed 27-point levels" below), the smaller ones in one block.
 //
 // Storage of a 27-point level: 14 coefficient planes in the padded layout
 // (level32.cuh), plane stride = padded_size(n); plane 0 the diagonal, planes
 // 1..13 the couplings to the 13 "forward" neighbours J+K (K.z > 0; or K.z == 0
 // and K.y > 0; or K = (1,0,0)).  The coupling to a backward neighbour J-K is
 // plane k(K) at J-K (symmetry).  Ghost entries are zero.
+#include <cuda_fp16.h>
+
 #include "common.cuh"
 #include "level32.cuh"
 
@@ -180,54 +183,6 @@ __global__ void level27_finish_kernel(const float* __restrict__ c, int64_t cs, G
 }
 
 // ---- 27-point smoothing, residual, transfers ------------------------------------
-// One colour pass: nodes of colour COLOUR get (rhs - sum_{K != 0} a e) / a_JJ,
-// neighbours of the other colour read from `next` when COLOUR == 1 (updated in
-// pass 0), everything else from `prev` (zero when ZERO).
-template <int COLOUR, bool ZERO>
-__global__ void __launch_bounds__(256) relax27_kernel(const float* __restrict__ prev, float* next,
-                                                      const float* __restrict__ rhs, const float* __restrict__ c,
-                                                      int64_t cs, const float* __restrict__ invD, Geom g) {
-    const int y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
-    const int x = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((y + z + COLOUR) & 1);
-    const int n = g.n;
-    if (x >= n || y >= n) return;
-    const int64_t p = g.at(x, y, z);
-    float s = 0.0f;
-#pragma unroll
-    for (int dz = -1; dz <= 1; ++dz)
-#pragma unroll
-        for (int dy = -1; dy <= 1; ++dy)
-#pragma unroll
-            for (int dx = -1; dx <= 1; ++dx) {
-                if (!(dx || dy || dz)) continue;
-                const bool other = ((dx + dy + dz) & 1) != 0;  // neighbour of the other colour
-                if (ZERO && !(COLOUR == 1 && other)) continue;
-                const int64_t q = p + offset_of(g, dx, dy, dz);
-                const float v = (COLOUR == 1 && other) ? next[q] : prev[q];
-                s += coupling(c, cs, g, p, dx, dy, dz) * v;
-            }
-    next[p] = (rhs[p] - s) * invD[p];
-}
-
-// res = s (rhs - A e) on the grid (ghosts untouched, zero).
-__global__ void __launch_bounds__(256) residual27_kernel(const float* __restrict__ e, const float* __restrict__ rhs,
-                                                         const float* __restrict__ c, int64_t cs,
-                                                         const float* __restrict__ fac, Geom g,
-                                                         float* __restrict__ res) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
-    const int n = g.n;
-    if (x >= n || y >= n) return;
-    const int64_t p = g.at(x, y, z);
-    float s = 0.0f;
-#pragma unroll
-    for (int dz = -1; dz <= 1; ++dz)
-#pragma unroll
-        for (int dy = -1; dy <= 1; ++dy)
-#pragma unroll
-            for (int dx = -1; dx <= 1; ++dx) s += coupling(c, cs, g, p, dx, dy, dz) * e[p + offset_of(g, dx, dy, dz)];
-    res[p] = fac[p] * (rhs[p] - s);
-}
-
 // coarse[J] = sum_o w(o)/64 res[2J+o], w = prod (2 on the axis, 1 off it);
 // out-of-grid fine nodes are ghosts holding zero.
 __global__ void __launch_bounds__(256) restrict27_kernel(const float* __restrict__ res, Geom gf,
@@ -244,6 +199,119 @@ __global__ void __launch_bounds__(256) restrict27_kernel(const float* __restrict
             for (int dx = -1; dx <= 1; ++dx)
                 s += res[p + offset_of(gf, dx, dy, dz)] * (float)((dx ? 1 : 2) * (dy ? 1 : 2) * (dz ? 1 : 2));
     coarse[gc.at(x, y, z)] = s * (1.0f / 64.0f);
+}
+
+// ---- packed 27-point levels: per-colour FP16 couplings --------------------------
+// A colour pass over the 14-plane storage reads its nodes' forward coupling
+// planes with stride 2 and the backward couplings at neighbours: about 140
+// bytes per node and sweep from DRAM on the 129^3 level.  Packed, each colour's nodes are
+// numbered compactly (row (y, z), i-th node of the colour: x = 2i + ((y+z+c)&1),
+// compact index (z*n + y)*Pc + i, Pc = (n+1)/2) and hold their 26 couplings
+// divided by the diagonal, c_K = -a(J, J+K) / a(J, J), in FP16 (|c_K| <= 1;
+// plane k = offset index over (dz, dy, dx) in lexicographic order, the centre
+// skipped), and 1/a(J, J) in FP32.  Relaxation and residual of the level both
+// use the rounded couplings, so the level's operator stays one operator:
+//   e_new(J) = invD(J) rhs(J) + sum_K c_K e(J+K)
+//   r(J)     = rhs(J) - (e(J) - sum_K c_K e(J+K)) / invD(J)
+// The rounding (relative 2^-11) changes the preconditioner only; convergence is
+// measured with the reference's FP64 operator.
+__host__ __device__ constexpr int packed_index(int dx, int dy, int dz) {
+    const int k = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+    return k < 13 ? k : k - 1;  // the centre (13) is not stored
+}
+
+struct Packed {
+    int n, Pc;
+    int64_t cs;  // compact nodes per colour = n * n * Pc (plane stride of the coupling array)
+    __host__ __device__ __forceinline__ int64_t at(int i, int y, int z) const { return ((int64_t)z * n + y) * Pc + i; }
+};
+
+inline Packed packed_of(int n) {
+    Packed p;
+    p.n = n;
+    p.Pc = (n + 1) / 2;
+    p.cs = (int64_t)n * n * p.Pc;
+    return p;
+}
+
+__global__ void __launch_bounds__(256) pack27_kernel(const float* __restrict__ c, int64_t cs, Geom g, Packed pk,
+                                                     __half* __restrict__ h0, __half* __restrict__ h1,
+                                                     float* __restrict__ i0, float* __restrict__ i1) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    const int n = g.n;
+    if (x >= n || y >= n) return;
+    const int colour = (x + y + z) & 1;
+    const int64_t q = pk.at(x >> 1, y, z);
+    const int64_t p = g.at(x, y, z);
+    const float inv = 1.0f / c[p];
+    __half* h = colour ? h1 : h0;
+    (colour ? i1 : i0)[q] = inv;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx) {
+                if (!(dx || dy || dz)) continue;
+                h[packed_index(dx, dy, dz) * pk.cs + q] = __float2half_rn(-coupling(c, cs, g, p, dx, dy, dz) * inv);
+            }
+}
+
+// One colour pass on a packed level: nodes of colour COLOUR get
+// invD rhs + sum_K c_K e(J+K), neighbours of the other colour read from `next`
+// when COLOUR == 1 (updated by pass 0), everything else from `prev` (zero when
+// ZERO).
+template <int COLOUR, bool ZERO>
+__global__ void __launch_bounds__(256) relax27p_kernel(const float* __restrict__ prev, float* next,
+                                                       const float* __restrict__ rhs, const __half* __restrict__ h,
+                                                       const float* __restrict__ inv, Geom g, Packed pk) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    const int x = 2 * i + ((y + z + COLOUR) & 1);
+    const int n = g.n;
+    if (x >= n || y >= n) return;
+    const int64_t p = g.at(x, y, z), q = pk.at(i, y, z);
+    float s = 0.0f;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx) {
+                if (!(dx || dy || dz)) continue;
+                const bool other = ((dx + dy + dz) & 1) != 0;
+                if (ZERO && !(COLOUR == 1 && other)) continue;
+                const int64_t o = p + offset_of(g, dx, dy, dz);
+                const float v = (COLOUR == 1 && other) ? next[o] : prev[o];
+                s += __half2float(h[packed_index(dx, dy, dz) * pk.cs + q]) * v;
+            }
+    next[p] = inv[q] * rhs[p] + s;
+}
+
+// res = s (rhs - A e) on a packed level, one thread per node.
+__global__ void __launch_bounds__(256) residual27p_kernel(const float* __restrict__ e, const float* __restrict__ rhs,
+                                                          const __half* __restrict__ h0,
+                                                          const __half* __restrict__ h1,
+                                                          const float* __restrict__ i0, const float* __restrict__ i1,
+                                                          const float* __restrict__ fac, Geom g, Packed pk,
+                                                          float* __restrict__ res) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    const int n = g.n;
+    if (x >= n || y >= n) return;
+    const int colour = (x + y + z) & 1;
+    const __half* __restrict__ h = colour ? h1 : h0;
+    const int64_t p = g.at(x, y, z), q = pk.at(x >> 1, y, z);
+    float s = 0.0f;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx) {
+                if (!(dx || dy || dz)) continue;
+                s += __half2float(h[packed_index(dx, dy, dz) * pk.cs + q]) * e[p + offset_of(g, dx, dy, dz)];
+            }
+    const float inv = colour ? i1[q] : i0[q];
+    res[p] = fac[p] * (rhs[p] - (e[p] - s) / inv);
 }
 
 // ---- exact solve on the 3^3 level -----------------------------------------------
@@ -328,7 +396,7 @@ __device__ float stencil27(const float* __restrict__ c, int64_t cs, const Geom& 
 
 // Red-black ordered sweeps in place: each colour's new values are staged in
 // registers and written after a barrier, so same-colour neighbours are read
-// from the previous iterate, as relax27_kernel does.
+// from the previous iterate, as the multi-block colour passes do.
 __device__ void c27_relax(const Coarse27& L, int l, int iters) {
     const Geom g = L.g[l];
     const int n = g.n, total = n * n * n;
@@ -478,45 +546,6 @@ extern "C" int pb_level27_finish_f32(const float* coef, int64_t n, float* invD, 
     return PB_OK;
 }
 
-// One red-black sweep e_next <- S(e_prev) on a 27-point level (e_prev null:
-// from zero).  e_next must not alias e_prev.
-extern "C" int pb_relax27_f32(const float* e_prev, float* e_next, const float* rhs, const float* coef,
-                              const float* invD, int64_t n, void* stream) {
-    if (!level_side_ok(n) || !e_next || !rhs || !coef || !invD || e_prev == e_next)
-        return fail(PB_ERR_INVALID, "relax27: bad args");
-    cudaStream_t s = (cudaStream_t)stream;
-    const Geom g = geom((int)n);
-    const int64_t cs = padded_size((int)n);
-    const dim3 block(32, 8);
-    const dim3 grid(((int)(n + 1) / 2 + 31) / 32, ((int)n + 7) / 8, (int)n);
-    if (e_prev) {
-        relax27_kernel<0, false><<<grid, block, 0, s>>>(e_prev, e_next, rhs, coef, cs, invD, g);
-        PB_CHECK_LAUNCH("relax27_kernel");
-        relax27_kernel<1, false><<<grid, block, 0, s>>>(e_prev, e_next, rhs, coef, cs, invD, g);
-    } else {
-        relax27_kernel<0, true><<<grid, block, 0, s>>>(nullptr, e_next, rhs, coef, cs, invD, g);
-        PB_CHECK_LAUNCH("relax27_kernel");
-        relax27_kernel<1, true><<<grid, block, 0, s>>>(nullptr, e_next, rhs, coef, cs, invD, g);
-    }
-    PB_CHECK_LAUNCH("relax27_kernel");
-    return PB_OK;
-}
-
-// res = weights * (rhs - A e), then coarse_rhs = P^T res / 8 on the next level.
-extern "C" int pb_residual_restrict27_f32(const float* e, const float* rhs, const float* coef, const float* weights,
-                                          int64_t n, float* res, float* coarse_rhs, void* stream) {
-    if (!level_side_ok(n) || n < 5 || !e || !rhs || !coef || !weights || !res || !coarse_rhs)
-        return fail(PB_ERR_INVALID, "residual_restrict27: bad args");
-    cudaStream_t s = (cudaStream_t)stream;
-    const int fn = (int)n, cn = (fn + 1) / 2;
-    const dim3 block(32, 8);
-    residual27_kernel<<<node_grid(fn, block), block, 0, s>>>(e, rhs, coef, padded_size(fn), weights, geom(fn), res);
-    PB_CHECK_LAUNCH("residual27_kernel");
-    restrict27_kernel<<<node_grid(cn, block), block, 0, s>>>(res, geom(fn), coarse_rhs, geom(cn));
-    PB_CHECK_LAUNCH("restrict27_kernel");
-    return PB_OK;
-}
-
 // Inverse (27 x 27, FP32 row-major) of a 27-point level of side 3.
 extern "C" int pb_coarse_inverse_f32(const float* coef, int64_t n, float* inverse, void* stream) {
     if (n != 3 || !coef || !inverse) return fail(PB_ERR_INVALID, "coarse inverse: side must be 3");
@@ -558,5 +587,67 @@ extern "C" int pb_coarse27_cycle_f32(int64_t count, const int64_t* sizes, const 
     if (sizes[count - 1] != 3) return fail(PB_ERR_INVALID, "coarse27 cycle: the last level must have side 3");
     coarse27_kernel<<<1, kC27Threads, 0, (cudaStream_t)stream>>>(L, (int)pre, (int)post, (int)inner);
     PB_CHECK_LAUNCH("coarse27_kernel");
+    return PB_OK;
+}
+
+// ---- packed levels ----------------------------------------------------------------
+// Bytes of one colour's packed couplings (26 FP16 planes) and of its 1/diagonal.
+extern "C" int pb_packed27_size(int64_t n, int64_t* coupling_bytes, int64_t* inverse_bytes) {
+    if (!level_side_ok(n)) return fail(PB_ERR_INVALID, "packed27 size: bad side");
+    const Packed pk = packed_of((int)n);
+    if (coupling_bytes) *coupling_bytes = 26 * pk.cs * (int64_t)sizeof(__half);
+    if (inverse_bytes) *inverse_bytes = pk.cs * (int64_t)sizeof(float);
+    return PB_OK;
+}
+
+// Packs a 27-point level (14 planes): per colour c, couplings h_c and 1/diagonal inv_c.
+extern "C" int pb_pack27_f32(const float* coef, int64_t n, void* h0, void* h1, float* inv0, float* inv1,
+                             void* stream) {
+    if (!level_side_ok(n) || !coef || !h0 || !h1 || !inv0 || !inv1) return fail(PB_ERR_INVALID, "pack27: bad args");
+    const dim3 block(32, 8);
+    pack27_kernel<<<node_grid((int)n, block), block, 0, (cudaStream_t)stream>>>(
+        coef, padded_size((int)n), geom((int)n), packed_of((int)n), (__half*)h0, (__half*)h1, inv0, inv1);
+    PB_CHECK_LAUNCH("pack27_kernel");
+    return PB_OK;
+}
+
+// One red-black ordered sweep e_next <- S(e_prev) on a packed level (e_prev null: from zero).
+extern "C" int pb_relax27p_f32(const float* e_prev, float* e_next, const float* rhs, const void* h0, const void* h1,
+                               const float* inv0, const float* inv1, int64_t n, void* stream) {
+    if (!level_side_ok(n) || !e_next || !rhs || !h0 || !h1 || !inv0 || !inv1 || e_prev == e_next)
+        return fail(PB_ERR_INVALID, "relax27p: bad args");
+    cudaStream_t s = (cudaStream_t)stream;
+    const Geom g = geom((int)n);
+    const Packed pk = packed_of((int)n);
+    const dim3 block(32, 8);
+    const dim3 grid((pk.Pc + 31) / 32, ((int)n + 7) / 8, (int)n);
+    const __half *a = (const __half*)h0, *b = (const __half*)h1;
+    if (e_prev) {
+        relax27p_kernel<0, false><<<grid, block, 0, s>>>(e_prev, e_next, rhs, a, inv0, g, pk);
+        PB_CHECK_LAUNCH("relax27p_kernel");
+        relax27p_kernel<1, false><<<grid, block, 0, s>>>(e_prev, e_next, rhs, b, inv1, g, pk);
+    } else {
+        relax27p_kernel<0, true><<<grid, block, 0, s>>>(nullptr, e_next, rhs, a, inv0, g, pk);
+        PB_CHECK_LAUNCH("relax27p_kernel");
+        relax27p_kernel<1, true><<<grid, block, 0, s>>>(nullptr, e_next, rhs, b, inv1, g, pk);
+    }
+    PB_CHECK_LAUNCH("relax27p_kernel");
+    return PB_OK;
+}
+
+// res = weights * (rhs - A e) with the packed operator, then coarse_rhs = P^T res / 8.
+extern "C" int pb_residual_restrict27p_f32(const float* e, const float* rhs, const void* h0, const void* h1,
+                                           const float* inv0, const float* inv1, const float* weights, int64_t n,
+                                           float* res, float* coarse_rhs, void* stream) {
+    if (!level_side_ok(n) || n < 5 || !e || !rhs || !h0 || !h1 || !inv0 || !inv1 || !weights || !res || !coarse_rhs)
+        return fail(PB_ERR_INVALID, "residual_restrict27p: bad args");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int fn = (int)n, cn = (fn + 1) / 2;
+    const dim3 block(32, 8);
+    residual27p_kernel<<<node_grid(fn, block), block, 0, s>>>(e, rhs, (const __half*)h0, (const __half*)h1, inv0,
+                                                               inv1, weights, geom(fn), packed_of(fn), res);
+    PB_CHECK_LAUNCH("residual27p_kernel");
+    restrict27_kernel<<<node_grid(cn, block), block, 0, s>>>(res, geom(fn), coarse_rhs, geom(cn));
+    PB_CHECK_LAUNCH("restrict27_kernel");
     return PB_OK;
 }

@@ -22,7 +22,8 @@ per FP64 residual, eager launches.
 The FP32 cycle: level 0 is the reference's operator with its red-black
 Gauss-Seidel smoother, 3 sweeps each way (core.py:141-193); the coarser
 levels are Galerkin operators with screening-scaled transfers (mg27.cu),
-smoothed by COARSE_SWEEPS sweeps each way, which cut the cycles needed for a
+smoothed by COARSE_SWEEPS sweeps each way (on levels of side > 9 with their
+couplings packed per colour in FP16), which cut the cycles needed for a
 given residual 2-4x against the reference's rediscretised hierarchy.  Levels
 of side <= 9 run in a single launch, the 3^3 level solved exactly with its
 inverse (built once per set-up).  Convergence is always measured with the
@@ -81,9 +82,23 @@ class Level32:
         self.D = zeros() if first else None
         self.coef = None if self.seven else zeros(14)
 
+        self.packed = None
+
+    def pack(self, device: torch.device, lib) -> None:
+        """Per-colour packed FP16 couplings and 1/diagonal for the multi-block
+        27-point kernels (mg27.cu); filled by Hierarchy32.setup."""
+        hb, ib = ctypes.c_int64(), ctypes.c_int64()
+        nat.check(lib.pb_packed27_size(self.n, ctypes.byref(hb), ctypes.byref(ib)), "packed27 size")
+        h = lambda: torch.zeros(hb.value // 2, dtype=torch.float16, device=device)
+        f = lambda: torch.zeros(ib.value // 4, dtype=torch.float32, device=device)
+        self.packed = (h(), h(), f(), f())
+
+    def packed_ptrs(self) -> tuple:
+        return tuple(t.data_ptr() for t in self.packed)
+
     def tensors(self) -> list:
         return [t for t in (self.invD, self.rhs, self.res, self.ea, self.eb, self.weights, self.D, self.coef)
-                if t is not None]
+                if t is not None] + list(self.packed or ())
 
 
 class Hierarchy32:
@@ -101,6 +116,9 @@ class Hierarchy32:
         self.sizes = level_sizes(n)
         self.levels = [Level32(m, device, self.lib, i == 0) for i, m in enumerate(self.sizes)]
         self.first_coarse = next(i for i, m in enumerate(self.sizes) if m <= COARSE_N)
+        for lv in self.levels[:self.first_coarse]:
+            if not lv.seven:
+                lv.pack(device, self.lib)
         self.inverse = torch.zeros(27 * 27, dtype=torch.float32, device=device)  # of the 3^3 level
         tail = self.levels[self.first_coarse:]
         k = len(tail)
@@ -143,6 +161,9 @@ class Hierarchy32:
                                         s), "galerkin")
             nat.check(L.pb_level27_finish_f32(lv.coef.data_ptr(), lv.n, lv.invD.data_ptr(), lv.weights.data_ptr(), s),
                       "level27 finish")
+        for lv in self.levels:
+            if lv.packed is not None:
+                nat.check(L.pb_pack27_f32(lv.coef.data_ptr(), lv.n, *lv.packed_ptrs(), s), "pack27")
         nat.check(L.pb_coarse_inverse_f32(self.levels[-1].coef.data_ptr(), 3, self.inverse.data_ptr(), s),
                   "coarse inverse")
 
@@ -155,8 +176,8 @@ class Hierarchy32:
                       "prolong32")
             mode = 0
         if not lv.seven:
-            nat.check(L.pb_relax27_f32(None if mode == 1 else src.data_ptr(), dst.data_ptr(), lv.rhs.data_ptr(),
-                                       lv.coef.data_ptr(), lv.invD.data_ptr(), lv.n, s), "relax27")
+            nat.check(L.pb_relax27p_f32(None if mode == 1 else src.data_ptr(), dst.data_ptr(), lv.rhs.data_ptr(),
+                                        *lv.packed_ptrs(), lv.n, s), "relax27p")
             return
         probe = PROBE if (PROBE is not None and lv is self.levels[0]) else None
         if probe is not None:
@@ -196,9 +217,9 @@ class Hierarchy32:
                                                  lv.weights.data_ptr(), nxt.rhs.data_ptr(), lv.n, s),
                       "residual_restrict32")
         else:
-            nat.check(L.pb_residual_restrict27_f32(src.data_ptr(), lv.rhs.data_ptr(), lv.coef.data_ptr(),
-                                                   lv.weights.data_ptr(), lv.n, lv.res.data_ptr(),
-                                                   nxt.rhs.data_ptr(), s), "residual_restrict27")
+            nat.check(L.pb_residual_restrict27p_f32(src.data_ptr(), lv.rhs.data_ptr(), *lv.packed_ptrs(),
+                                                    lv.weights.data_ptr(), lv.n, lv.res.data_ptr(),
+                                                    nxt.rhs.data_ptr(), s), "residual_restrict27p")
         coarse = self.v_cycle(level + 1, pre, post)
         self._sweep(lv, src, dst, 2, coarse)  # post-smoothing; the first adds the correction
         src, dst = dst, src

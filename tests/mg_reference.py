@@ -165,3 +165,53 @@ def v_cycle(ops, ws, sizes, level, rhs, pre=3, post=3, coarse_sweeps=2):
     for _ in range(post):
         e = relax(A, e, rhs, n)
     return e
+
+
+def packed_offsets():
+    """The 26 coupling offsets (dx, dy, dz) of a packed level, plane order."""
+    return [(dx, dy, dz) for dz in (-1, 0, 1) for dy in (-1, 0, 1) for dx in (-1, 0, 1) if dx or dy or dz]
+
+
+def pack(A, n):
+    """Per-colour packed couplings (FP16, 26 x n x n x Pc) and 1/diagonal (FP32,
+    n x n x Pc) of a 27-point level, as pb_pack27_f32 computes them from FP32
+    coefficients: inv = 1/d and c_K = (-a_JK) * inv in FP32, rounded to FP16."""
+    pc = (n + 1) // 2
+    A = A.tocsr()
+    d = A.diagonal().astype(np.float32)
+    inv = (np.float32(1.0) / d).astype(np.float32)
+    z, y, x = coords(n)
+    h = [np.zeros((26, n, n, pc), np.float16) for _ in range(2)]
+    iv = [np.zeros((n, n, pc), np.float32) for _ in range(2)]
+    dense = {}
+    coo = A.tocoo()
+    for r, c, v in zip(coo.row, coo.col, coo.data):
+        dense[(r, c)] = v
+    for j in range(n ** 3):
+        col = (x[j] + y[j] + z[j]) & 1
+        iv[col][z[j], y[j], x[j] >> 1] = inv[j]
+        for k, (dx, dy, dz) in enumerate(packed_offsets()):
+            xx, yy, zz = x[j] + dx, y[j] + dy, z[j] + dz
+            a = 0.0
+            if 0 <= xx < n and 0 <= yy < n and 0 <= zz < n:
+                a = dense.get((j, (zz * n + yy) * n + xx), 0.0)
+            h[col][k, z[j], y[j], x[j] >> 1] = np.float16(np.float32(-np.float32(a)) * inv[j])
+    return h[0], h[1], iv[0], iv[1]
+
+
+def packed_operator(h0, h1, inv0, inv1, n):
+    """The row operator a packed level applies: a_JJ = 1/inv_J, a_JK = -c_K / inv_J."""
+    z, y, x = coords(n)
+    colour = (x + y + z) & 1
+    i = x >> 1
+    inv = np.where(colour == 0, inv0[z, y, i], inv1[z, y, i]).astype(np.float64)
+    idx = np.arange(n ** 3)
+    rows, cols, vals = [idx], [idx], [1.0 / inv]
+    for k, (dx, dy, dz) in enumerate(packed_offsets()):
+        c = np.where(colour == 0, h0[k, z, y, i], h1[k, z, y, i]).astype(np.float64)
+        ok = (x + dx >= 0) & (x + dx < n) & (y + dy >= 0) & (y + dy < n) & (z + dz >= 0) & (z + dz < n) & (c != 0)
+        rows.append(idx[ok])
+        cols.append(idx[ok] + dx + dy * n + dz * n * n)
+        vals.append(-c[ok] / inv[ok])
+    return sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                         shape=(n ** 3, n ** 3)).tocsr()

@@ -3,10 +3,12 @@ transfers) against the CPU restatement in tests/mg_reference.py.
 
 Tolerances (max norm, relative to the largest magnitude of the compared
 quantity): Galerkin planes 3e-5 (FP32 products and sums of up to ~1300 terms,
-compounded over levels); weights and 1/diagonal 1e-5; a single sweep,
+compounded over levels); weights and 1/diagonal 1e-5; packed FP16 couplings
+exactly (the same FP32 operations, then rounding to FP16); a single sweep,
 residual, restriction or prolongation 2e-6 to 4e-6 of the largest term,
-evaluated on the GPU's own FP32 planes so only that kernel's rounding is
-measured; the 3^3 inverse 1e-5; whole cycles 1e-4."""
+evaluated on the GPU's own coefficients (FP32 planes, or the packed FP16
+couplings) so only that kernel's rounding is measured; the 3^3 inverse 1e-5;
+whole cycles 1e-4."""
 
 import numpy as np
 import pytest
@@ -49,6 +51,13 @@ def gpu_planes(L, lv):
     return np.stack([from_padded(L, lv.coef[k], lv.n) for k in range(14)])
 
 
+def gpu_packed(lv):
+    """The GPU's packed arrays of a level as (h0, h1, inv0, inv1) NumPy arrays."""
+    n, pc = lv.n, (lv.n + 1) // 2
+    h0, h1, i0, i1 = (t.cpu().numpy() for t in lv.packed)
+    return (h0.reshape(26, n, n, pc), h1.reshape(26, n, n, pc), i0.reshape(n, n, pc), i1.reshape(n, n, pc))
+
+
 def stream():
     return torch.cuda.current_stream().cuda_stream
 
@@ -59,6 +68,8 @@ def gpu_ops(L, h):
     for lv in h.levels:
         if lv.coef is None:  # level 0 with the reference's 7-point operator
             ops.append(mg.operator7(from_padded(L, lv.D, lv.n)))
+        elif lv.packed is not None:  # the rounded couplings the packed kernels apply
+            ops.append(mg.packed_operator(*gpu_packed(lv), lv.n))
         else:
             ops.append(mg.from_planes(gpu_planes(L, lv), lv.n))
         ws.append(from_padded(L, lv.weights, lv.n).ravel())
@@ -85,14 +96,26 @@ def test_galerkin_levels_match_restatement(L, n):
             assert ghosts_zero(L, lv.coef[k], lv.n)
 
 
+@pytest.mark.parametrize("n", [33, 65])
+def test_pack27_matches_restatement(L, n):
+    """Packed FP16 couplings and FP32 1/diagonal of level 1, exactly."""
+    h = gpu_hierarchy(n, shell_screen(n, 2 * n))
+    lv = h.levels[1]
+    want = mg.pack(mg.from_planes(gpu_planes(L, lv), lv.n), lv.n)
+    for got, w in zip(gpu_packed(lv), want):
+        assert np.array_equal(got.view(np.uint16) if got.dtype == np.float16 else got.view(np.uint32),
+                              w.view(np.uint16) if w.dtype == np.float16 else w.view(np.uint32))
+
+
 @pytest.mark.parametrize("n", [33, 65, 129])
-def test_relax27_and_transfers(L, n):
-    """One sweep (from a start and from zero), the residual with the scaled
-    restriction, and the scaled prolongation on level 1 (27-point)."""
+def test_relax27p_and_transfers(L, n):
+    """One sweep (from a start and from zero) and the residual with the scaled
+    restriction on a packed level (level 1), against the restated packed
+    operator; the scaled prolongation on level 1."""
     h = gpu_hierarchy(n, shell_screen(n, 3 * n))
     lv, nxt = h.levels[1], h.levels[2]
     m, cm = lv.n, nxt.n
-    A = mg.from_planes(gpu_planes(L, lv), m)
+    A = mg.packed_operator(*gpu_packed(lv), m)
     s1 = from_padded(L, lv.weights, m).ravel()
     rng = np.random.default_rng(n)
     e = rng.normal(size=(m,) * 3).astype(np.float32).astype(np.float64)
@@ -104,16 +127,16 @@ def test_relax27_and_transfers(L, n):
     terms = np.abs(A).sum(axis=1).max() * np.abs(e).max() + np.abs(rhs).max()
     dmin = A.diagonal().min()
     for zero in (False, True):
-        assert L.pb_relax27_f32(None if zero else e_in.data_ptr(), out.data_ptr(), lv.rhs.data_ptr(),
-                                lv.coef.data_ptr(), lv.invD.data_ptr(), m, stream()) == 0, L.pb_last_error()
+        assert L.pb_relax27p_f32(None if zero else e_in.data_ptr(), out.data_ptr(), lv.rhs.data_ptr(),
+                                 *lv.packed_ptrs(), m, stream()) == 0, L.pb_last_error()
         want = mg.relax(A, e, rhs, m, zero=zero)
         # two dependent half-sweeps: an FP32 sum of 27 terms each, divided by the diagonal
         assert np.abs(from_padded(L, out, m) - want).max() <= 4e-6 * terms / dmin
         assert ghosts_zero(L, out, m)
     coarse_rhs = torch.zeros_like(nxt.rhs)
-    assert L.pb_residual_restrict27_f32(e_in.data_ptr(), lv.rhs.data_ptr(), lv.coef.data_ptr(),
-                                        lv.weights.data_ptr(), m, lv.res.data_ptr(), coarse_rhs.data_ptr(),
-                                        stream()) == 0
+    assert L.pb_residual_restrict27p_f32(e_in.data_ptr(), lv.rhs.data_ptr(), *lv.packed_ptrs(),
+                                         lv.weights.data_ptr(), m, lv.res.data_ptr(), coarse_rhs.data_ptr(),
+                                         stream()) == 0
     want_c, want_r = mg.residual_restrict(A, s1, e, rhs, m)
     assert np.abs(from_padded(L, lv.res, m) - want_r).max() <= 2e-6 * terms
     assert np.abs(from_padded(L, coarse_rhs, cm) - want_c).max() <= 2e-6 * terms
