@@ -217,6 +217,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     torch.cuda.synchronize()
     solver32.PROBE = None
     sweep_ms = [a.elapsed_time(b) for a, b, mode in probe if mode == 0]
+    kernel_table = kernel_rooflines(eng, n_side, _native.lib()) if rank == 0 and not args.profile else None
     if args.profile:
         if rank == 0:
             print(json.dumps({"profile": True, "value": value, "launches_per_step": launches / args.steps}))
@@ -317,10 +318,63 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
                 "d2h_bytes_per_step": int(d2h), "p50_ms": round(statistics.median(per_e2e), 3),
                 "p99_ms": round(float(np.percentile(per_e2e, 99)), 3)},
         "roofline": roofline,
+        "kernels": kernel_table,
         "gpu_launches": int(launches),
         "clocks": clock_info,
     }
     return result
+
+
+def kernel_rooflines(eng, n: int, L) -> list:
+    """The other hot kernels of an FP32-refined solve, each timed with CUDA
+    events on the engine's stream (20 launches after one warm-up, on the timed
+    solves' engine and buffers), against its algorithmic bytes per launch
+    (each array read or written once) and the measured HBM copy peak."""
+    import torch
+
+    from mojo_poissonrecon_b200 import _native as nat
+
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json"), encoding="utf8") as f:
+            peak = float(json.loads(f.read()).get("hbm_gbs", 6650.0))
+    except OSError:
+        peak = 6650.0
+    h = eng.h
+    l0, l1 = h.levels[0], h.levels[1]
+    N, N1 = n ** 3, l1.n ** 3
+    p0, p1 = (t.data_ptr() for t in eng.ps)
+    x0, x1 = (t.data_ptr() for t in eng.xs)
+    out = []
+
+    def timed(name, fn, nbytes):
+        with torch.cuda.stream(eng.stream):
+            s = nat.stream_handle()
+            fn(s)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(20):
+                fn(s)
+            b.record()
+            b.synchronize()
+        us = a.elapsed_time(b) / 20 * 1e3
+        gbs = nbytes / (us * 1e-6) / 1e9
+        out.append({"kernel": name, "us": round(us, 1), "algorithmic_bytes": int(nbytes),
+                    "achieved_gbs": round(gbs, 1), "frac_of_measured_hbm": round(gbs / peak, 3)})
+
+    timed("residual_restrict32_kernel (level 0)", lambda s: L.pb_residual_restrict_f32(
+        l0.ea.data_ptr(), l0.rhs.data_ptr(), l0.D.data_ptr(), l0.weights.data_ptr(), l1.rhs.data_ptr(), n, s),
+        16 * N + 4 * N1)
+    timed("prolong_add32_kernel (level 0)", lambda s: L.pb_prolong_fac_f32(
+        l1.ea.data_ptr(), l0.eb.data_ptr(), l0.weights.data_ptr(), n, s), 12 * N + 4 * N1)
+    timed("relax27p_kernel x2 (one sweep, level 1, packed FP16)", lambda s: L.pb_relax27p_f32(
+        l1.ea.data_ptr(), l1.eb.data_ptr(), l1.rhs.data_ptr(), *l1.packed_ptrs(), l1.n, s), 68 * N1)
+    timed("fcg::direction_sums_kernel", lambda s: L.pb_fcg_direction_f64(
+        l0.ea.data_ptr(), p0, p1, l0.rhs.data_ptr(), eng.screen.data_ptr(), n, eng.pw, eng.scal.data_ptr(),
+        eng.flags.data_ptr(), eng.ws_ptr, eng.ws_size, s), 24 * N)
+    timed("fcg::update_residual_kernel", lambda s: L.pb_fcg_update_f64(
+        l0.ea.data_ptr(), p0, p1, x0, x1, eng.b.data_ptr(), eng.screen.data_ptr(), l0.rhs.data_ptr(), n, eng.pw,
+        eng.scal.data_ptr(), eng.flags.data_ptr(), eng.ws_ptr, eng.ws_size, s), 56 * N)
+    return out
 
 
 def read_profile_traffic():

@@ -96,6 +96,28 @@ __global__ void splat_records_kernel(const double* __restrict__ points, const do
     if (threadIdx.x == 0 && block_accepted) atomicAdd(accepted, (unsigned long long)block_accepted);
 }
 
+// Runs of records with the same node are consumed kRun at a time: the keys
+// of the next kRun records are loaded together and the run's length within
+// them counted, then their values and gathered weights are loaded together,
+// and only then added, one after another in record order.  The additions are
+// exactly the serial ones; only the loads overlap.
+constexpr int kRun = 8;
+
+__device__ __forceinline__ int run_length(const uint32_t* __restrict__ keys, int64_t k, int64_t records,
+                                          uint32_t node) {
+    uint32_t kk[kRun];
+#pragma unroll
+    for (int t = 0; t < kRun; ++t) kk[t] = k + t < records ? keys[k + t] : node + 1;
+    int m = 0;
+    bool run = true;
+#pragma unroll
+    for (int t = 0; t < kRun; ++t) {
+        run = run && kk[t] == node;
+        m += run;
+    }
+    return m;
+}
+
 // Pass 1 (capi.mojo:171-172): density += 2w, screen += w, per node in point order.
 __global__ void splat_density_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
                                      int64_t records, uint32_t sentinel, const double* __restrict__ weight,
@@ -105,10 +127,18 @@ __global__ void splat_density_kernel(const uint32_t* __restrict__ keys, const ui
     const uint32_t node = keys[j];
     if (node == sentinel || (j > 0 && keys[j - 1] == node)) return;
     double d = density[node], s = screen[node];
-    for (int64_t k = j; k < records && keys[k] == node; ++k) {
-        double w = weight[vals[k]];
-        d += 2.0 * w;
-        s += w;
+    for (int64_t k = j;; k += kRun) {
+        const int m = run_length(keys, k, records, node);
+        double w[kRun];
+#pragma unroll
+        for (int t = 0; t < kRun; ++t) w[t] = t < m ? weight[vals[k + t]] : 0.0;
+#pragma unroll
+        for (int t = 0; t < kRun; ++t)
+            if (t < m) {
+                d += 2.0 * w[t];
+                s += w[t];
+            }
+        if (m < kRun) break;
     }
     density[node] = d;
     screen[node] = s;
@@ -172,13 +202,29 @@ __global__ void splat_vector_kernel(const uint32_t* __restrict__ keys, const uin
     const uint32_t node = keys[j];
     if (node == sentinel || (j > 0 && keys[j - 1] == node)) return;
     double ax = vx[node], ay = vy[node], az = vz[node];
-    for (int64_t k = j; k < records && keys[k] == node; ++k) {
-        const uint32_t r = vals[k];
-        const double vw = weight[r];
-        const double* u = unit_normals + 3 * (int64_t)(r >> 3);
-        ax -= u[0] * vw;
-        ay -= u[1] * vw;
-        az -= u[2] * vw;
+    for (int64_t k = j;; k += kRun) {
+        const int m = run_length(keys, k, records, node);
+        double vw[kRun], u0[kRun], u1[kRun], u2[kRun];
+#pragma unroll
+        for (int t = 0; t < kRun; ++t) {
+            vw[t] = u0[t] = u1[t] = u2[t] = 0.0;
+            if (t < m) {
+                const uint32_t r = vals[k + t];
+                const double* u = unit_normals + 3 * (int64_t)(r >> 3);
+                vw[t] = weight[r];
+                u0[t] = u[0];
+                u1[t] = u[1];
+                u2[t] = u[2];
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < kRun; ++t)
+            if (t < m) {
+                ax -= u0[t] * vw[t];
+                ay -= u1[t] * vw[t];
+                az -= u2[t] * vw[t];
+            }
+        if (m < kRun) break;
     }
     vx[node] = ax;
     vy[node] = ay;
