@@ -290,9 +290,9 @@ int pb_level27_from7_f32(const float *D, int64_t n, float *coef, void *stream);
 /* invD = 1 / diagonal and the prolongation weights of a 27-point level. */
 int pb_level27_finish_f32(const float *coef, int64_t n, float *invD, float *weights, void *stream);
 /* Packed 27-point levels: per colour c, the 26 couplings divided by the
- * diagonal, -a(J, J+K) / a(J, J), in FP16 (h_c, 26 planes) and 1/a(J, J) in
- * FP32 (inv_c), over the colour's nodes numbered compactly; sizes in bytes
- * from pb_packed27_size.  Relaxation and residual of a packed level both use
+ * diagonal, -a(J, J+K) / a(J, J), in FP16 (h_c, 32 halves per node, node-major)
+ * and 1/a(J, J) in FP32 (inv_c), over the colour's nodes numbered compactly;
+ * sizes in bytes from pb_packed27_size.  Relaxation and residual of a packed level both use
  * the rounded couplings. */
 int pb_packed27_size(int64_t n, int64_t *coupling_bytes, int64_t *inverse_bytes);
 int pb_pack27_f32(const float *coef, int64_t n, void *h0, void *h1, float *inv0, float *inv1, void *stream);

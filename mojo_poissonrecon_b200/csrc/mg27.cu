@@ -263,9 +263,10 @@ __global__ void __launch_bounds__(256) restrict27_kernel(const float* __restrict
 // bytes per node and sweep from DRAM on the 129^3 level.  Packed, each colour's nodes are
 // numbered compactly (row (y, z), i-th node of the colour: x = 2i + ((y+z+c)&1),
 // compact index (z*n + y)*Pc + i, Pc = (n+1)/2) and hold their 26 couplings
-// divided by the diagonal, c_K = -a(J, J+K) / a(J, J), in FP16 (|c_K| <= 1;
-// plane k = offset index over (dz, dy, dx) in lexicographic order, the centre
-// skipped), and 1/a(J, J) in FP32.  Relaxation and residual of the level both
+// divided by the diagonal, c_K = -a(J, J+K) / a(J, J), in FP16 (|c_K| <= 1),
+// node-major: 32 halves (64 bytes, the last 6 zero) per node, coupling k =
+// offset index over (dz, dy, dx) in lexicographic order with the centre
+// skipped, read as four 16-byte loads; and 1/a(J, J) in FP32.  Relaxation and residual of the level both
 // use the rounded couplings, so the level's operator stays one operator:
 //   e_new(J) = invD(J) rhs(J) + sum_K c_K e(J+K)
 //   r(J)     = rhs(J) - (e(J) - sum_K c_K e(J+K)) / invD(J)
@@ -276,9 +277,11 @@ __host__ __device__ constexpr int packed_index(int dx, int dy, int dz) {
     return k < 13 ? k : k - 1;  // the centre (13) is not stored
 }
 
+constexpr int kPackedStride = 32;  // halves per node
+
 struct Packed {
     int n, Pc;
-    int64_t cs;  // compact nodes per colour = n * n * Pc (plane stride of the coupling array)
+    int64_t cs;  // compact nodes per colour = n * n * Pc
     __host__ __device__ __forceinline__ int64_t at(int i, int y, int z) const { return ((int64_t)z * n + y) * Pc + i; }
 };
 
@@ -300,8 +303,10 @@ __global__ void __launch_bounds__(256) pack27_kernel(const float* __restrict__ c
     const int64_t q = pk.at(x >> 1, y, z);
     const int64_t p = g.at(x, y, z);
     const float inv = 1.0f / c[p];
-    __half* h = colour ? h1 : h0;
     (colour ? i1 : i0)[q] = inv;
+    __align__(16) __half v[kPackedStride];
+#pragma unroll
+    for (int k = 26; k < kPackedStride; ++k) v[k] = __float2half_rn(0.0f);
 #pragma unroll
     for (int dz = -1; dz <= 1; ++dz)
 #pragma unroll
@@ -309,8 +314,23 @@ __global__ void __launch_bounds__(256) pack27_kernel(const float* __restrict__ c
 #pragma unroll
             for (int dx = -1; dx <= 1; ++dx) {
                 if (!(dx || dy || dz)) continue;
-                h[packed_index(dx, dy, dz) * pk.cs + q] = __float2half_rn(-coupling(c, cs, g, p, dx, dy, dz) * inv);
+                v[packed_index(dx, dy, dz)] = __float2half_rn(-coupling(c, cs, g, p, dx, dy, dz) * inv);
             }
+    uint4* dst = reinterpret_cast<uint4*>((colour ? h1 : h0) + q * kPackedStride);
+    const uint4* src = reinterpret_cast<const uint4*>(v);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) dst[k] = src[k];
+}
+
+// The 26 couplings of compact node q, as floats.
+__device__ __forceinline__ void load_couplings(const __half* __restrict__ h, int64_t q, float* c) {
+    const uint4* src = reinterpret_cast<const uint4*>(h + q * kPackedStride);
+    __align__(16) __half v[kPackedStride];
+    uint4* d = reinterpret_cast<uint4*>(v);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) d[k] = src[k];
+#pragma unroll
+    for (int k = 0; k < 26; ++k) c[k] = __half2float(v[k]);
 }
 
 // One colour pass on a packed level: nodes of colour COLOUR get
@@ -326,6 +346,8 @@ __global__ void __launch_bounds__(256) relax27p_kernel(const float* __restrict__
     const int n = g.n;
     if (x >= n || y >= n) return;
     const int64_t p = g.at(x, y, z), q = pk.at(i, y, z);
+    float cf[26];
+    load_couplings(h, q, cf);
     float s = 0.0f;
 #pragma unroll
     for (int dz = -1; dz <= 1; ++dz)
@@ -338,7 +360,7 @@ __global__ void __launch_bounds__(256) relax27p_kernel(const float* __restrict__
                 if (ZERO && !(COLOUR == 1 && other)) continue;
                 const int64_t o = p + offset_of(g, dx, dy, dz);
                 const float v = (COLOUR == 1 && other) ? next[o] : prev[o];
-                s += __half2float(h[packed_index(dx, dy, dz) * pk.cs + q]) * v;
+                s += cf[packed_index(dx, dy, dz)] * v;
             }
     next[p] = inv[q] * rhs[p] + s;
 }
@@ -356,6 +378,8 @@ __global__ void __launch_bounds__(256) residual27p_kernel(const float* __restric
     const int colour = (x + y + z) & 1;
     const __half* __restrict__ h = colour ? h1 : h0;
     const int64_t p = g.at(x, y, z), q = pk.at(x >> 1, y, z);
+    float cf[26];
+    load_couplings(h, q, cf);
     float s = 0.0f;
 #pragma unroll
     for (int dz = -1; dz <= 1; ++dz)
@@ -364,7 +388,7 @@ __global__ void __launch_bounds__(256) residual27p_kernel(const float* __restric
 #pragma unroll
             for (int dx = -1; dx <= 1; ++dx) {
                 if (!(dx || dy || dz)) continue;
-                s += __half2float(h[packed_index(dx, dy, dz) * pk.cs + q]) * e[p + offset_of(g, dx, dy, dz)];
+                s += cf[packed_index(dx, dy, dz)] * e[p + offset_of(g, dx, dy, dz)];
             }
     const float inv = colour ? i1[q] : i0[q];
     res[p] = fac[p] * (rhs[p] - (e[p] - s) / inv);
@@ -647,11 +671,11 @@ extern "C" int pb_coarse27_cycle_f32(int64_t count, const int64_t* sizes, const 
 }
 
 // ---- packed levels ----------------------------------------------------------------
-// Bytes of one colour's packed couplings (26 FP16 planes) and of its 1/diagonal.
+// Bytes of one colour's packed couplings (32 FP16 per node) and of its 1/diagonal.
 extern "C" int pb_packed27_size(int64_t n, int64_t* coupling_bytes, int64_t* inverse_bytes) {
     if (!level_side_ok(n)) return fail(PB_ERR_INVALID, "packed27 size: bad side");
     const Packed pk = packed_of((int)n);
-    if (coupling_bytes) *coupling_bytes = 26 * pk.cs * (int64_t)sizeof(__half);
+    if (coupling_bytes) *coupling_bytes = kPackedStride * pk.cs * (int64_t)sizeof(__half);
     if (inverse_bytes) *inverse_bytes = pk.cs * (int64_t)sizeof(float);
     return PB_OK;
 }

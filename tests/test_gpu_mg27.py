@@ -55,7 +55,9 @@ def gpu_packed(lv):
     """The GPU's packed arrays of a level as (h0, h1, inv0, inv1) NumPy arrays."""
     n, pc = lv.n, (lv.n + 1) // 2
     h0, h1, i0, i1 = (t.cpu().numpy() for t in lv.packed)
-    return (h0.reshape(26, n, n, pc), h1.reshape(26, n, n, pc), i0.reshape(n, n, pc), i1.reshape(n, n, pc))
+    planes = lambda h: np.ascontiguousarray(np.moveaxis(h.reshape(n, n, pc, 32)[..., :26], -1, 0))
+    assert not h0.reshape(n, n, pc, 32)[..., 26:].any() and not h1.reshape(n, n, pc, 32)[..., 26:].any()
+    return (planes(h0), planes(h1), i0.reshape(n, n, pc), i1.reshape(n, n, pc))
 
 
 def stream():
