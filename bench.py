@@ -223,20 +223,22 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
             print(json.dumps({"profile": True, "value": value, "launches_per_step": launches / args.steps}))
         return None
 
-    fp64_ms, per64 = timed(fp64_device, max(3, args.steps // 2))
-    value64 = world * len(per64) / (fp64_ms / 1e3)
-
-    # end to end through the public API with host buffers
+    # end to end through the public API with host buffers, on the same warm
+    # engine as the headline (one untimed call after the kernel table above)
     mesh_holder = {}
 
     def e2e_step():
         mesh_holder["m"] = refined_e2e()
 
-    e2e_ms, per_e2e = timed(e2e_step, max(3, args.steps // 2))
+    e2e_step()
+    e2e_ms, per_e2e = timed(e2e_step, args.steps)
     mesh = mesh_holder["m"]
     h2d = 2 * args.points * 3 * 8
     d2h = mesh.vertices.nbytes + mesh.faces.nbytes + mesh.density.nbytes
     e2e_value = world * len(per_e2e) / (e2e_ms / 1e3)
+
+    fp64_ms, per64 = timed(fp64_device, max(3, args.steps // 2))
+    value64 = world * len(per64) / (fp64_ms / 1e3)
 
     # accuracy of the refined result against the FP64 solve (not timed)
     keep_solution = {}
@@ -370,10 +372,10 @@ def kernel_rooflines(eng, n: int, L) -> list:
         l1.ea.data_ptr(), l1.eb.data_ptr(), l1.rhs.data_ptr(), *l1.packed_ptrs(), l1.n, s), 68 * N1)
     timed("fcg::direction_sums_kernel", lambda s: L.pb_fcg_direction_f64(
         l0.ea.data_ptr(), p0, p1, l0.rhs.data_ptr(), eng.screen.data_ptr(), n, eng.pw, eng.scal.data_ptr(),
-        eng.flags.data_ptr(), eng.ws_ptr, eng.ws_size, s), 24 * N)
+        eng.flags.data_ptr(), eng.ws_ptr, eng.ws_size, s), 20 * N)
     timed("fcg::update_residual_kernel", lambda s: L.pb_fcg_update_f64(
         l0.ea.data_ptr(), p0, p1, x0, x1, eng.b.data_ptr(), eng.screen.data_ptr(), l0.rhs.data_ptr(), n, eng.pw,
-        eng.scal.data_ptr(), eng.flags.data_ptr(), eng.ws_ptr, eng.ws_size, s), 56 * N)
+        eng.scal.data_ptr(), eng.flags.data_ptr(), eng.ws_ptr, eng.ws_size, s), 48 * N)
     return out
 
 

@@ -199,16 +199,17 @@ int pb_defect_f64(const double *x_old, const float *e, double *x_new, const doub
  * repeats V-cycles, core.py:274-285).  Device scalars scal[0..4]: (p, Ap),
  * beta, alpha, (p, r), ||b - A x||^2; flags[0] != 0 on the first step,
  * flags[1] = iterations done, whose parity selects the buffers: directions
- * p[it & 1] -> p[(it+1) & 1], iterates x[it & 1] -> x[(it+1) & 1].  Every
- * iteration touches the same pointers, so one can be captured in a graph. */
+ * p[it & 1] -> p[(it+1) & 1] (dense FP32), iterates x[it & 1] -> x[(it+1) & 1]
+ * (dense FP64).  Every iteration touches the same pointers, so one can be
+ * captured in a graph. */
 size_t pb_fcg_workspace_size(int64_t n);
 /* Pass 1, after z = M(r32): beta, (p, Ap) and alpha from one stencil pass over z. */
-int pb_fcg_direction_f64(const float *z, const double *p0, const double *p1, const float *r32,
+int pb_fcg_direction_f64(const float *z, const float *p0, const float *p1, const float *r32,
                          const double *screen, int64_t n, double point_weight, double *scal, const int *flags,
                          void *workspace, size_t workspace_bytes, void *stream);
 /* Pass 2: p, x += alpha p and the true residual b - A x into r32 (padded FP32),
  * ||b - A x||^2 into scal[4]. */
-int pb_fcg_update_f64(const float *z, double *p0, double *p1, double *x0, double *x1, const double *b,
+int pb_fcg_update_f64(const float *z, float *p0, float *p1, double *x0, double *x1, const double *b,
                       const double *screen, float *r32, int64_t n, double point_weight, double *scal,
                       const int *flags, void *workspace, size_t workspace_bytes, void *stream);
 /* One red-black Gauss-Seidel sweep (colour 0 then colour 1), out of place,
@@ -306,15 +307,22 @@ int pb_residual_restrict27p_f32(const float *e, const float *rhs, const void *h0
                                 float *res, float *coarse_rhs, void *stream);
 /* Inverse (27 x 27, FP32 row-major) of the 27-point level of side 3. */
 int pb_coarse_inverse_f32(const float *coef, int64_t n, float *inverse, void *stream);
-/* The V-cycle below a 27-point level of side <= 17 in one block: count
- * levels, finest first, the last of side 3 and solved with `inverse` (host
- * arrays of device pointers); (pre, post) sweeps on the first level, `inner`
- * each way on the others; rhs[0] holds the right-hand side, e[0] receives the
+/* Levels of side <= 9 (sizes: count levels halving down to 3, finest first)
+ * run in one block from a compact image written at set-up: per level but the
+ * last, the 27 couplings of each node, 1/diagonal and prolongation weights
+ * (host arrays of device pointers to each level's 14 planes, invD and
+ * weights), then the 3^3 inverse.  image: 16-byte aligned, of
+ * pb_coarse27_image_size bytes (0 for invalid sizes). */
+size_t pb_coarse27_image_size(int64_t count, const int64_t *sizes);
+int pb_coarse27_image_f32(int64_t count, const int64_t *sizes, const float *const *coef,
+                          const float *const *invD, const float *const *weights, const float *inverse,
+                          float *image, size_t image_bytes, void *stream);
+/* The V-cycle over those levels in shared memory: (pre, post) sweeps on the
+ * first, `inner` each way on the others, the last solved with its inverse.
+ * rhs: the first level's right-hand side (padded layout); e receives its
  * correction. */
-int pb_coarse27_cycle_f32(int64_t count, const int64_t *sizes, const float *const *coef,
-                          const float *const *invD, const float *const *weights, float *const *e,
-                          float *const *rhs, float *const *res, int64_t pre, int64_t post, int64_t inner,
-                          const float *inverse, void *stream);
+int pb_coarse27_cycle_f32(int64_t count, const int64_t *sizes, const float *image, const float *rhs, float *e,
+                          int64_t pre, int64_t post, int64_t inner, void *stream);
 
 /* ---- host-orchestration helpers (core.py steps done on the device) ---------- */
 

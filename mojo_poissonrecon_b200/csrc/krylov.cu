@@ -19,8 +19,13 @@
 // residual never drifts from the iterate and no final residual pass is needed.
 // x and p alternate between two buffers by iteration parity (flags[1], on the
 // device), so every iteration launches the same kernels on the same pointers
-// and can be captured once in a graph.  Vectors are FP64 and dense except z
-// and r32 (the FP32 padded copy of r that the next V-cycle reads).
+// and can be captured once in a graph.  x, b and the screening are FP64 and
+// dense; z and r32 (the FP32 padded copy of r that the next V-cycle reads) are
+// padded FP32; the direction p is stored in FP32 (dense): x moves along the
+// unrounded z - beta p_prev, the stored copy only orthogonalises the next
+// direction, and the residual is recomputed from x in FP64 every iteration,
+// so the rounding perturbs alpha and beta by ~1e-7 relative and never the
+// measured residual.
 #include "common.cuh"
 
 namespace pb {
@@ -76,8 +81,8 @@ __device__ __forceinline__ int64_t block_index() {
 // no tests.  Compiled for 4 resident blocks per SM (64 registers), which keeps
 // more loads in flight than the occupancy-first default.
 __global__ void __launch_bounds__(kThreads, 4) direction_sums_kernel(const float* __restrict__ z, Pad g,
-                                                                     const double* __restrict__ p0,
-                                                                     const double* __restrict__ p1,
+                                                                     const float* __restrict__ p0,
+                                                                     const float* __restrict__ p1,
                                                                      const float* __restrict__ r32,
                                                                      const double* __restrict__ screen, double pw,
                                                                      const int* __restrict__ flags,
@@ -88,7 +93,7 @@ __global__ void __launch_bounds__(kThreads, 4) direction_sums_kernel(const float
     const int z0 = blockIdx.z * kTZ, z1 = min(n, z0 + kTZ);
     const double h = (double)(n - 1), h2 = h * h;
     const bool first = flags[0] != 0;
-    const double* __restrict__ pp = (flags[1] & 1) ? p1 : p0;
+    const float* __restrict__ pp = (flags[1] & 1) ? p1 : p0;
     double v[4] = {0.0, 0.0, 0.0, 0.0};
     if (x < n && y < n) {
         const int degxy = (x > 0) + (x + 1 < n) + (y > 0) + (y + 1 < n);
@@ -108,7 +113,7 @@ __global__ void __launch_bounds__(kThreads, 4) direction_sums_kernel(const float
             v[0] += zc * az;
             v[2] += zc * rc;
             if (!first) {
-                const double pv = pp[i];
+                const double pv = (double)pp[i];
                 v[1] += az * pv;
                 v[3] += pv * rc;
             }
@@ -179,7 +184,7 @@ struct Halo {
 // every neighbour formed from memory).  Nodes outside the domain hold 0 and
 // the neighbour sum adds x-, x+, y-, y+, z-, z+ in that order.
 __global__ void __launch_bounds__(kUThreads) update_residual_kernel(
-    const float* __restrict__ z, Pad g, double* p0, double* p1, double* x0, double* x1, const double* __restrict__ b,
+    const float* __restrict__ z, Pad g, float* p0, float* p1, double* x0, double* x1, const double* __restrict__ b,
     const double* __restrict__ screen, double pw, const double* __restrict__ scal, const int* __restrict__ flags,
     float* __restrict__ r32, double* __restrict__ part) {
     __shared__ double tile[kUY + 2][kUX + 2];
@@ -192,15 +197,15 @@ __global__ void __launch_bounds__(kUThreads) update_residual_kernel(
     const double h = (double)(n - 1), h2 = h * h;
     const int odd = flags[1] & 1;
     const bool first = flags[0] != 0;
-    const double* __restrict__ pp = odd ? p1 : p0;
-    double* __restrict__ pn = odd ? p0 : p1;
+    const float* __restrict__ pp = odd ? p1 : p0;
+    float* __restrict__ pn = odd ? p0 : p1;
     const double* __restrict__ xc = odd ? x1 : x0;
     double* __restrict__ xn = odd ? x0 : x1;
     const double beta = first ? 0.0 : scal[1], alpha = scal[2];
     const int64_t nn = (int64_t)n * n;
     auto dir_at = [&](int64_t ii, int64_t cc) -> double {
         double val = (double)z[cc];
-        if (!first) val -= beta * pp[ii];
+        if (!first) val -= beta * (double)pp[ii];
         return val;
     };
     const Halo hl(tid, bx, by);
@@ -247,7 +252,7 @@ __global__ void __launch_bounds__(kUThreads) update_residual_kernel(
             s += xb;
             s += xa;
             const int deg = degxy + (k > 0) + up;
-            pn[i] = dm;
+            pn[i] = (float)dm;
             xn[i] = xm;
             const double r = bi - (((double)deg * h2 + pw * sc * h2) * xm - s * h2);
             r32[c] = (float)r;
@@ -321,9 +326,9 @@ static int fcg_check(int64_t n, size_t workspace_bytes, const void* workspace) {
 
 // FCG(1) pass 1 after the preconditioner produced z (padded FP32): the step's
 // scalars into scal[0..3] (scal[0] holds the previous (p, Ap) on entry).
-// p0/p1: the two dense FP64 direction buffers, p_prev = p[flags[1] & 1];
+// p0/p1: the two dense FP32 direction buffers, p_prev = p[flags[1] & 1];
 // r32: the padded FP32 residual the preconditioner read.
-extern "C" int pb_fcg_direction_f64(const float* z, const double* p0, const double* p1, const float* r32,
+extern "C" int pb_fcg_direction_f64(const float* z, const float* p0, const float* p1, const float* r32,
                                     const double* screen, int64_t n, double point_weight, double* scal,
                                     const int* flags, void* workspace, size_t workspace_bytes, void* stream) {
     using namespace pb::fcg;
@@ -344,7 +349,7 @@ extern "C" int pb_fcg_direction_f64(const float* z, const double* p0, const doub
 // FCG(1) pass 2: p_new, x_new = x + alpha p_new and the true residual
 // r = b - A x_new into r32, scal[4] = ||r||^2.  Iterate and direction buffers
 // alternate by parity of flags[1]: x[it & 1] -> x[(it+1) & 1].
-extern "C" int pb_fcg_update_f64(const float* z, double* p0, double* p1, double* x0, double* x1, const double* b,
+extern "C" int pb_fcg_update_f64(const float* z, float* p0, float* p1, double* x0, double* x1, const double* b,
                                  const double* screen, float* r32, int64_t n, double point_weight, double* scal,
                                  const int* flags, void* workspace, size_t workspace_bytes, void* stream) {
     using namespace pb::fcg;

@@ -434,24 +434,64 @@ __global__ void __launch_bounds__(32) coarse_inverse_kernel(const float* __restr
         for (int j = 0; j < kInvN; ++j) inv[lane * kInvN + j] = (float)a[lane][j];
 }
 
-// ---- levels with n <= kC27N in one block ----------------------------------------
-constexpr int kC27N = 17;
+// ---- levels of side <= 9 in one block, from shared memory -------------------------
+// The first level of side <= 9 and those below it (9, 5, 3) run in one block.
+// Their operators do not change during a solve, so set-up writes them once
+// into a compact image (pb_coarse27_image_f32): per level above the last, the
+// 27 couplings of every node (offsets (dz, dy, dx) in lexicographic order, zero
+// outside the grid), 1/diagonal and the prolongation weights, node-major; then
+// the 3^3 inverse.  Each cycle copies the image into shared memory and keeps e,
+// rhs and the residual of every level there in padded cubes ((n+2)^3 floats,
+// zero ghosts), so global memory sees only the first level's rhs and its
+// correction.
+constexpr int kC27N = 9;
 constexpr int kC27Threads = 1024;
-constexpr int kC27PerThread = (kC27N * kC27N * kC27N + kC27Threads - 1) / kC27Threads;
-constexpr int kC27MaxLevels = 8;
+constexpr int kC27MaxLevels = 3;  // 9, 5, 3
+static_assert(kC27N * kC27N * kC27N <= kC27Threads, "one node per thread on the largest level");
 
-struct Coarse27 {
+__host__ __device__ inline int round4(int v) { return (v + 3) & ~3; }
+__host__ __device__ inline int cube_size(int n) { return (n + 2) * (n + 2) * (n + 2); }
+
+// Float offsets of the image sections and of the shared work cubes (after the image).
+struct CoarseLayout {
     int count;
-    Geom g[kC27MaxLevels];
-    int64_t cs[kC27MaxLevels];
-    const float* c[kC27MaxLevels];
-    const float* invD[kC27MaxLevels];
-    const float* fac[kC27MaxLevels];
-    float* e[kC27MaxLevels];
-    float* rhs[kC27MaxLevels];
-    float* res[kC27MaxLevels];
-    const float* inverse;  // of the last level (side 3)
+    int n[kC27MaxLevels];
+    int coef[kC27MaxLevels], invD[kC27MaxLevels], fac[kC27MaxLevels], inverse;
+    int image;  // floats of the image (a multiple of 4)
+    int e[kC27MaxLevels], rhs[kC27MaxLevels], res[kC27MaxLevels];
+    int total;  // floats of shared memory
 };
+
+__host__ __device__ inline CoarseLayout coarse_layout(int count, const int* sizes) {
+    CoarseLayout c{};
+    c.count = count;
+    int off = 0;
+    for (int l = 0; l < count; ++l) {
+        const int n = sizes[l], N = n * n * n;
+        c.n[l] = n;
+        if (l == count - 1) break;  // the last level keeps its inverse only
+        c.coef[l] = off;
+        off += round4(27 * N);
+        c.invD[l] = off;
+        off += round4(N);
+        c.fac[l] = off;
+        off += round4(N);
+    }
+    c.inverse = off;
+    off += round4(kInvN * kInvN);
+    c.image = off;
+    for (int l = 0; l < count; ++l) {
+        const int m = round4(cube_size(sizes[l]));
+        c.e[l] = off;
+        c.rhs[l] = off + m;
+        c.res[l] = off + 2 * m;
+        off += 3 * m;
+    }
+    c.total = off;
+    return c;
+}
+
+__device__ __forceinline__ int cube_at(int x, int y, int z, int n) { return ((z + 1) * (n + 2) + (y + 1)) * (n + 2) + (x + 1); }
 
 __device__ __forceinline__ void unflatten(int i, int n, int& x, int& y, int& z) {
     x = i % n;
@@ -459,121 +499,147 @@ __device__ __forceinline__ void unflatten(int i, int n, int& x, int& y, int& z) 
     z = i / (n * n);
 }
 
-__device__ float stencil27(const float* __restrict__ c, int64_t cs, const Geom& g, int64_t p, const float* e,
-                           bool skip_centre) {
+// sum over the 27 (or 26) offsets of a_K e[J+K], in the couplings' order.
+__device__ __forceinline__ float stencil_cube(const float* a, const float* e, int c, int n, bool skip_centre) {
+    const int sy = n + 2, sz = (n + 2) * (n + 2);
     float s = 0.0f;
+    int k = 0;
 #pragma unroll
     for (int dz = -1; dz <= 1; ++dz)
 #pragma unroll
         for (int dy = -1; dy <= 1; ++dy)
 #pragma unroll
-            for (int dx = -1; dx <= 1; ++dx) {
+            for (int dx = -1; dx <= 1; ++dx, ++k) {
                 if (skip_centre && !(dx || dy || dz)) continue;
-                s += coupling(c, cs, g, p, dx, dy, dz) * e[p + offset_of(g, dx, dy, dz)];
+                s += a[k] * e[c + dx + dy * sy + dz * sz];
             }
     return s;
 }
 
-// Red-black ordered sweeps in place: each colour's new values are staged in
-// registers and written after a barrier, so same-colour neighbours are read
-// from the previous iterate, as the multi-block colour passes do.
-__device__ void c27_relax(const Coarse27& L, int l, int iters) {
-    const Geom g = L.g[l];
-    const int n = g.n, total = n * n * n;
-    float* e = L.e[l];
+// One node's couplings, 1/diagonal and weight into the image (set-up).
+__global__ void coarse_image_kernel(const float* __restrict__ c, int64_t cs, Geom g, const float* __restrict__ invD,
+                                    const float* __restrict__ fac, float* __restrict__ coef_out,
+                                    float* __restrict__ invD_out, float* __restrict__ fac_out) {
+    const int n = g.n, N = n * n * n;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int x, y, z;
+    unflatten(i, n, x, y, z);
+    const int64_t p = g.at(x, y, z);
+    int k = 0;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx, ++k)
+                coef_out[27 * i + k] = inside(x + dx, y + dy, z + dz, n) ? coupling(c, cs, g, p, dx, dy, dz) : 0.0f;
+    invD_out[i] = invD[p];
+    fac_out[i] = fac[p];
+}
+
+// Red-black ordered sweeps in place on a cube: each colour's new values are
+// computed from the current iterate and written after a barrier, so
+// same-colour neighbours are read from the previous iterate, as the
+// multi-block colour passes do.
+__device__ void cube_relax(const float* cf, const float* invD, const float* rhs, float* e, int n, int iters) {
+    const int N = n * n * n, i = threadIdx.x;
+    int x = 0, y = 0, z = 0;
+    if (i < N) unflatten(i, n, x, y, z);
+    const int c = cube_at(x, y, z, n);
     for (int it = 0; it < iters; ++it)
         for (int colour = 0; colour < 2; ++colour) {
-            float v[kC27PerThread];
-#pragma unroll
-            for (int k = 0; k < kC27PerThread; ++k) {
-                const int i = threadIdx.x + k * kC27Threads;
-                v[k] = 0.0f;
-                if (i < total) {
-                    int x, y, z;
-                    unflatten(i, n, x, y, z);
-                    if (((x + y + z) & 1) == colour) {
-                        const int64_t p = g.at(x, y, z);
-                        v[k] = (L.rhs[l][p] - stencil27(L.c[l], L.cs[l], g, p, e, true)) * L.invD[l][p];
-                    }
-                }
-            }
+            const bool mine = i < N && ((x + y + z) & 1) == colour;
+            float v = 0.0f;
+            if (mine) v = (rhs[c] - stencil_cube(cf + 27 * i, e, c, n, true)) * invD[i];
             __syncthreads();
-#pragma unroll
-            for (int k = 0; k < kC27PerThread; ++k) {
-                const int i = threadIdx.x + k * kC27Threads;
-                if (i < total) {
-                    int x, y, z;
-                    unflatten(i, n, x, y, z);
-                    if (((x + y + z) & 1) == colour) e[g.at(x, y, z)] = v[k];
-                }
-            }
+            if (mine) e[c] = v;
             __syncthreads();
         }
 }
 
-__global__ void __launch_bounds__(kC27Threads) coarse27_kernel(Coarse27 L, int pre, int post, int inner) {
-    for (int l = 0; l < L.count; ++l) {
-        const Geom g = L.g[l];
-        const int n = g.n, total = n * n * n;
-        if (l == L.count - 1) {  // side 3: e = A^-1 rhs
-            if (threadIdx.x < kInvN) {
+__global__ void __launch_bounds__(kC27Threads) coarse27_kernel(const float4* __restrict__ image, CoarseLayout lay,
+                                                               const float* __restrict__ rhs0,
+                                                               float* __restrict__ e0, Geom g0, int pre, int post,
+                                                               int inner) {
+    extern __shared__ float4 smem4[];
+    float* sm = reinterpret_cast<float*>(smem4);
+    const int tid = threadIdx.x;
+    for (int i = tid; i < lay.image / 4; i += kC27Threads) smem4[i] = image[i];
+    for (int i = lay.image + tid; i < lay.total; i += kC27Threads) sm[i] = 0.0f;
+    __syncthreads();
+    {
+        const int n = lay.n[0];
+        if (tid < n * n * n) {
+            int x, y, z;
+            unflatten(tid, n, x, y, z);
+            sm[lay.rhs[0] + cube_at(x, y, z, n)] = rhs0[g0.at(x, y, z)];
+        }
+    }
+    __syncthreads();
+    const int count = lay.count;
+    for (int l = 0; l < count; ++l) {
+        const int n = lay.n[l];
+        float* e = sm + lay.e[l];
+        const float* rhs = sm + lay.rhs[l];
+        if (l == count - 1) {  // side 3: e = A^-1 rhs
+            if (tid < kInvN) {
+                const float* inv = sm + lay.inverse;
                 float v = 0.0f;
-                for (int j = 0; j < kInvN; ++j)
-                    v += L.inverse[threadIdx.x * kInvN + j] * L.rhs[l][g.at(j % 3, (j / 3) % 3, j / 9)];
-                const int t = threadIdx.x;
-                L.e[l][g.at(t % 3, (t / 3) % 3, t / 9)] = v;
+                for (int j = 0; j < kInvN; ++j) v += inv[tid * kInvN + j] * rhs[cube_at(j % 3, (j / 3) % 3, j / 9, 3)];
+                e[cube_at(tid % 3, (tid / 3) % 3, tid / 9, 3)] = v;
             }
             __syncthreads();
             break;
         }
-        for (int i = threadIdx.x; i < total; i += blockDim.x) {
+        const float* cf = sm + lay.coef[l];
+        cube_relax(cf, sm + lay.invD[l], rhs, e, n, l == 0 ? pre : inner);  // e starts at zero
+        float* res = sm + lay.res[l];
+        if (tid < n * n * n) {
             int x, y, z;
-            unflatten(i, n, x, y, z);
-            L.e[l][g.at(x, y, z)] = 0.0f;
+            unflatten(tid, n, x, y, z);
+            const int c = cube_at(x, y, z, n);
+            res[c] = sm[lay.fac[l] + tid] * (rhs[c] - stencil_cube(cf + 27 * tid, e, c, n, false));
         }
         __syncthreads();
-        c27_relax(L, l, l == 0 ? pre : inner);
-        for (int i = threadIdx.x; i < total; i += blockDim.x) {
+        const int cn = lay.n[l + 1], sy = n + 2, sz = (n + 2) * (n + 2);
+        if (tid < cn * cn * cn) {
             int x, y, z;
-            unflatten(i, n, x, y, z);
-            const int64_t p = g.at(x, y, z);
-            L.res[l][p] = L.fac[l][p] * (L.rhs[l][p] - stencil27(L.c[l], L.cs[l], g, p, L.e[l], false));
-        }
-        __syncthreads();
-        const Geom gc = L.g[l + 1];
-        const int cn = gc.n;
-        for (int i = threadIdx.x; i < cn * cn * cn; i += blockDim.x) {
-            int x, y, z;
-            unflatten(i, cn, x, y, z);
-            const int64_t p = g.at(2 * x, 2 * y, 2 * z);
+            unflatten(tid, cn, x, y, z);
+            const int c = cube_at(2 * x, 2 * y, 2 * z, n);
             float s = 0.0f;
             for (int dz = -1; dz <= 1; ++dz)
                 for (int dy = -1; dy <= 1; ++dy)
                     for (int dx = -1; dx <= 1; ++dx)
-                        s += L.res[l][p + offset_of(g, dx, dy, dz)] *
-                             (float)((dx ? 1 : 2) * (dy ? 1 : 2) * (dz ? 1 : 2));
-            L.rhs[l + 1][gc.at(x, y, z)] = s * (1.0f / 64.0f);
+                        s += res[c + dx + dy * sy + dz * sz] * (float)((dx ? 1 : 2) * (dy ? 1 : 2) * (dz ? 1 : 2));
+            sm[lay.rhs[l + 1] + cube_at(x, y, z, cn)] = s * (1.0f / 64.0f);
         }
         __syncthreads();
     }
-    for (int l = L.count - 2; l >= 0; --l) {
-        const Geom g = L.g[l], gc = L.g[l + 1];
-        const int n = g.n, total = n * n * n;
-        const float* ec = L.e[l + 1];
-        for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    for (int l = count - 2; l >= 0; --l) {
+        const int n = lay.n[l], cn = lay.n[l + 1];
+        float* e = sm + lay.e[l];
+        const float* ec = sm + lay.e[l + 1];
+        if (tid < n * n * n) {
             int x, y, z;
-            unflatten(i, n, x, y, z);
+            unflatten(tid, n, x, y, z);
             // trilinear: the mean of the 8 corners, a corner repeated on even axes
             const int x0 = x >> 1, y0 = y >> 1, z0 = z >> 1;
             const int x1 = x0 + (x & 1), y1 = y0 + (y & 1), z1 = z0 + (z & 1);
-            const float v = 0.125f * (ec[gc.at(x0, y0, z0)] + ec[gc.at(x1, y0, z0)] + ec[gc.at(x0, y1, z0)] +
-                                      ec[gc.at(x1, y1, z0)] + ec[gc.at(x0, y0, z1)] + ec[gc.at(x1, y0, z1)] +
-                                      ec[gc.at(x0, y1, z1)] + ec[gc.at(x1, y1, z1)]);
-            const int64_t p = g.at(x, y, z);
-            L.e[l][p] += L.fac[l][p] * v;
+            const float v = 0.125f * (ec[cube_at(x0, y0, z0, cn)] + ec[cube_at(x1, y0, z0, cn)] +
+                                      ec[cube_at(x0, y1, z0, cn)] + ec[cube_at(x1, y1, z0, cn)] +
+                                      ec[cube_at(x0, y0, z1, cn)] + ec[cube_at(x1, y0, z1, cn)] +
+                                      ec[cube_at(x0, y1, z1, cn)] + ec[cube_at(x1, y1, z1, cn)]);
+            e[cube_at(x, y, z, n)] += sm[lay.fac[l] + tid] * v;
         }
         __syncthreads();
-        c27_relax(L, l, l == 0 ? post : inner);
+        cube_relax(sm + lay.coef[l], sm + lay.invD[l], sm + lay.rhs[l], e, n, l == 0 ? post : inner);
+    }
+    const int n = lay.n[0];
+    if (tid < n * n * n) {
+        int x, y, z;
+        unflatten(tid, n, x, y, z);
+        e0[g0.at(x, y, z)] = sm[lay.e[0] + cube_at(x, y, z, n)];
     }
 }
 
@@ -634,38 +700,70 @@ extern "C" int pb_coarse_inverse_f32(const float* coef, int64_t n, float* invers
     return PB_OK;
 }
 
-// Levels with side <= 17 in one block (27-point operators, V(pre, post) on the
-// first of them and `inner` sweeps each way on the others, the last level, of
-// side 3, solved with its inverse from pb_coarse_inverse_f32).  Arrays per
-// level, finest first; rhs[0] holds the restricted residual from above; e[0]
-// receives the correction.
-extern "C" int pb_coarse27_cycle_f32(int64_t count, const int64_t* sizes, const float* const* coef,
-                                     const float* const* invD, const float* const* weights, float* const* e,
-                                     float* const* rhs, float* const* res, int64_t pre, int64_t post,
-                                     int64_t inner, const float* inverse, void* stream) {
-    if (count < 1 || count > kC27MaxLevels || !sizes || !coef || !invD || !weights || !e || !rhs || !res || !inverse)
+static int coarse_sizes(int64_t count, const int64_t* sizes, int* out) {
+    if (count < 1 || count > kC27MaxLevels || !sizes) return fail(PB_ERR_INVALID, "coarse27: 1 to 3 levels");
+    for (int l = 0; l < count; ++l) {
+        if (!level_side_ok(sizes[l]) || sizes[l] > kC27N || (l && sizes[l] != (sizes[l - 1] + 1) / 2))
+            return fail(PB_ERR_INVALID, "coarse27: level sides must halve from <= 9 down to 3");
+        out[l] = (int)sizes[l];
+    }
+    if (sizes[count - 1] != 3) return fail(PB_ERR_INVALID, "coarse27: the last level must have side 3");
+    return PB_OK;
+}
+
+// Bytes of the image of levels `sizes` (finest first, side <= 9 halving to 3).
+extern "C" size_t pb_coarse27_image_size(int64_t count, const int64_t* sizes) {
+    int sz[kC27MaxLevels];
+    if (coarse_sizes(count, sizes, sz) != PB_OK) return 0;
+    return (size_t)coarse_layout((int)count, sz).image * sizeof(float);
+}
+
+// The image the single-block cycle reads: per level but the last, couplings
+// (from its 14 planes), 1/diagonal and prolongation weights; then the 3^3
+// inverse (from pb_coarse_inverse_f32).  image: 16-byte aligned.
+extern "C" int pb_coarse27_image_f32(int64_t count, const int64_t* sizes, const float* const* coef,
+                                     const float* const* invD, const float* const* weights, const float* inverse,
+                                     float* image, size_t image_bytes, void* stream) {
+    int sz[kC27MaxLevels];
+    PB_TRY(coarse_sizes(count, sizes, sz));
+    if (!coef || !invD || !weights || !inverse || !image || (reinterpret_cast<uintptr_t>(image) & 15))
+        return fail(PB_ERR_INVALID, "coarse27 image: bad args");
+    const CoarseLayout lay = coarse_layout((int)count, sz);
+    if (image_bytes < (size_t)lay.image * sizeof(float)) return fail(PB_ERR_WORKSPACE, "coarse27 image: too small");
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int l = 0; l + 1 < count; ++l) {
+        if (!coef[l] || !invD[l] || !weights[l]) return fail(PB_ERR_INVALID, "coarse27 image: null level array");
+        const int N = sz[l] * sz[l] * sz[l];
+        coarse_image_kernel<<<(N + 255) / 256, 256, 0, s>>>(coef[l], padded_size(sz[l]), geom(sz[l]), invD[l],
+                                                            weights[l], image + lay.coef[l], image + lay.invD[l],
+                                                            image + lay.fac[l]);
+        PB_CHECK_LAUNCH("coarse_image_kernel");
+    }
+    PB_CHECK_CUDA(cudaMemcpyAsync(image + lay.inverse, inverse, sizeof(float) * kInvN * kInvN,
+                                  cudaMemcpyDeviceToDevice, s),
+                  "coarse27 image inverse");
+    return PB_OK;
+}
+
+// Levels of side <= 9 in one block from their image: V(pre, post) on the
+// first, `inner` sweeps each way on the others, the last (side 3) solved with
+// its inverse.  rhs: the first level's right-hand side (padded layout); e
+// receives its correction (padded layout; ghosts untouched).
+extern "C" int pb_coarse27_cycle_f32(int64_t count, const int64_t* sizes, const float* image, const float* rhs,
+                                     float* e, int64_t pre, int64_t post, int64_t inner, void* stream) {
+    int sz[kC27MaxLevels];
+    PB_TRY(coarse_sizes(count, sizes, sz));
+    if (!image || !rhs || !e || (reinterpret_cast<uintptr_t>(image) & 15))
         return fail(PB_ERR_INVALID, "coarse27 cycle: bad args");
     if (pre < 0 || post < 0 || inner < 0 || pre > 64 || post > 64 || inner > 64)
         return fail(PB_ERR_INVALID, "coarse27 cycle: sweep counts must be in [0, 64]");
-    Coarse27 L;
-    L.count = (int)count;
-    L.inverse = inverse;
-    for (int l = 0; l < count; ++l) {
-        if (!level_side_ok(sizes[l]) || sizes[l] > kC27N || (l && sizes[l] != (sizes[l - 1] + 1) / 2))
-            return fail(PB_ERR_INVALID, "coarse27 cycle: bad level sizes");
-        if (!coef[l] || !invD[l] || !weights[l] || !e[l] || !rhs[l] || !res[l])
-            return fail(PB_ERR_INVALID, "coarse27 cycle: null level array");
-        L.g[l] = geom((int)sizes[l]);
-        L.cs[l] = padded_size((int)sizes[l]);
-        L.c[l] = coef[l];
-        L.invD[l] = invD[l];
-        L.fac[l] = weights[l];
-        L.e[l] = e[l];
-        L.rhs[l] = rhs[l];
-        L.res[l] = res[l];
-    }
-    if (sizes[count - 1] != 3) return fail(PB_ERR_INVALID, "coarse27 cycle: the last level must have side 3");
-    coarse27_kernel<<<1, kC27Threads, 0, (cudaStream_t)stream>>>(L, (int)pre, (int)post, (int)inner);
+    const CoarseLayout lay = coarse_layout((int)count, sz);
+    const size_t smem = (size_t)lay.total * sizeof(float);
+    PB_CHECK_CUDA(cudaFuncSetAttribute(coarse27_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                  "coarse27 smem");
+    coarse27_kernel<<<1, kC27Threads, smem, (cudaStream_t)stream>>>(reinterpret_cast<const float4*>(image), lay,
+                                                                     rhs, e, geom(sz[0]), (int)pre, (int)post,
+                                                                     (int)inner);
     PB_CHECK_LAUNCH("coarse27_kernel");
     return PB_OK;
 }

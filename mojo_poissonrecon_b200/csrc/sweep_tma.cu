@@ -285,24 +285,22 @@ static int make_map(CUtensorMap* map, const float* base, int n, int P, int rows)
 // fine += s * trilinear(coarse) (the P_s of mg27.cu; trilinear as in
 // capi.mojo:677-742), s the fine level's prolongation weights.
 // A thread owns four consecutive fine x (one float4 of e and of s; x offset 4
-// keeps them 16-byte aligned), a block a 128 x 8 (x, y) tile and kProTZ fine
-// planes.  The four fine nodes of a thread share three coarse values per
+// keeps them 16-byte aligned), a block a 128 x 8 (x, y) tile and `tz` fine
+// planes (up to kProTZ, fewer on small levels so that the grid still fills
+// the GPU: the planes of a block run one after another).  The four fine nodes of a thread share three coarse values per
 // coarse row: fine x = 4k + j lies on coarse 2k + j/2 (even j) or between
 // 2k + j/2 and the next (odd j).  Fine x >= n (ghost and padding) is never
 // written.
-#ifndef PB_PROLONG_TZ
-#define PB_PROLONG_TZ 16  // fine planes per block
-#endif
-constexpr int kProTX = 32, kProTY = 8, kProTZ = PB_PROLONG_TZ;
+constexpr int kProTX = 32, kProTY = 8, kProTZ = 16;
 
 __global__ void __launch_bounds__(kProTX* kProTY) prolong_add32_kernel(const float* __restrict__ c,
                                                                        float* __restrict__ f,
                                                                        const float* __restrict__ w, int n, int P,
-                                                                       int cn, int cP) {
+                                                                       int cn, int cP, int tz) {
     const int k = blockIdx.x * kProTX + threadIdx.x, y = blockIdx.y * kProTY + threadIdx.y;
     const int x = 4 * k;
     if (x >= n || y >= n) return;
-    const int z0 = blockIdx.z * kProTZ, z1 = min(n, z0 + kProTZ);
+    const int z0 = blockIdx.z * tz, z1 = min(n, z0 + tz);
     const int ya = y >> 1, yb = min(ya + 1, cn - 1);
     const float ty = (y & 1) ? 0.5f : 0.f;
     const int64_t cplane = (int64_t)(cn + 2) * cP;
@@ -348,10 +346,6 @@ using namespace pb;
 
 static int pitch_for(int n) { return ((n + 5) + 7) & ~7; }
 
-// One TMA-staged fused sweep.  n = 2^k + 1 >= 33 (smaller levels use the
-// single-block coarse kernel).  mode 0: from e_in; mode 1: from zero.
-// z_chunk <= 0 picks one that fills the 148 SMs with two blocks each.
-// *status (device int) is set to 1 if a bounded wait gave up.
 // One TMA-staged fused sweep.  n = 2^k + 1 >= 33 (smaller levels use the
 // single-block coarse kernel).  mode 0: from e_in; mode 1: from zero.
 // z_chunk <= 0 picks one that puts two blocks on each of the 148 SMs.
@@ -405,9 +399,13 @@ extern "C" int pb_prolong_fac_f32(const float* coarse, float* fine, const float*
     if (fine_n < 3 || fine_n > 4097 || !coarse || !fine || !weights) return fail(PB_ERR_INVALID, "prolong32: bad args");
     const int n = (int)fine_n, cn = (n + 1) / 2;
     const int groups = (n + 3) / 4;
-    const dim3 grid((groups + kProTX - 1) / kProTX, (n + kProTY - 1) / kProTY, (n + kProTZ - 1) / kProTZ);
+    const int gx = (groups + kProTX - 1) / kProTX, gy = (n + kProTY - 1) / kProTY;
+    // planes per block: as many as keep at least 4 blocks per SM, at most kProTZ
+    const int64_t fill = (int64_t)gx * gy * n / (4 * kSMs);
+    const int tz = fill < 1 ? 1 : (fill > kProTZ ? kProTZ : (int)fill);
+    const dim3 grid(gx, gy, (n + tz - 1) / tz);
     prolong_add32_kernel<<<grid, dim3(kProTX, kProTY), 0, (cudaStream_t)stream>>>(coarse, fine, weights, n,
-                                                                                   pitch_for(n), cn, pitch_for(cn));
+                                                                                   pitch_for(n), cn, pitch_for(cn), tz);
     PB_CHECK_LAUNCH("prolong_add32_kernel");
     return PB_OK;
 }

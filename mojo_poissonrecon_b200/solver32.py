@@ -20,12 +20,13 @@ Defect correction (``precision="fp32_defect"``): x += V(r), one FP32 V-cycle
 per FP64 residual, eager launches.
 
 The FP32 cycle: level 0 is the reference's operator with its red-black
-Gauss-Seidel smoother, 3 sweeps each way (core.py:141-193); the coarser
+Gauss-Seidel smoother (core.py:141-193; the reference runs 3 sweeps each way,
+the preconditioner level0_sweeps(n)); the coarser
 levels are Galerkin operators with screening-scaled transfers (mg27.cu),
 smoothed by COARSE_SWEEPS sweeps each way (on levels of side > 9 with their
 couplings packed per colour in FP16), which cut the cycles needed for a
 given residual 2-4x against the reference's rediscretised hierarchy.  Levels
-of side <= 9 run in a single launch, the 3^3 level solved exactly with its
+of side <= 9 run in a single launch from shared memory, the 3^3 level solved exactly with its
 inverse (built once per set-up).  Convergence is always measured with the
 reference's FP64 operator.
 """
@@ -44,7 +45,15 @@ from .solver import SolveStats, level_sizes, norm
 
 COARSE_N = 9  # levels of this side or smaller: one single-block launch
 TMA_MIN_N = 33  # smallest side the TMA sweep takes (level 0 below it is a 27-point level)
-COARSE_SWEEPS = 2  # pre- and post-smoothing sweeps on every level below level 0
+COARSE_SWEEPS = 1  # pre- and post-smoothing sweeps on every level below level 0
+
+
+def level0_sweeps(n: int) -> tuple[int, int]:
+    """(pre, post) smoothing sweeps on level 0 of the FCG preconditioner.
+    Measured on B200 over torus and sphere-union clouds at depths 6-9 (solve
+    time to rel-res 1e-8): with one coarse sweep, V(2,2) is fastest up to
+    257^3 and V(2,3) above, both ahead of V(3,3) with two coarse sweeps."""
+    return (2, 2) if n <= 257 else (2, 3)
 MAX_ITER = 512  # capacity of the device iteration history (and hard cap)
 
 # When true, RefinedEngine runs its iterations as eager launches with a host
@@ -120,19 +129,18 @@ class Hierarchy32:
             if not lv.seven:
                 lv.pack(device, self.lib)
         self.inverse = torch.zeros(27 * 27, dtype=torch.float32, device=device)  # of the 3^3 level
+        # levels of side <= COARSE_N: one block from their image (couplings, 1/diagonal, weights, inverse)
         tail = self.levels[self.first_coarse:]
         k = len(tail)
         ptrs = lambda ts: (ctypes.c_void_p * k)(*[t.data_ptr() for t in ts])
-        self._coarse_args = (
-            k,
-            (ctypes.c_int64 * k)(*[lv.n for lv in tail]),
-            ptrs([lv.coef for lv in tail]),
-            ptrs([lv.invD for lv in tail]),
-            ptrs([lv.weights for lv in tail]),
-            ptrs([lv.ea for lv in tail]),
-            ptrs([lv.rhs for lv in tail]),
-            ptrs([lv.res for lv in tail]),
-        )
+        self._tail = (k, (ctypes.c_int64 * k)(*[lv.n for lv in tail]))
+        image_bytes = self.lib.pb_coarse27_image_size(*self._tail)
+        if image_bytes == 0:
+            raise ValueError(f"no single-block image for levels {[lv.n for lv in tail]}")
+        self.image = torch.zeros(image_bytes // 4, dtype=torch.float32, device=device)
+        self._image_args = (*self._tail, ptrs([lv.coef for lv in tail]), ptrs([lv.invD for lv in tail]),
+                            ptrs([lv.weights for lv in tail]), self.inverse.data_ptr(), self.image.data_ptr(),
+                            image_bytes)
         self.pw = None
 
     @property
@@ -141,7 +149,7 @@ class Hierarchy32:
 
     def nbytes(self) -> int:
         return sum(t.numel() * t.element_size() for lv in self.levels for t in lv.tensors()) + \
-            self.inverse.numel() * 4
+            self.inverse.numel() * 4 + self.image.numel() * 4
 
     def setup(self, screen: torch.Tensor, point_weight: float) -> None:
         """Level 0 from the FP64 screen (D = (deg + pw*screen) h^-2, core.py:150-163),
@@ -166,6 +174,7 @@ class Hierarchy32:
                 nat.check(L.pb_pack27_f32(lv.coef.data_ptr(), lv.n, *lv.packed_ptrs(), s), "pack27")
         nat.check(L.pb_coarse_inverse_f32(self.levels[-1].coef.data_ptr(), 3, self.inverse.data_ptr(), s),
                   "coarse inverse")
+        nat.check(L.pb_coarse27_image_f32(*self._image_args, s), "coarse image")
 
     def _sweep(self, lv: Level32, src, dst, mode: int, coarse=None) -> None:
         """One red-black sweep dst <- S(src); mode 1 starts from zero, mode 2
@@ -201,9 +210,10 @@ class Hierarchy32:
         if level > 0:
             pre = post = self.coarse_sweeps
         if level >= self.first_coarse:
-            nat.check(L.pb_coarse27_cycle_f32(*self._coarse_args, pre, post, self.coarse_sweeps,
-                                              self.inverse.data_ptr(), s), "coarse cycle")
-            return self.levels[level].ea
+            lv = self.levels[self.first_coarse]
+            nat.check(L.pb_coarse27_cycle_f32(*self._tail, self.image.data_ptr(), lv.rhs.data_ptr(), lv.ea.data_ptr(),
+                                              pre, post, self.coarse_sweeps, s), "coarse cycle")
+            return lv.ea
         lv = self.levels[level]
         a, b = lv.ea, lv.eb
         self._sweep(lv, None, a, 1)  # pre-smoothing from zero
@@ -251,7 +261,8 @@ class RefinedEngine:
         f64 = lambda: torch.empty((n, n, n), dtype=torch.float64, device=device)
         self.screen, self.b = f64(), f64()
         self.xs = (f64(), f64())  # iterate, alternating by iteration parity
-        self.ps = (f64(), f64())  # search direction, alternating by iteration parity
+        f32 = lambda: torch.empty((n, n, n), dtype=torch.float32, device=device)
+        self.ps = (f32(), f32())  # search direction (stored in FP32), alternating by iteration parity
         self.scal = torch.zeros(8, dtype=torch.float64, device=device)
         self.ctrl = torch.zeros(2, dtype=torch.float64, device=device)
         self.flags = torch.zeros(4, dtype=torch.int32, device=device)
@@ -280,7 +291,7 @@ class RefinedEngine:
 
     def _iteration(self, handle: int) -> None:
         L, s = self.lib, nat.stream_handle()
-        z = self.h.v_cycle(0)
+        z = self.h.v_cycle(0, *level0_sweeps(self.n))
         r32 = self.h.levels[0].rhs
         p0, p1 = (t.data_ptr() for t in self.ps)
         x0, x1 = (t.data_ptr() for t in self.xs)
