@@ -283,9 +283,13 @@ int pb_residual_restrict_f32(const float *e, const float *rhs, const float *D, c
                              float *coarse_rhs, int64_t n, void *stream);
 /* 14 planes of the Galerkin operator of the level below a level of side
  * fine_n with prolongation weights fine_weights: from level 0 (fine_is_7pt
- * != 0, `fine` = D) or from 14 planes. */
+ * != 0, `fine` = D; no workspace) or from 14 planes, one axis at a time over
+ * slabs of coarse planes that fit the workspace.  pb_galerkin_workspace_size
+ * gives the bytes for a single slab; smaller workspaces work down to the size
+ * of one coarse plane's slab (the call reports it when too small). */
+size_t pb_galerkin_workspace_size(int64_t fine_n, int fine_is_7pt);
 int pb_galerkin_f32(const float *fine, int64_t fine_n, int fine_is_7pt, const float *fine_weights,
-                    float *coarse, void *stream);
+                    float *coarse, void *workspace, size_t workspace_bytes, void *stream);
 /* 14 planes of a 7-point level (diagonal D, off-diagonals -(n-1)^2). */
 int pb_level27_from7_f32(const float *D, int64_t n, float *coef, void *stream);
 /* invD = 1 / diagonal and the prolongation weights of a 27-point level. */

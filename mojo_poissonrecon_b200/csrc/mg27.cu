@@ -158,48 +158,123 @@ __global__ void __launch_bounds__(128) galerkin7_kernel(const float* __restrict_
     galerkin_store<true>(acc, cc, cs, gc, xc, yc, zc);
 }
 
-// A 27-point fine level (small: side <= 129).  4 blocks per SM caps it at 128
-// registers, where the gather runs 1.5x faster than at its natural 135.
-#ifndef PB_GALERKIN_MIN_BLOCKS
-#define PB_GALERKIN_MIN_BLOCKS 4
-#endif
-__global__ void __launch_bounds__(128, PB_GALERKIN_MIN_BLOCKS) galerkin27_kernel(const float* __restrict__ fc,
-                                                                                 int64_t fs,
-                                                                                 const float* __restrict__ S,
-                                                                                 Geom gf, float* __restrict__ cc,
-                                                                                 int64_t cs, Geom gc) {
-    const int xc = blockIdx.x * blockDim.x + threadIdx.x, yc = blockIdx.y * blockDim.y + threadIdx.y;
-    const int zc = blockIdx.z;
-    const int cn = gc.n;
-    if (xc >= cn || yc >= cn) return;
-    float acc[14];
-#pragma unroll
-    for (int k = 0; k < 14; ++k) acc[k] = 0.0f;
-    const bool interior = xc >= 1 && yc >= 1 && zc >= 1 && xc <= cn - 2 && yc <= cn - 2 && zc <= cn - 2;
-    // one code path with a runtime test per term: two specialised paths spill here
+// ---- separable product for a 27-point fine level ---------------------------------
+// P is the tensor product of 1D linear interpolation (coarse M -> fine j with
+// weight 1 at j = 2M and 1/2 at j = 2M +- 1), so P^T (S A S) P / 8 contracts
+// one axis at a time: x, then y, then z.  Each stage maps fine positions 2M +
+// a (a in {-1, 0, 1}) and their offsets d to coarse offsets m with weights
+// P(a) P(a + d - 2m), keeping the other two axes' offsets, and takes 81
+// products per output node against the direct sum's 27 x 27 per coarse node
+// scattered over 14 entries.  Stages x and y write full 27-entry stencils,
+// entry e = (oz+1)*9 + (oy+1)*3 + (ox+1), as 27 planes of a dense grid into
+// scratch, a slab of fine z-planes at a time; stage z writes the 14 stored
+// planes.  Out-of-grid fine nodes and neighbours contribute nothing.
+__host__ __device__ constexpr float wt1(int d) { return d == 0 ? 1.0f : (d == 1 || d == -1 ? 0.5f : 0.0f); }
+
+// Stage x: node (I, y, z) of the grid cn x fn x (slab of fine z from zlo);
+// entry (m, dy, dz) = sum over a, dx of P(a) s_i a(i, j) s_j P(a + dx - 2m),
+// i = (2I + a, y, z), j = i + (dx, dy, dz).
+__global__ void __launch_bounds__(128) galerkin_x_kernel(const float* __restrict__ c, int64_t cs,
+                                                         const float* __restrict__ S, Geom gf, int cn, int zlo,
+                                                         float* __restrict__ out, int64_t ps) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     const int fn = gf.n;
+    if (I >= cn || y >= fn) return;
+    const int z = zlo + blockIdx.z;
+    const int64_t o = ((int64_t)blockIdx.z * fn + y) * cn + I;
 #pragma unroll
-    for (int oz = -1; oz <= 1; ++oz)
+    for (int dz = -1; dz <= 1; ++dz)
 #pragma unroll
-        for (int oy = -1; oy <= 1; ++oy)
+        for (int dy = -1; dy <= 1; ++dy) {
+            float acc[3] = {0.0f, 0.0f, 0.0f};
+            if (inside(0, y + dy, z + dz, fn)) {
 #pragma unroll
-            for (int ox = -1; ox <= 1; ++ox) {
-                const int xi = 2 * xc + ox, yi = 2 * yc + oy, zi = 2 * zc + oz;
-                if (!interior && !inside(xi, yi, zi, fn)) continue;
-                const int64_t pi = gf.at(xi, yi, zi);
-                const float si = wt(ox) * wt(oy) * wt(oz) * S[pi];
+                for (int a = -1; a <= 1; ++a) {
+                    const int xi = 2 * I + a;
+                    if (xi < 0 || xi >= fn) continue;
+                    const int64_t pi = gf.at(xi, y, z);
+                    const float si = wt1(a) * S[pi];
 #pragma unroll
-                for (int kz = -1; kz <= 1; ++kz)
+                    for (int dx = -1; dx <= 1; ++dx) {
+                        if (xi + dx < 0 || xi + dx >= fn) continue;
+                        const float t = si * coupling(c, cs, gf, pi, dx, dy, dz) * S[pi + offset_of(gf, dx, dy, dz)];
 #pragma unroll
-                    for (int ky = -1; ky <= 1; ++ky)
-#pragma unroll
-                        for (int kx = -1; kx <= 1; ++kx) {
-                            if (!interior && !inside(xi + kx, yi + ky, zi + kz, fn)) continue;
-                            scatter14(si * coupling(fc, fs, gf, pi, kx, ky, kz) * S[pi + offset_of(gf, kx, ky, kz)],
-                                      ox + kx, oy + ky, oz + kz, acc);
-                        }
+                        for (int m = -1; m <= 1; ++m)
+                            if (wt1(a + dx - 2 * m) != 0.0f) acc[m + 1] += t * wt1(a + dx - 2 * m);
+                    }
+                }
             }
-    galerkin_store<false>(acc, cc, cs, gc, xc, yc, zc);
+#pragma unroll
+            for (int m = -1; m <= 1; ++m) out[((dz + 1) * 9 + (dy + 1) * 3 + (m + 1)) * ps + o] = acc[m + 1];
+        }
+}
+
+// Stage y: node (I, J, z) of cn x cn x slab from stage x's cn x fn x slab.
+__global__ void __launch_bounds__(128) galerkin_y_kernel(const float* __restrict__ in, int64_t pin, int fn, int cn,
+                                                         float* __restrict__ out, int64_t pout) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
+    if (I >= cn || J >= cn) return;
+    const int zr = blockIdx.z;
+    const int64_t o = ((int64_t)zr * cn + J) * cn + I;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int m = -1; m <= 1; ++m) {
+            float acc[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+            for (int b = -1; b <= 1; ++b) {
+                const int yj = 2 * J + b;
+                if (yj < 0 || yj >= fn) continue;
+                const int64_t q = ((int64_t)zr * fn + yj) * cn + I;
+#pragma unroll
+                for (int dy = -1; dy <= 1; ++dy) {
+                    const float v = wt1(b) * in[((dz + 1) * 9 + (dy + 1) * 3 + (m + 1)) * pin + q];
+#pragma unroll
+                    for (int my = -1; my <= 1; ++my)
+                        if (wt1(b + dy - 2 * my) != 0.0f) acc[my + 1] += v * wt1(b + dy - 2 * my);
+                }
+            }
+#pragma unroll
+            for (int my = -1; my <= 1; ++my) out[((dz + 1) * 9 + (my + 1) * 3 + (m + 1)) * pout + o] = acc[my + 1];
+        }
+}
+
+// Stage z: coarse node (I, J, K), K in [k0, k1), from stage y's slab (fine z
+// from zlo, nz planes); the diagonal and the 13 forward couplings / 8 into the
+// 14 planes, zero where the coarse neighbour lies outside the grid.
+__global__ void __launch_bounds__(128) galerkin_z_kernel(const float* __restrict__ in, int64_t pin, int fn, int zlo,
+                                                         int k0, float* __restrict__ cc, int64_t cs, Geom gc) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
+    const int cn = gc.n;
+    if (I >= cn || J >= cn) return;
+    const int K = k0 + blockIdx.z;
+    const int64_t p = gc.at(I, J, K);
+#pragma unroll
+    for (int my = -1; my <= 1; ++my)
+#pragma unroll
+        for (int m = -1; m <= 1; ++m) {
+            float acc[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+            for (int c = -1; c <= 1; ++c) {
+                const int zf = 2 * K + c;
+                if (zf < 0 || zf >= fn) continue;
+                const int64_t q = ((int64_t)(zf - zlo) * cn + J) * cn + I;
+#pragma unroll
+                for (int dz = -1; dz <= 1; ++dz) {
+                    const float v = wt1(c) * in[((dz + 1) * 9 + (my + 1) * 3 + (m + 1)) * pin + q];
+#pragma unroll
+                    for (int mz = -1; mz <= 1; ++mz)
+                        if (wt1(c + dz - 2 * mz) != 0.0f) acc[mz + 1] += v * wt1(c + dz - 2 * mz);
+                }
+            }
+#pragma unroll
+            for (int mz = -1; mz <= 1; ++mz) {
+                const bool centre = m == 0 && my == 0 && mz == 0;
+                if (!centre && !is_forward(m, my, mz)) continue;
+                const float val = inside(I + m, J + my, K + mz, cn) ? acc[mz + 1] * 0.125f : 0.0f;
+                cc[(centre ? 0 : fwd_index(m, my, mz)) * cs + p] = val;
+            }
+        }
 }
 
 // A 7-point level (diagonal D, off-diagonals -h2 inside the grid) as 14 planes.
@@ -651,24 +726,64 @@ using namespace pb;
 
 static bool level_side_ok(int64_t n) { return n >= 3 && n <= 4097 && ((n - 1) & (n - 2)) == 0; }
 
+// Scratch floats of the separable product for a slab of kp coarse planes:
+// stage x (cn x fn x nz) and stage y (cn x cn x nz), 27 planes each, nz =
+// 2 kp + 1 fine planes.
+static int64_t galerkin_slab_floats(int fn, int kp) {
+    const int cn = (fn + 1) / 2;
+    const int64_t nz = 2 * (int64_t)kp + 1;
+    return 27 * ((int64_t)cn * fn + (int64_t)cn * cn) * nz;
+}
+
+// Scratch bytes for the whole level in one slab (any size down to one coarse
+// plane, galerkin_slab_floats(fn, 1) * 4 bytes, works in more slabs); 0 for
+// a 7-point fine level.
+extern "C" size_t pb_galerkin_workspace_size(int64_t fine_n, int fine_is_7pt) {
+    if (!level_side_ok(fine_n) || fine_is_7pt) return 0;
+    return (size_t)galerkin_slab_floats((int)fine_n, (int)((fine_n + 1) / 2)) * sizeof(float) + 256;
+}
+
 // Coarse 27-point operator (14 planes, plane stride padded_size(cn)) of the
 // level below a fine level of side fine_n with prolongation weights
 // fine_weights.  fine_is_7pt: `fine` is the level-0 diagonal D (couplings
-// -(n-1)^2); otherwise `fine` holds 14 planes.
+// -(n-1)^2, direct sum, no scratch); otherwise `fine` holds 14 planes and the
+// separable stages run over slabs of coarse planes that fit the workspace.
 extern "C" int pb_galerkin_f32(const float* fine, int64_t fine_n, int fine_is_7pt, const float* fine_weights,
-                               float* coarse, void* stream) {
+                               float* coarse, void* workspace, size_t workspace_bytes, void* stream) {
     if (!level_side_ok(fine_n) || !fine || !coarse || !fine_weights) return fail(PB_ERR_INVALID, "galerkin: bad args");
     const int fn = (int)fine_n, cn = (fn + 1) / 2;
     const Geom gf = geom(fn), gc = geom(cn);
-    const float h2 = (float)(fn - 1) * (float)(fn - 1);
+    cudaStream_t s = (cudaStream_t)stream;
     const dim3 block(32, 4);
-    if (fine_is_7pt)
-        galerkin7_kernel<<<node_grid(cn, block), block, 0, (cudaStream_t)stream>>>(fine, fine_weights, gf, h2, coarse,
-                                                                                  padded_size(cn), gc);
-    else
-        galerkin27_kernel<<<node_grid(cn, block), block, 0, (cudaStream_t)stream>>>(
-            fine, padded_size(fn), fine_weights, gf, coarse, padded_size(cn), gc);
-    PB_CHECK_LAUNCH("galerkin_kernel");
+    if (fine_is_7pt) {
+        const float h2 = (float)(fn - 1) * (float)(fn - 1);
+        galerkin7_kernel<<<node_grid(cn, block), block, 0, s>>>(fine, fine_weights, gf, h2, coarse, padded_size(cn),
+                                                                gc);
+        PB_CHECK_LAUNCH("galerkin7_kernel");
+        return PB_OK;
+    }
+    const int64_t have = workspace ? (int64_t)(workspace_bytes / sizeof(float)) : 0;
+    if (have < galerkin_slab_floats(fn, 1))
+        return fail(PB_ERR_WORKSPACE, "galerkin: workspace needs at least %lld bytes",
+                    (long long)(galerkin_slab_floats(fn, 1) * (int64_t)sizeof(float)));
+    int kp = cn;
+    while (kp > 1 && galerkin_slab_floats(fn, kp) > have) kp = (kp + 1) / 2;
+    float* bx = static_cast<float*>(workspace);
+    for (int k0 = 0; k0 < cn; k0 += kp) {
+        const int k1 = min(cn, k0 + kp);
+        const int zlo = max(0, 2 * k0 - 1), zhi = min(fn, 2 * k1);
+        const int nz = zhi - zlo;
+        const int64_t px = (int64_t)cn * fn * nz, py = (int64_t)cn * cn * nz;
+        float* by = bx + 27 * px;
+        galerkin_x_kernel<<<dim3((cn + 31) / 32, (fn + 3) / 4, nz), block, 0, s>>>(fine, padded_size(fn),
+                                                                                fine_weights, gf, cn, zlo, bx, px);
+        PB_CHECK_LAUNCH("galerkin_x_kernel");
+        galerkin_y_kernel<<<dim3((cn + 31) / 32, (cn + 3) / 4, nz), block, 0, s>>>(bx, px, fn, cn, by, py);
+        PB_CHECK_LAUNCH("galerkin_y_kernel");
+        galerkin_z_kernel<<<dim3((cn + 31) / 32, (cn + 3) / 4, k1 - k0), block, 0, s>>>(by, py, fn, zlo, k0, coarse,
+                                                                                     padded_size(cn), gc);
+        PB_CHECK_LAUNCH("galerkin_z_kernel");
+    }
     return PB_OK;
 }
 

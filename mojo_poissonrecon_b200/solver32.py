@@ -55,6 +55,7 @@ def level0_sweeps(n: int) -> tuple[int, int]:
     257^3 and V(2,3) above, both ahead of V(3,3) with two coarse sweeps."""
     return (2, 2) if n <= 257 else (2, 3)
 MAX_ITER = 512  # capacity of the device iteration history (and hard cap)
+GALERKIN_SCRATCH = 512 << 20  # bytes; larger Galerkin products run in slabs of coarse planes
 
 # When true, RefinedEngine runs its iterations as eager launches with a host
 # read of the residual after each (the same kernels as the captured loop), for
@@ -129,6 +130,12 @@ class Hierarchy32:
             if not lv.seven:
                 lv.pack(device, self.lib)
         self.inverse = torch.zeros(27 * 27, dtype=torch.float32, device=device)  # of the 3^3 level
+        # scratch of the separable Galerkin products (27-point fine levels), at most GALERKIN_SCRATCH bytes
+        fine27 = [lv.n for lv in self.levels[:-1] if not lv.seven]
+        need = max([self.lib.pb_galerkin_workspace_size(m, 0) for m in fine27], default=0)
+        one_plane = max([27 * 4 * 3 * ((m + 1) // 2) * (m + (m + 1) // 2) for m in fine27], default=0)
+        size = min(need, max(GALERKIN_SCRATCH, one_plane))
+        self.galerkin_ws = torch.empty((size + 3) // 4, dtype=torch.float32, device=device)
         # levels of side <= COARSE_N: one block from their image (couplings, 1/diagonal, weights, inverse)
         tail = self.levels[self.first_coarse:]
         k = len(tail)
@@ -149,7 +156,7 @@ class Hierarchy32:
 
     def nbytes(self) -> int:
         return sum(t.numel() * t.element_size() for lv in self.levels for t in lv.tensors()) + \
-            self.inverse.numel() * 4 + self.image.numel() * 4
+            self.inverse.numel() * 4 + self.image.numel() * 4 + self.galerkin_ws.numel() * 4
 
     def setup(self, screen: torch.Tensor, point_weight: float) -> None:
         """Level 0 from the FP64 screen (D = (deg + pw*screen) h^-2, core.py:150-163),
@@ -166,7 +173,7 @@ class Hierarchy32:
         for fine, lv in zip(self.levels[:-1], self.levels[1:]):
             src, seven = (fine.D, 1) if fine.seven else (fine.coef, 0)
             nat.check(L.pb_galerkin_f32(src.data_ptr(), fine.n, seven, fine.weights.data_ptr(), lv.coef.data_ptr(),
-                                        s), "galerkin")
+                                        self.galerkin_ws.data_ptr(), self.galerkin_ws.numel() * 4, s), "galerkin")
             nat.check(L.pb_level27_finish_f32(lv.coef.data_ptr(), lv.n, lv.invD.data_ptr(), lv.weights.data_ptr(), s),
                       "level27 finish")
         for lv in self.levels:

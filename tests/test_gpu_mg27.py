@@ -2,8 +2,8 @@
 transfers) against the CPU restatement in tests/mg_reference.py.
 
 Tolerances (max norm, relative to the largest magnitude of the compared
-quantity): Galerkin planes 3e-5 (FP32 products and sums of up to ~1300 terms,
-compounded over levels); weights and 1/diagonal 1e-5; packed FP16 couplings
+quantity): Galerkin planes 3e-5 (FP32 products and sums over three
+separable stages of 81 terms each, compounded over levels); weights and 1/diagonal 1e-5; packed FP16 couplings
 exactly (the same FP32 operations, then rounding to FP16); a single sweep,
 residual, restriction or prolongation 2e-6 to 4e-6 of the largest term,
 evaluated on the GPU's own coefficients (FP32 planes, or the packed FP16
@@ -76,6 +76,31 @@ def gpu_ops(L, h):
             ops.append(mg.from_planes(gpu_planes(L, lv), lv.n))
         ws.append(from_padded(L, lv.weights, lv.n).ravel())
     return ops, ws, [lv.n for lv in h.levels]
+
+
+@pytest.mark.parametrize("n", [33, 65])
+def test_galerkin_slabs_match_single_pass(L, n):
+    """The separable product over slabs of one or three coarse planes (small
+    workspaces) equals the single-slab product bit for bit: every node's
+    arithmetic is the same whatever the slab; too small a workspace is an error."""
+    from mojo_poissonrecon_b200 import _native
+
+    h = gpu_hierarchy(n, shell_screen(n, 7))
+    fine, coarse = h.levels[1], h.levels[2]
+    fn, cn = fine.n, coarse.n
+    full = coarse.coef.clone()
+    one_plane = 27 * 4 * 3 * cn * (fn + cn)
+    for nbytes in (one_plane, 27 * 4 * 7 * cn * (fn + cn) + 100):
+        ws = torch.empty(nbytes // 4 + 1, dtype=torch.float32, device="cuda")
+        out = torch.zeros_like(full)
+        _native.check(L.pb_galerkin_f32(fine.coef.data_ptr(), fn, 0, fine.weights.data_ptr(), out.data_ptr(),
+                                        ws.data_ptr(), nbytes, stream()), "galerkin slabs")
+        torch.cuda.synchronize()
+        assert torch.equal(out, full)
+    ws = torch.empty(one_plane // 4, dtype=torch.float32, device="cuda")
+    assert L.pb_galerkin_f32(fine.coef.data_ptr(), fn, 0, fine.weights.data_ptr(), full.data_ptr(), ws.data_ptr(),
+                             one_plane - 4, stream()) != 0
+    assert L.pb_galerkin_workspace_size(fn, 1) == 0 and L.pb_galerkin_workspace_size(fn, 0) >= one_plane
 
 
 @pytest.mark.parametrize("n", [9, 17, 33, 65])
