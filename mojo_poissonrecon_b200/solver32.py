@@ -50,10 +50,12 @@ COARSE_SWEEPS = 1  # pre- and post-smoothing sweeps on every level below level 0
 
 def level0_sweeps(n: int) -> tuple[int, int]:
     """(pre, post) smoothing sweeps on level 0 of the FCG preconditioner.
-    Measured on B200 over torus and sphere-union clouds at depths 6-9 (solve
-    time to rel-res 1e-8): with one coarse sweep, V(2,2) is fastest up to
-    257^3 and V(2,3) above, both ahead of V(3,3) with two coarse sweeps."""
-    return (2, 2) if n <= 257 else (2, 3)
+    Measured on B200 (solve time to rel-res 1e-8, torus and sphere-union clouds,
+    depths 7-9, one or two coarse sweeps, V(1,1) to V(5,5)): V(1,2) with one
+    coarse sweep is fastest at every depth tried (depth 8: 6 iterations in
+    6.7 ms against 7.1 ms for V(2,2) and 8.1 ms for V(3,3) with two coarse
+    sweeps); a cheaper cycle moves the iteration count by one at most."""
+    return (1, 2)
 MAX_ITER = 512  # capacity of the device iteration history (and hard cap)
 GALERKIN_SCRATCH = 512 << 20  # bytes; larger Galerkin products run in slabs of coarse planes
 
