@@ -44,6 +44,7 @@ POINTS = 1_000_000
 DEPTH = 8
 TOL = 1e-8
 SWEEP_PROFILE = os.path.join(ROOT, "profiles", "sweep_tma_f32_257.md")
+UPDATE_PROFILE = os.path.join(ROOT, "profiles", "fcg_update_residual_257.md")
 
 
 def parse_args():
@@ -93,7 +94,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
-                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+                 "-lms", "100", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
         return self
@@ -270,27 +271,29 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
 
     n = (1 << args.depth) + 1
     roofline = None
-    if sweep_ms:
-        from json import loads
-
-        peaks = {}
-        try:
-            with open(os.path.join(ROOT, "MEASURED_PEAKS.json"), encoding="utf8") as f:
-                peaks = loads(f.read())
-        except OSError:
-            pass
-        peak = float(peaks.get("hbm_gbs", 6650.0))
-        peak_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
-        avg_ms = statistics.mean(sweep_ms)
-        algorithmic = 16.0 * n**3  # read e, rhs, 1/D and write e, FP32, per launch
-        achieved = algorithmic / (avg_ms / 1e3) / 1e9
-        roofline = {"kernel": "pb::tma::sweep_kernel<0, 5> (fused red-black sweep, level 0, 257^3)",
+    if kernel_table:
+        if sweep_ms:  # the level-0 sweep from the probe above, beside the other kernels
+            avg_ms = statistics.mean(sweep_ms)
+            algorithmic = 16.0 * n**3  # read e, rhs, 1/D and write e, FP32, per launch
+            gbs = algorithmic / (avg_ms / 1e3) / 1e9
+            kernel_table.insert(0, {
+                "kernel": "tma::sweep_kernel<0, 5> (fused red-black sweep, level 0)", "us": round(avg_ms * 1e3, 1),
+                "algorithmic_bytes": int(algorithmic), "achieved_gbs": round(gbs, 1),
+                "frac_of_measured_hbm": round(gbs / hbm_peak()[0], 3),
+                "traffic": read_profile_traffic(SWEEP_PROFILE),
+                "timing": "CUDA events around each finest-level sweep of 5 eager V-cycles"})
+        # the dominant kernel of the launch list (profiles/launches_refined_d8.md)
+        top = next(k for k in kernel_table if k["kernel"].startswith("fcg::update_residual_kernel"))
+        peak, peak_src = hbm_peak()
+        achieved = top["algorithmic_bytes"] / (top["us"] * 1e-6) / 1e9
+        roofline = {"kernel": "pb::fcg::update_residual_kernel (FCG pass 2, FP64 residual, 257^3)",
                     "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                     "frac": round(achieved / peak, 4), "peak_source": peak_src,
-                    "avg_launch_ms": round(avg_ms, 4), "launches_timed": len(sweep_ms),
-                    "timing": "CUDA events on the launching stream around each finest-level sweep of 5 eager "
-                              "V-cycles on the timed solves' engine, right after the timed region",
-                    "algorithmic_bytes_per_launch": int(algorithmic), "traffic": read_profile_traffic()}
+                    "avg_launch_ms": round(top["us"] / 1e3, 4), "launches_timed": 20,
+                    "timing": "CUDA events on the engine's stream around 20 launches on the timed solves' "
+                              "engine and buffers, right after the timed region (inputs 0.8 GB > L2)",
+                    "algorithmic_bytes_per_launch": top["algorithmic_bytes"],
+                    "traffic": read_profile_traffic(UPDATE_PROFILE)}
 
     if rank != 0:
         return None
@@ -328,19 +331,15 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
 
 
 def kernel_rooflines(eng, n: int, L) -> list:
-    """The other hot kernels of an FP32-refined solve, each timed with CUDA
-    events on the engine's stream (20 launches after one warm-up, on the timed
-    solves' engine and buffers), against its algorithmic bytes per launch
-    (each array read or written once) and the measured HBM copy peak."""
+    """The hot kernels of an FP32-refined solve, each timed with CUDA events on
+    the engine's stream (20 launches after one warm-up, on the timed solves'
+    engine and buffers), against its algorithmic bytes per launch (each array
+    read or written once) and the measured HBM copy peak."""
     import torch
 
     from mojo_poissonrecon_b200 import _native as nat
 
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json"), encoding="utf8") as f:
-            peak = float(json.loads(f.read()).get("hbm_gbs", 6650.0))
-    except OSError:
-        peak = 6650.0
+    peak = hbm_peak()[0]
     h = eng.h
     l0, l1 = h.levels[0], h.levels[1]
     N, N1 = n ** 3, l1.n ** 3
@@ -379,10 +378,22 @@ def kernel_rooflines(eng, n: int, L) -> list:
     return out
 
 
-def read_profile_traffic():
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+def hbm_peak() -> tuple:
+    """The measured HBM copy bandwidth (GB/s) and where it came from."""
     try:
-        with open(SWEEP_PROFILE, encoding="utf8") as f:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json"), encoding="utf8") as f:
+            peaks = json.loads(f.read())
+    except OSError:
+        peaks = {}
+    if "hbm_gbs" in peaks:
+        return float(peaks["hbm_gbs"]), "of measured"
+    return 6650.0, "of fallback"
+
+
+def read_profile_traffic(path):
+    """DRAM bytes per launch of a kernel from its committed ncu summary."""
+    try:
+        with open(path, encoding="utf8") as f:
             for line in f:
                 m = re.match(r"\s*traffic_bytes_per_launch_257:\s*([\d.eE+]+)", line)
                 if m:
