@@ -179,15 +179,16 @@ struct Halo {
 // x = x[it & 1] -> x_new = x[(it+1) & 1].
 //
 // A 32 x 8 tile marches down z: the new iterate of plane k over the tile and
-// its one-node halo goes to shared memory once, the column's planes k - 1 and
-// k + 1 stay in registers (about 7 global loads per node instead of 23 with
-// every neighbour formed from memory).  Nodes outside the domain hold 0 and
+// its one-node halo goes to shared memory once (two tiles by plane parity, so
+// one barrier per plane), the column's planes k - 1 and k + 1 stay in
+// registers (about 7 global loads per node instead of 23 with every neighbour
+// formed from memory).  Nodes outside the domain hold 0 and
 // the neighbour sum adds x-, x+, y-, y+, z-, z+ in that order.
 __global__ void __launch_bounds__(kUThreads) update_residual_kernel(
     const float* __restrict__ z, Pad g, float* p0, float* p1, double* x0, double* x1, const double* __restrict__ b,
     const double* __restrict__ screen, double pw, const double* __restrict__ scal, const int* __restrict__ flags,
     float* __restrict__ r32, double* __restrict__ part) {
-    __shared__ double tile[kUY + 2][kUX + 2];
+    __shared__ double tiles[2][kUY + 2][kUX + 2];  // by plane parity: one barrier per plane
     __shared__ double shared[1][32];
     const int n = g.n;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kUX + tx;
@@ -239,7 +240,8 @@ __global__ void __launch_bounds__(kUThreads) update_residual_kernel(
             bi = b[i];
             sc = screen[i];
         }
-        __syncthreads();  // the previous plane's reads of the tile are done
+        // plane k - 2's reads of this tile ended before plane k - 1's barrier
+        double(*tile)[kUX + 2] = tiles[k & 1];
         tile[ty + 1][tx + 1] = inside ? xm : 0.0;
         if (hl.has) tile[hl.sy][hl.sx] = hv;
         __syncthreads();
