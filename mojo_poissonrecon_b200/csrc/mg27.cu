@@ -177,11 +177,12 @@ __host__ __device__ constexpr float wt1(int d) { return d == 0 ? 1.0f : (d == 1 
 __global__ void __launch_bounds__(128) galerkin_x_kernel(const float* __restrict__ c, int64_t cs,
                                                          const float* __restrict__ S, Geom gf, int cn, int zlo,
                                                          float* __restrict__ out, int64_t ps) {
-    const int I = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;  // flattened over (I, y)
     const int fn = gf.n;
-    if (I >= cn || y >= fn) return;
-    const int z = zlo + blockIdx.z;
-    const int64_t o = ((int64_t)blockIdx.z * fn + y) * cn + I;
+    if (t >= (unsigned)(cn * fn)) return;
+    const int y = (int)(t / (unsigned)cn), I = (int)(t - (unsigned)y * cn);
+    const int z = zlo + blockIdx.y;
+    const int64_t o = ((int64_t)blockIdx.y * fn + y) * cn + I;
 #pragma unroll
     for (int dz = -1; dz <= 1; ++dz)
 #pragma unroll
@@ -212,9 +213,10 @@ __global__ void __launch_bounds__(128) galerkin_x_kernel(const float* __restrict
 // Stage y: node (I, J, z) of cn x cn x slab from stage x's cn x fn x slab.
 __global__ void __launch_bounds__(128) galerkin_y_kernel(const float* __restrict__ in, int64_t pin, int fn, int cn,
                                                          float* __restrict__ out, int64_t pout) {
-    const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
-    if (I >= cn || J >= cn) return;
-    const int zr = blockIdx.z;
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;  // flattened over (I, J)
+    if (t >= (unsigned)(cn * cn)) return;
+    const int J = (int)(t / (unsigned)cn), I = (int)(t - (unsigned)J * cn);
+    const int zr = blockIdx.y;
     const int64_t o = ((int64_t)zr * cn + J) * cn + I;
 #pragma unroll
     for (int dz = -1; dz <= 1; ++dz)
@@ -244,10 +246,11 @@ __global__ void __launch_bounds__(128) galerkin_y_kernel(const float* __restrict
 // 14 planes, zero where the coarse neighbour lies outside the grid.
 __global__ void __launch_bounds__(128) galerkin_z_kernel(const float* __restrict__ in, int64_t pin, int fn, int zlo,
                                                          int k0, float* __restrict__ cc, int64_t cs, Geom gc) {
-    const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;  // flattened over (I, J)
     const int cn = gc.n;
-    if (I >= cn || J >= cn) return;
-    const int K = k0 + blockIdx.z;
+    if (t >= (unsigned)(cn * cn)) return;
+    const int J = (int)(t / (unsigned)cn), I = (int)(t - (unsigned)J * cn);
+    const int K = k0 + blockIdx.y;
     const int64_t p = gc.at(I, J, K);
 #pragma unroll
     for (int my = -1; my <= 1; ++my)
@@ -416,10 +419,13 @@ template <int COLOUR, bool ZERO>
 __global__ void __launch_bounds__(256) relax27p_kernel(const float* __restrict__ prev, float* next,
                                                        const float* __restrict__ rhs, const __half* __restrict__ h,
                                                        const float* __restrict__ inv, Geom g, Packed pk) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    // threads flattened over the plane's compact (i, y) nodes: full warps on odd rows
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = g.n, z = blockIdx.y;
+    if (t >= (unsigned)(pk.Pc * n)) return;
+    const int y = (int)(t / (unsigned)pk.Pc), i = (int)(t - (unsigned)y * pk.Pc);
     const int x = 2 * i + ((y + z + COLOUR) & 1);
-    const int n = g.n;
-    if (x >= n || y >= n) return;
+    if (x >= n) return;
     const int64_t p = g.at(x, y, z), q = pk.at(i, y, z);
     float cf[26];
     load_couplings(h, q, cf);
@@ -447,9 +453,10 @@ __global__ void __launch_bounds__(256) residual27p_kernel(const float* __restric
                                                           const float* __restrict__ i0, const float* __restrict__ i1,
                                                           const float* __restrict__ fac, Geom g, Packed pk,
                                                           float* __restrict__ res) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
-    const int n = g.n;
-    if (x >= n || y >= n) return;
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;  // flattened over the plane's (x, y)
+    const int n = g.n, z = blockIdx.y;
+    if (t >= (unsigned)(n * n)) return;
+    const int y = (int)(t / (unsigned)n), x = (int)(t - (unsigned)y * n);
     const int colour = (x + y + z) & 1;
     const __half* __restrict__ h = colour ? h1 : h0;
     const int64_t p = g.at(x, y, z), q = pk.at(x >> 1, y, z);
@@ -775,13 +782,13 @@ extern "C" int pb_galerkin_f32(const float* fine, int64_t fine_n, int fine_is_7p
         const int nz = zhi - zlo;
         const int64_t px = (int64_t)cn * fn * nz, py = (int64_t)cn * cn * nz;
         float* by = bx + 27 * px;
-        galerkin_x_kernel<<<dim3((cn + 31) / 32, (fn + 3) / 4, nz), block, 0, s>>>(fine, padded_size(fn),
-                                                                                fine_weights, gf, cn, zlo, bx, px);
+        galerkin_x_kernel<<<dim3((cn * fn + 127) / 128, nz), 128, 0, s>>>(fine, padded_size(fn), fine_weights, gf,
+                                                                          cn, zlo, bx, px);
         PB_CHECK_LAUNCH("galerkin_x_kernel");
-        galerkin_y_kernel<<<dim3((cn + 31) / 32, (cn + 3) / 4, nz), block, 0, s>>>(bx, px, fn, cn, by, py);
+        galerkin_y_kernel<<<dim3((cn * cn + 127) / 128, nz), 128, 0, s>>>(bx, px, fn, cn, by, py);
         PB_CHECK_LAUNCH("galerkin_y_kernel");
-        galerkin_z_kernel<<<dim3((cn + 31) / 32, (cn + 3) / 4, k1 - k0), block, 0, s>>>(by, py, fn, zlo, k0, coarse,
-                                                                                     padded_size(cn), gc);
+        galerkin_z_kernel<<<dim3((cn * cn + 127) / 128, k1 - k0), 128, 0, s>>>(by, py, fn, zlo, k0, coarse,
+                                                                              padded_size(cn), gc);
         PB_CHECK_LAUNCH("galerkin_z_kernel");
     }
     return PB_OK;
@@ -912,8 +919,8 @@ extern "C" int pb_relax27p_f32(const float* e_prev, float* e_next, const float* 
     cudaStream_t s = (cudaStream_t)stream;
     const Geom g = geom((int)n);
     const Packed pk = packed_of((int)n);
-    const dim3 block(32, 8);
-    const dim3 grid((pk.Pc + 31) / 32, ((int)n + 7) / 8, (int)n);
+    const dim3 block(256);
+    const dim3 grid((pk.Pc * (int)n + 255) / 256, (int)n);
     const __half *a = (const __half*)h0, *b = (const __half*)h1;
     if (e_prev) {
         relax27p_kernel<0, false><<<grid, block, 0, s>>>(e_prev, e_next, rhs, a, inv0, g, pk);
@@ -937,8 +944,9 @@ extern "C" int pb_residual_restrict27p_f32(const float* e, const float* rhs, con
     cudaStream_t s = (cudaStream_t)stream;
     const int fn = (int)n, cn = (fn + 1) / 2;
     const dim3 block(32, 8);
-    residual27p_kernel<<<node_grid(fn, block), block, 0, s>>>(e, rhs, (const __half*)h0, (const __half*)h1, inv0,
-                                                               inv1, weights, geom(fn), packed_of(fn), res);
+    residual27p_kernel<<<dim3((fn * fn + 255) / 256, fn), 256, 0, s>>>(e, rhs, (const __half*)h0, (const __half*)h1,
+                                                                     inv0, inv1, weights, geom(fn), packed_of(fn),
+                                                                     res);
     PB_CHECK_LAUNCH("residual27p_kernel");
     restrict27_kernel<<<node_grid(cn, block), block, 0, s>>>(res, geom(fn), coarse_rhs, geom(cn));
     PB_CHECK_LAUNCH("restrict27_kernel");

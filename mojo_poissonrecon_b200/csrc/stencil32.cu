@@ -115,14 +115,13 @@ __global__ void sum_partials_kernel(const double* __restrict__ partial, int coun
 // The fine residual of the tile's region (fine x from 2 xc0 - 4, 136 columns;
 // fine y from 2 yc0 - 1, 9 rows), already multiplied by the prolongation weight
 // s, is computed four x at a time (float4 loads of e, rhs, D and s; the row
-// starts stay 16-byte aligned) into a three-plane ring in shared memory, plane
-// 2zc+1 being reused as plane 2(zc+1)-1 of the next coarse plane.  Out-of-grid
+// starts stay 16-byte aligned) into a five-plane ring in shared memory, plane
+// 2zc+1 being reused as plane 2(zc+1)-1 of the next coarse plane; five slots
+// let each coarse plane pass a single barrier.  Out-of-grid
 // ring entries are zero, so the restriction sums all 27 entries with weights
 // (1,2,1)^3 / 64.
-#ifndef PB_RR_CZ
-#define PB_RR_CZ 8  // coarse planes per block
-#endif
-constexpr int kRrCX = 64, kRrCY = 4, kRrCZ = PB_RR_CZ;
+constexpr int kRrCX = 64, kRrCY = 4, kRrCZ = 4;  // coarse tile and planes per block (measured: 8 -> 4, 108 -> 90 us)
+constexpr int kRrRing = 5;                        // fine planes held in shared memory
 constexpr int kRrFX = 2 * kRrCX + 8, kRrFY = 2 * kRrCY + 1;  // 136 x 9 fine nodes
 constexpr int kRrGroups = kRrFX / 4;                            // float4 groups per ring row
 constexpr int kRrThreads = 256;
@@ -133,14 +132,14 @@ __global__ void __launch_bounds__(kRrThreads) residual_restrict32_kernel(const f
                                                                           const float* __restrict__ w, Geom gf,
                                                                           float h2, float* __restrict__ coarse,
                                                                           Geom gc) {
-    __shared__ __align__(16) float ring[3][kRrFY][kRrFX];
+    __shared__ __align__(16) float ring[kRrRing][kRrFY][kRrFX];
     const int fn = gf.n, cn = gc.n;
     const int xc0 = blockIdx.x * kRrCX, yc0 = blockIdx.y * kRrCY;
     const int zc0 = blockIdx.z * kRrCZ, zc1 = min(cn, zc0 + kRrCZ);
     const int fx0 = 2 * xc0 - 4, fy0 = 2 * yc0 - 1;
     const int tid = threadIdx.x;
     auto fine_plane = [&](int f) {  // s-weighted residual of fine plane f over the tile region
-        float(*dst)[kRrFX] = ring[(f + 3) % 3];
+        float(*dst)[kRrFX] = ring[(f + kRrRing) % kRrRing];
         for (int i = tid; i < kRrFY * kRrGroups; i += kRrThreads) {
             const int ly = i / kRrGroups, g = i - ly * kRrGroups;
             const int x = fx0 + 4 * g, y = fy0 + ly;
@@ -184,7 +183,7 @@ __global__ void __launch_bounds__(kRrThreads) residual_restrict32_kernel(const f
                     const int zz = 2 * zc + oz;
 #pragma unroll
                     for (int oy = -1; oy <= 1; ++oy) {
-                        const float* row = ring[(zz + 3) % 3][2 * cy + 1 + oy];
+                        const float* row = ring[(zz + kRrRing) % kRrRing][2 * cy + 1 + oy];
 #pragma unroll
                         for (int ox = -1; ox <= 1; ++ox)
                             sum += row[2 * cx + 4 + ox] * (float)((ox ? 1 : 2) * (oy ? 1 : 2) * (oz ? 1 : 2));
@@ -193,7 +192,9 @@ __global__ void __launch_bounds__(kRrThreads) residual_restrict32_kernel(const f
                 coarse[gc.at(xc, yc, zc)] = sum * (1.0f / 64.0f);
             }
         }
-        __syncthreads();  // the ring slots of planes 2zc-1 and 2zc are rewritten next
+        // no second barrier: the next coarse plane writes fine planes 2zc+2 and
+        // 2zc+3, whose slots (mod 5) differ from the three read here, and the one
+        // after it rewrites these only after all threads pass its first barrier
     }
 }
 

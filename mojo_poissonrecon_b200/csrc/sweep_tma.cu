@@ -285,8 +285,8 @@ static int make_map(CUtensorMap* map, const float* base, int n, int P, int rows)
 // fine += s * trilinear(coarse) (the P_s of mg27.cu; trilinear as in
 // capi.mojo:677-742), s the fine level's prolongation weights.
 // A thread owns four consecutive fine x (one float4 of e and of s; x offset 4
-// keeps them 16-byte aligned), a block a 128 x 8 (x, y) tile and `tz` fine
-// planes (up to kProTZ, fewer on small levels so that the grid still fills
+// keeps them 16-byte aligned), a block 256 consecutive (group, y) slots of a
+// plane and `tz` fine planes (up to kProTZ, fewer on small levels so that the grid still fills
 // the GPU: the planes of a block run one after another).  The four fine nodes of a thread share three coarse values per
 // coarse row: fine x = 4k + j lies on coarse 2k + j/2 (even j) or between
 // 2k + j/2 and the next (odd j).  Fine x >= n (ghost and padding) is never
@@ -296,11 +296,16 @@ constexpr int kProTX = 32, kProTY = 8, kProTZ = 16;
 __global__ void __launch_bounds__(kProTX* kProTY) prolong_add32_kernel(const float* __restrict__ c,
                                                                        float* __restrict__ f,
                                                                        const float* __restrict__ w, int n, int P,
-                                                                       int cn, int cP, int tz) {
-    const int k = blockIdx.x * kProTX + threadIdx.x, y = blockIdx.y * kProTY + threadIdx.y;
+                                                                       int cn, int cP, int tz, int row) {
+    // threads flattened over the plane's (float4 group, y), `row` threads per y:
+    // the group count on short rows (full warps), a whole number of warps on
+    // long ones (a warp's coarse reads stay on one row)
+    const unsigned t = blockIdx.x * (kProTX * kProTY) + threadIdx.x;
+    const int groups = (n + 3) / 4;
+    const int y = (int)(t / (unsigned)row), k = (int)(t - (unsigned)y * row);
+    if (y >= n || k >= groups) return;
     const int x = 4 * k;
-    if (x >= n || y >= n) return;
-    const int z0 = blockIdx.z * tz, z1 = min(n, z0 + tz);
+    const int z0 = blockIdx.y * tz, z1 = min(n, z0 + tz);
     const int ya = y >> 1, yb = min(ya + 1, cn - 1);
     const float ty = (y & 1) ? 0.5f : 0.f;
     const int64_t cplane = (int64_t)(cn + 2) * cP;
@@ -310,7 +315,7 @@ __global__ void __launch_bounds__(kProTX* kProTY) prolong_add32_kernel(const flo
     const int valid = min(4, n - x);
     for (int z = z0; z < z1; ++z) {
         const int za = z >> 1, zb = min(za + 1, cn - 1);
-        const float tz = (z & 1) ? 0.5f : 0.f;
+        const float wz = (z & 1) ? 0.5f : 0.f;
         const float* c0 = ca + (int64_t)(za + 1) * cplane;
         const float* c1 = ca + (int64_t)(zb + 1) * cplane;
         float q[3];
@@ -318,7 +323,7 @@ __global__ void __launch_bounds__(kProTX* kProTY) prolong_add32_kernel(const flo
         for (int i = 0; i < 3; ++i) {
             const float a0 = c0[i] * (1.f - ty) + c0[dy + i] * ty;
             const float a1 = c1[i] * (1.f - ty) + c1[dy + i] * ty;
-            q[i] = a0 * (1.f - tz) + a1 * tz;
+            q[i] = a0 * (1.f - wz) + a1 * wz;
         }
         // x interpolation: t = 0 on even x, 1/2 on odd x (coarse 2k + 2 only weighs odd x < n - 1)
         const float v0 = q[0], v1 = q[0] * 0.5f + q[1] * 0.5f, v2 = q[1], v3 = q[1] * 0.5f + q[2] * 0.5f;
@@ -399,13 +404,14 @@ extern "C" int pb_prolong_fac_f32(const float* coarse, float* fine, const float*
     if (fine_n < 3 || fine_n > 4097 || !coarse || !fine || !weights) return fail(PB_ERR_INVALID, "prolong32: bad args");
     const int n = (int)fine_n, cn = (n + 1) / 2;
     const int groups = (n + 3) / 4;
-    const int gx = (groups + kProTX - 1) / kProTX, gy = (n + kProTY - 1) / kProTY;
+    const int row = groups < 64 ? groups : (groups + 31) / 32 * 32;  // measured: 257^3 keeps whole-warp rows
+    const int gxy = (row * n + kProTX * kProTY - 1) / (kProTX * kProTY);
     // planes per block: as many as keep at least 4 blocks per SM, at most kProTZ
-    const int64_t fill = (int64_t)gx * gy * n / (4 * kSMs);
+    const int64_t fill = (int64_t)gxy * n / (4 * kSMs);
     const int tz = fill < 1 ? 1 : (fill > kProTZ ? kProTZ : (int)fill);
-    const dim3 grid(gx, gy, (n + tz - 1) / tz);
-    prolong_add32_kernel<<<grid, dim3(kProTX, kProTY), 0, (cudaStream_t)stream>>>(coarse, fine, weights, n,
-                                                                                   pitch_for(n), cn, pitch_for(cn), tz);
+    const dim3 grid(gxy, (n + tz - 1) / tz);
+    prolong_add32_kernel<<<grid, kProTX * kProTY, 0, (cudaStream_t)stream>>>(coarse, fine, weights, n, pitch_for(n),
+                                                                              cn, pitch_for(cn), tz, row);
     PB_CHECK_LAUNCH("prolong_add32_kernel");
     return PB_OK;
 }
