@@ -31,7 +31,7 @@
 namespace pb {
 namespace fcg {
 
-constexpr int kTX = 64, kTY = 4, kTZ = 16, kThreads = kTX * kTY;
+constexpr int kTZ = 16, kThreads = 256;  // pass 1: 256 (x, y) columns per block, 16 planes deep
 
 // Pass 2 tile: 32 x 8 nodes per block, 16 planes deep (kTZ).
 constexpr int kUX = 32, kUY = 8, kUThreads = kUX * kUY;
@@ -89,8 +89,9 @@ __global__ void __launch_bounds__(kThreads, 4) direction_sums_kernel(const float
                                                                      double* __restrict__ part) {
     __shared__ double shared[4][32];
     const int n = g.n;
-    const int x = blockIdx.x * kTX + threadIdx.x, y = blockIdx.y * kTY + threadIdx.y;
-    const int z0 = blockIdx.z * kTZ, z1 = min(n, z0 + kTZ);
+    const unsigned t = blockIdx.x * kThreads + threadIdx.x;  // flattened over the plane's (x, y): full warps
+    const int y = t < (unsigned)(n * n) ? (int)(t / (unsigned)n) : n, x = (int)(t - (unsigned)y * n);
+    const int z0 = blockIdx.y * kTZ, z1 = min(n, z0 + kTZ);
     const double h = (double)(n - 1), h2 = h * h;
     const bool first = flags[0] != 0;
     const float* __restrict__ pp = (flags[1] & 1) ? p1 : p0;
@@ -298,11 +299,11 @@ __global__ void loop_kernel(cudaGraphConditionalHandle handle, int use_handle, c
     if (use_handle) cudaGraphSetConditional(handle, more ? 1u : 0u);
 }
 
-static dim3 grid_of(int n) { return dim3((n + kTX - 1) / kTX, (n + kTY - 1) / kTY, (n + kTZ - 1) / kTZ); }
+static dim3 flat_grid_of(int n) { return dim3((n * n + kThreads - 1) / kThreads, (n + kTZ - 1) / kTZ); }
 static dim3 tile_grid_of(int n) { return dim3((n + kUX - 1) / kUX, (n + kUY - 1) / kUY, (n + kTZ - 1) / kTZ); }
 static unsigned count(dim3 g) { return g.x * g.y * g.z; }
 static unsigned blocks_of(int n) {
-    const unsigned a = count(grid_of(n)), t = count(tile_grid_of(n));
+    const unsigned a = count(flat_grid_of(n)), t = count(tile_grid_of(n));
     return a > t ? a : t;
 }
 static Pad pad_of(int n) {
@@ -339,8 +340,8 @@ extern "C" int pb_fcg_direction_f64(const float* z, const float* p0, const float
     PB_TRY(fcg_check(n, workspace_bytes, workspace));
     double* part = (double*)workspace;
     cudaStream_t s = (cudaStream_t)stream;
-    const dim3 grid = grid_of((int)n);
-    direction_sums_kernel<<<grid, dim3(kTX, kTY), 0, s>>>(z, pad_of((int)n), p0, p1, r32, screen, point_weight,
+    const dim3 grid = flat_grid_of((int)n);
+    direction_sums_kernel<<<grid, kThreads, 0, s>>>(z, pad_of((int)n), p0, p1, r32, screen, point_weight,
                                                           flags, part);
     PB_CHECK_LAUNCH("fcg direction_sums_kernel");
     direction_finish_kernel<<<1, 1024, 0, s>>>(part, (int)count(grid), flags, scal);

@@ -51,21 +51,21 @@ __device__ __forceinline__ double warp_block_sum(double v, double* shared) {
     return r;
 }
 
-// Tiled variant: a block owns a 64 x 4 (x, y) tile and a z range; coordinates
-// come from the launch shape (no 64-bit division per node), rows are read
+// A block owns 256 consecutive (x, y) columns of a plane (one 32-bit division
+// per thread; full warps on 2^k + 1 sides) and a z range; rows are read
 // coalesced, and the z-neighbours of consecutive planes stay in L1/L2.
-constexpr int kDefTX = 64, kDefTY = 4, kDefZ = 16;
+constexpr int kDefThreads = 256, kDefZ = 16;
 
 template <bool UPDATE>
-__global__ void __launch_bounds__(kDefTX* kDefTY) defect_tile_kernel(
+__global__ void __launch_bounds__(kDefThreads) defect_tile_kernel(
     const double* __restrict__ x_old, const float* __restrict__ e, double* __restrict__ x_new,
     const double* __restrict__ b, const double* __restrict__ screen, Geom g, double pw, float* __restrict__ r32,
     double* __restrict__ r64, double* __restrict__ partial) {
     __shared__ double shared[32];
     const int n = g.n;
-    const int x = blockIdx.x * kDefTX + threadIdx.x;
-    const int y = blockIdx.y * kDefTY + threadIdx.y;
-    const int z0 = blockIdx.z * kDefZ, z1 = min(n, z0 + kDefZ);
+    const unsigned t = blockIdx.x * kDefThreads + threadIdx.x;
+    const int y = t < (unsigned)(n * n) ? (int)(t / (unsigned)n) : n, x = (int)(t - (unsigned)y * n);
+    const int z0 = blockIdx.y * kDefZ, z1 = min(n, z0 + kDefZ);
     const double h = (double)(n - 1), h2 = h * h;
     const int64_t nn = (int64_t)n * n;
     double sq = 0.0;
@@ -96,9 +96,8 @@ __global__ void __launch_bounds__(kDefTX* kDefTY) defect_tile_kernel(
             sq += r * r;
         }
     }
-    const double t = warp_block_sum(sq, shared);
-    if (threadIdx.x == 0 && threadIdx.y == 0)
-        partial[(blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = t;
+    const double total = warp_block_sum(sq, shared);
+    if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = total;
 }
 
 __global__ void sum_partials_kernel(const double* __restrict__ partial, int count, double* __restrict__ out) {
@@ -200,7 +199,7 @@ __global__ void __launch_bounds__(kRrThreads) residual_restrict32_kernel(const f
 
 
 static dim3 defect_grid(int n) {
-    return dim3((n + kDefTX - 1) / kDefTX, (n + kDefTY - 1) / kDefTY, (n + kDefZ - 1) / kDefZ);
+    return dim3((n * n + kDefThreads - 1) / kDefThreads, (n + kDefZ - 1) / kDefZ);
 }
 
 unsigned defect_blocks(int n) {
@@ -241,7 +240,7 @@ extern "C" int pb_defect_f64(const double* x_old, const float* e, double* x_new,
     if (!workspace || workspace_bytes < (size_t)blocks * 8) return fail(PB_ERR_WORKSPACE, "defect: workspace too small");
     cudaStream_t s = (cudaStream_t)stream;
     double* partial = (double*)workspace;
-    const dim3 grid = defect_grid((int)n), block(kDefTX, kDefTY);
+    const dim3 grid = defect_grid((int)n), block(kDefThreads);
     if (e)
         defect_tile_kernel<true><<<grid, block, 0, s>>>(x_old, e, x_new, rhs, screen, geom((int)n), point_weight, r32,
                                                         r64, partial);
