@@ -17,6 +17,7 @@ from .core import (
     reconstruct_mesh,
     solve_screened_poisson,
 )
+from .ply import read_ply, write_ply
 
 __version__ = "0.1.0"
 __all__ = [
@@ -28,6 +29,8 @@ __all__ = [
     "extract_isosurface",
     "oriented_points_from_mesh",
     "reconstruct",
+    "read_ply",
     "reconstruct_mesh",
     "solve_screened_poisson",
+    "write_ply",
 ]
