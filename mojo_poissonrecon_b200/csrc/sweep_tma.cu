@@ -371,10 +371,23 @@ extern "C" int pb_sweep_tma_f32(const float* e_in, float* e_out, const float* rh
     prm.nty = (N - 1) / kTY > 0 ? (N - 1) / kTY : 1;
     const int tiles = prm.ntx * prm.nty;
     if (z_chunk <= 0) {
-        const int want = 2 * kSMs;
-        int chunks = want / tiles > 1 ? want / tiles : 1;
-        z_chunk = (N + chunks - 1) / chunks;
-        if (z_chunk < 4) z_chunk = 4;
+        // c chunks per tile: minimise waves x (planes per chunk + the 4 planes a
+        // chunk loads beyond its range), waves = ceil(tiles c / (2 blocks x 148
+        // SMs)).  At 257^3 this picks c = 9 (two waves, 66 us a sweep) over the
+        // one-wave c = 4 (70 us, 40 of 296 slots idle); measured on B200.
+        const int64_t slots = 2 * kSMs;
+        int64_t best = -1;
+        int chosen = 1;
+        for (int c = 1; c <= N; ++c) {
+            const int zc = (N + c - 1) / c;
+            if (zc < 4) break;
+            const int64_t cost = ((int64_t)tiles * c + slots - 1) / slots * (zc + 4);
+            if (best < 0 || cost < best) {
+                best = cost;
+                chosen = c;
+            }
+        }
+        z_chunk = (N + chosen - 1) / chosen;
     }
     prm.z_chunk = (int)z_chunk;
     prm.h2 = (float)((N - 1) * (N - 1));
