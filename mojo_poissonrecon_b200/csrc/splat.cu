@@ -119,9 +119,34 @@ __device__ __forceinline__ int run_length(const uint32_t* __restrict__ keys, int
 }
 
 // Pass 1 (capi.mojo:171-172): density += 2w, screen += w, per node in point order.
-__global__ void splat_density_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
-                                     int64_t records, uint32_t sentinel, const double* __restrict__ weight,
-                                     double* __restrict__ density, double* __restrict__ screen) {
+// The gathers of a run's values (weight[vals[k]], the sample's unit normal) are
+// done first for every record at once, one thread per record, into arrays in
+// sorted record order (gather_weights_kernel, gather_vectors_kernel); a run's
+// head then reads its values contiguously.  Products are rounded where the
+// serial loop rounds them, so the sums are unchanged bit for bit.
+__global__ void gather_weights_kernel(const uint32_t* __restrict__ vals, int64_t records,
+                                      const double* __restrict__ weight, double* __restrict__ out) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < records) out[k] = weight[vals[k]];
+}
+
+// (u_x w, u_y w, u_z w) of each record, w its vector weight, u its sample's unit normal.
+__global__ void gather_vectors_kernel(const uint32_t* __restrict__ vals, int64_t records,
+                                      const double* __restrict__ weight, const double* __restrict__ unit_normals,
+                                      double* __restrict__ px, double* __restrict__ py, double* __restrict__ pz) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= records) return;
+    const uint32_t r = vals[k];
+    const double vw = weight[r];
+    const double* u = unit_normals + 3 * (int64_t)(r >> 3);
+    px[k] = u[0] * vw;
+    py[k] = u[1] * vw;
+    pz[k] = u[2] * vw;
+}
+
+__global__ void splat_density_kernel(const uint32_t* __restrict__ keys, int64_t records, uint32_t sentinel,
+                                     const double* __restrict__ gathered, double* __restrict__ density,
+                                     double* __restrict__ screen) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= records) return;
     const uint32_t node = keys[j];
@@ -131,7 +156,7 @@ __global__ void splat_density_kernel(const uint32_t* __restrict__ keys, const ui
         const int m = run_length(keys, k, records, node);
         double w[kRun];
 #pragma unroll
-        for (int t = 0; t < kRun; ++t) w[t] = t < m ? weight[vals[k + t]] : 0.0;
+        for (int t = 0; t < kRun; ++t) w[t] = t < m ? gathered[k + t] : 0.0;
 #pragma unroll
         for (int t = 0; t < kRun; ++t)
             if (t < m) {
@@ -193,9 +218,9 @@ __global__ void splat_vector_weights_kernel(const double* __restrict__ points, c
 }
 
 // Pass 2 (capi.mojo:221-223): V -= n_hat * vector_weight, per node in point order.
-__global__ void splat_vector_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
-                                    int64_t records, uint32_t sentinel, const double* __restrict__ weight,
-                                    const double* __restrict__ unit_normals, double* __restrict__ vx,
+__global__ void splat_vector_kernel(const uint32_t* __restrict__ keys, int64_t records, uint32_t sentinel,
+                                    const double* __restrict__ px, const double* __restrict__ py,
+                                    const double* __restrict__ pz, double* __restrict__ vx,
                                     double* __restrict__ vy, double* __restrict__ vz) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= records) return;
@@ -204,25 +229,19 @@ __global__ void splat_vector_kernel(const uint32_t* __restrict__ keys, const uin
     double ax = vx[node], ay = vy[node], az = vz[node];
     for (int64_t k = j;; k += kRun) {
         const int m = run_length(keys, k, records, node);
-        double vw[kRun], u0[kRun], u1[kRun], u2[kRun];
+        double qx[kRun], qy[kRun], qz[kRun];
 #pragma unroll
         for (int t = 0; t < kRun; ++t) {
-            vw[t] = u0[t] = u1[t] = u2[t] = 0.0;
-            if (t < m) {
-                const uint32_t r = vals[k + t];
-                const double* u = unit_normals + 3 * (int64_t)(r >> 3);
-                vw[t] = weight[r];
-                u0[t] = u[0];
-                u1[t] = u[1];
-                u2[t] = u[2];
-            }
+            qx[t] = t < m ? px[k + t] : 0.0;
+            qy[t] = t < m ? py[k + t] : 0.0;
+            qz[t] = t < m ? pz[k + t] : 0.0;
         }
 #pragma unroll
         for (int t = 0; t < kRun; ++t)
-            if (t < m) {
-                ax -= u0[t] * vw[t];
-                ay -= u1[t] * vw[t];
-                az -= u2[t] * vw[t];
+            if (t < m) {  // V -= n_hat * w: the product was rounded by the gather, as here
+                ax -= qx[t];
+                ay -= qy[t];
+                az -= qz[t];
             }
         if (m < kRun) break;
     }
@@ -238,6 +257,7 @@ __global__ void store_count_kernel(const unsigned long long* __restrict__ src, i
 struct SplatWork {
     uint32_t *keys, *keys_alt, *vals, *vals_alt;
     double* weight;
+    double *gx, *gy, *gz;  // gathered values in sorted record order
     double* unit_normals;
     unsigned long long* accepted;
 };
@@ -250,6 +270,9 @@ static SplatWork splat_carve(Workspace& w, int64_t count) {
     o.vals = w.take<uint32_t>(records);
     o.vals_alt = w.take<uint32_t>(records);
     o.weight = w.take<double>(records);
+    o.gx = w.take<double>(records);
+    o.gy = w.take<double>(records);
+    o.gz = w.take<double>(records);
     o.unit_normals = w.take<double>(count * 3);
     o.accepted = w.take<unsigned long long>(1);
     return o;
@@ -310,14 +333,18 @@ extern "C" int pb_splat_f64(const double* points, const double* normals, int64_t
                                       w, s));
     const uint32_t* keys = in_alt ? o.keys_alt : o.keys;
     const uint32_t* vals = in_alt ? o.vals_alt : o.vals;
-    splat_density_kernel<<<blocks_for(records, 256), 256, 0, s>>>(keys, vals, records, sentinel, o.weight, density,
-                                                                   screen);
+    gather_weights_kernel<<<blocks_for(records, 256), 256, 0, s>>>(vals, records, o.weight, o.gx);
+    PB_CHECK_LAUNCH("gather_weights_kernel");
+    splat_density_kernel<<<blocks_for(records, 256), 256, 0, s>>>(keys, records, sentinel, o.gx, density, screen);
     PB_CHECK_LAUNCH("splat_density_kernel");
     splat_vector_weights_kernel<<<blocks_for(point_count, 256), 256, 0, s>>>(
         points, normals, point_count, n, (int)confidence, samples_per_node, density, o.weight, o.unit_normals);
     PB_CHECK_LAUNCH("splat_vector_weights_kernel");
-    splat_vector_kernel<<<blocks_for(records, 256), 256, 0, s>>>(keys, vals, records, sentinel, o.weight,
-                                                                  o.unit_normals, vx, vy, vz);
+    gather_vectors_kernel<<<blocks_for(records, 256), 256, 0, s>>>(vals, records, o.weight, o.unit_normals, o.gx,
+                                                                    o.gy, o.gz);
+    PB_CHECK_LAUNCH("gather_vectors_kernel");
+    splat_vector_kernel<<<blocks_for(records, 256), 256, 0, s>>>(keys, records, sentinel, o.gx, o.gy, o.gz, vx, vy,
+                                                                  vz);
     PB_CHECK_LAUNCH("splat_vector_kernel");
     store_count_kernel<<<1, 1, 0, s>>>(o.accepted, accepted);
     PB_CHECK_LAUNCH("store_count_kernel");
