@@ -49,6 +49,8 @@ __device__ __forceinline__ void pass2_cell(double p, int64_t res, int64_t& i, do
 
 // Records: key = grid node (or the sentinel n^3 for a rejected sample), value =
 // point*8 + corner, corner = dz*4 + dy*2 + dx; weight[record] = pass-1 weight.
+// One thread per record (the eight threads of a point repeat its cell
+// arithmetic), so each array is written with coalesced stores.
 __global__ void splat_records_kernel(const double* __restrict__ points, const double* __restrict__ normals,
                                      int64_t count, int64_t n, int confidence, uint32_t* __restrict__ keys,
                                      uint32_t* __restrict__ vals, double* __restrict__ weight,
@@ -56,19 +58,17 @@ __global__ void splat_records_kernel(const double* __restrict__ points, const do
     __shared__ unsigned int block_accepted;
     if (threadIdx.x == 0) block_accepted = 0;
     __syncthreads();
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < count) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < 8 * count) {
+        const int64_t p = r >> 3;
+        const int c = (int)(r & 7), dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
         const int64_t res = n - 1;
         double nx = normals[3 * p], ny = normals[3 * p + 1], nz = normals[3 * p + 2];
         double length = norm3(nx, ny, nz);
-        const uint32_t r0 = (uint32_t)(p * 8);
+        vals[r] = (uint32_t)r;
         if (length <= 0.0) {  // capi.mojo:132-133
-            const uint32_t sentinel = (uint32_t)(n * n * n);
-            for (int c = 0; c < 8; ++c) {
-                keys[r0 + c] = sentinel;
-                vals[r0 + c] = r0 + c;
-                weight[r0 + c] = 0.0;
-            }
+            keys[r] = (uint32_t)(n * n * n);
+            weight[r] = 0.0;
         } else {
             double sw = confidence ? length : 1.0;
             int64_t ix, iy, iz;
@@ -76,20 +76,12 @@ __global__ void splat_records_kernel(const double* __restrict__ points, const do
             pass1_cell(points[3 * p], res, ix, fx);
             pass1_cell(points[3 * p + 1], res, iy, fy);
             pass1_cell(points[3 * p + 2], res, iz, fz);
-            for (int dz = 0; dz < 2; ++dz) {
-                double wz = dz == 1 ? fz : 1.0 - fz;
-                for (int dy = 0; dy < 2; ++dy) {
-                    double wy = dy == 1 ? fy : 1.0 - fy;
-                    for (int dx = 0; dx < 2; ++dx) {
-                        double wx = dx == 1 ? fx : 1.0 - fx;
-                        const int c = dz * 4 + dy * 2 + dx;
-                        keys[r0 + c] = (uint32_t)grid_index(ix + dx, iy + dy, iz + dz, n);
-                        vals[r0 + c] = r0 + c;
-                        weight[r0 + c] = wx * wy * wz * sw;
-                    }
-                }
-            }
-            atomicAdd(&block_accepted, 1u);
+            const double wz = dz == 1 ? fz : 1.0 - fz;
+            const double wy = dy == 1 ? fy : 1.0 - fy;
+            const double wx = dx == 1 ? fx : 1.0 - fx;
+            keys[r] = (uint32_t)grid_index(ix + dx, iy + dy, iz + dz, n);
+            weight[r] = wx * wy * wz * sw;
+            if (c == 0) atomicAdd(&block_accepted, 1u);
         }
     }
     __syncthreads();
@@ -175,46 +167,63 @@ __global__ void splat_vector_weights_kernel(const double* __restrict__ points, c
                                             int64_t count, int64_t n, int confidence, double samples_per_node,
                                             const double* __restrict__ density, double* __restrict__ weight,
                                             double* __restrict__ unit_normals) {
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= count) return;
-    double nx = normals[3 * p], ny = normals[3 * p + 1], nz = normals[3 * p + 2];
-    double length = norm3(nx, ny, nz);
-    if (length <= 0.0) return;  // capi.mojo:181-182
-    const int64_t res = n - 1;
-    double sw = confidence ? length : 1.0;
-    unit_normals[3 * p] = nx / length;
-    unit_normals[3 * p + 1] = ny / length;
-    unit_normals[3 * p + 2] = nz / length;
-    int64_t ix, iy, iz;
-    double fx, fy, fz;
-    pass2_cell(points[3 * p], res, ix, fx);
-    pass2_cell(points[3 * p + 1], res, iy, fy);
-    pass2_cell(points[3 * p + 2], res, iz, fz);
-    double local = 0.0;
-    for (int dz = 0; dz < 2; ++dz) {
-        double wz = dz == 1 ? fz : 1.0 - fz;
-        for (int dy = 0; dy < 2; ++dy) {
-            double wy = dy == 1 ? fy : 1.0 - fy;
-            for (int dx = 0; dx < 2; ++dx) {
-                double wx = dx == 1 ? fx : 1.0 - fx;
-                local += density[grid_index(ix + dx, iy + dy, iz + dz, n)] * wx * wy * wz;
+    // each warp's 32 x 8 weights go through shared memory so the stores are
+    // contiguous; records of points that set none keep their pass-1 weight
+    __shared__ double staged[256 / 32][32 * 8];
+    __shared__ unsigned char written[256 / 32][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    written[warp][lane] = 0;
+    bool active = p < count;
+    double nx = 0.0, ny = 0.0, nz = 0.0, length = 0.0;
+    if (active) {
+        nx = normals[3 * p];
+        ny = normals[3 * p + 1];
+        nz = normals[3 * p + 2];
+        length = norm3(nx, ny, nz);
+        active = length > 0.0;  // capi.mojo:181-182
+    }
+    if (active) {
+        const int64_t res = n - 1;
+        double sw = confidence ? length : 1.0;
+        unit_normals[3 * p] = nx / length;
+        unit_normals[3 * p + 1] = ny / length;
+        unit_normals[3 * p + 2] = nz / length;
+        int64_t ix, iy, iz;
+        double fx, fy, fz;
+        pass2_cell(points[3 * p], res, ix, fx);
+        pass2_cell(points[3 * p + 1], res, iy, fy);
+        pass2_cell(points[3 * p + 2], res, iz, fz);
+        double local = 0.0;
+        for (int dz = 0; dz < 2; ++dz) {
+            double wz = dz == 1 ? fz : 1.0 - fz;
+            for (int dy = 0; dy < 2; ++dy) {
+                double wy = dy == 1 ? fy : 1.0 - fy;
+                for (int dx = 0; dx < 2; ++dx) {
+                    double wx = dx == 1 ? fx : 1.0 - fx;
+                    local += density[grid_index(ix + dx, iy + dy, iz + dz, n)] * wx * wy * wz;
+                }
             }
         }
-    }
-    double q = local / samples_per_node;
-    double factor = 1.0 > q ? 1.0 : q;
-    const int64_t r0 = p * 8;
-    for (int dz = 0; dz < 2; ++dz) {
-        double wz = dz == 1 ? fz : 1.0 - fz;
-        for (int dy = 0; dy < 2; ++dy) {
-            double wy = dy == 1 ? fy : 1.0 - fy;
-            for (int dx = 0; dx < 2; ++dx) {
-                double wx = dx == 1 ? fx : 1.0 - fx;
-                double w = wx * wy * wz * sw;
-                weight[r0 + dz * 4 + dy * 2 + dx] = w * (double)res / factor;
+        double q = local / samples_per_node;
+        double factor = 1.0 > q ? 1.0 : q;
+        for (int dz = 0; dz < 2; ++dz) {
+            double wz = dz == 1 ? fz : 1.0 - fz;
+            for (int dy = 0; dy < 2; ++dy) {
+                double wy = dy == 1 ? fy : 1.0 - fy;
+                for (int dx = 0; dx < 2; ++dx) {
+                    double wx = dx == 1 ? fx : 1.0 - fx;
+                    double w = wx * wy * wz * sw;
+                    staged[warp][lane * 8 + dz * 4 + dy * 2 + dx] = w * (double)res / factor;
+                }
             }
         }
+        written[warp][lane] = 1;
     }
+    __syncwarp();
+    const int64_t r0 = ((int64_t)blockIdx.x * blockDim.x + warp * 32) * 8;  // the warp's first record
+    for (int e = lane; e < 32 * 8; e += 32)
+        if (written[warp][e >> 3]) weight[r0 + e] = staged[warp][e];
 }
 
 // Pass 2 (capi.mojo:221-223): V -= n_hat * vector_weight, per node in point order.
@@ -325,8 +334,9 @@ extern "C" int pb_splat_f64(const double* points, const double* normals, int64_t
     const int64_t records = point_count * 8;
     const uint32_t sentinel = (uint32_t)(n * n * n);
     PB_CHECK_CUDA(cudaMemsetAsync(o.accepted, 0, sizeof(unsigned long long), s), "splat accepted");
-    splat_records_kernel<<<blocks_for(point_count, 256), 256, 0, s>>>(points, normals, point_count, n, (int)confidence,
-                                                                      o.keys, o.vals, o.weight, o.accepted);
+    splat_records_kernel<<<blocks_for(8 * point_count, 256), 256, 0, s>>>(points, normals, point_count, n,
+                                                                          (int)confidence, o.keys, o.vals, o.weight,
+                                                                          o.accepted);
     PB_CHECK_LAUNCH("splat_records_kernel");
     bool in_alt = false;
     PB_TRY(radix_sort_pairs<uint32_t>(o.keys, o.vals, o.keys_alt, o.vals_alt, records, bit_width(sentinel), &in_alt,
