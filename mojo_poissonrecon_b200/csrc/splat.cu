@@ -136,29 +136,48 @@ __global__ void gather_vectors_kernel(const uint32_t* __restrict__ vals, int64_t
     pz[k] = u[2] * vw;
 }
 
-__global__ void splat_density_kernel(const uint32_t* __restrict__ keys, int64_t records, uint32_t sentinel,
-                                     const double* __restrict__ gathered, double* __restrict__ density,
-                                     double* __restrict__ screen) {
-    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+// Run heads: the first record of each node's run (sentinel runs excluded),
+// compacted in record order so the run sums below take one thread per run
+// with full warps (one thread per record left ~2 of 32 lanes busy).
+__global__ void run_head_flags_kernel(const uint32_t* __restrict__ keys, int64_t records, uint32_t sentinel,
+                                      uint32_t* __restrict__ flag) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= records) return;
     const uint32_t node = keys[j];
-    if (node == sentinel || (j > 0 && keys[j - 1] == node)) return;
-    double d = density[node], s = screen[node];
-    for (int64_t k = j;; k += kRun) {
-        const int m = run_length(keys, k, records, node);
-        double w[kRun];
+    flag[j] = node != sentinel && (j == 0 || keys[j - 1] != node);
+}
+
+__global__ void run_heads_kernel(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ rank,
+                                 int64_t records, uint32_t* __restrict__ heads) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < records && flag[j]) heads[rank[j]] = (uint32_t)j;
+}
+
+__global__ void splat_density_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ heads,
+                                     const uint32_t* __restrict__ head_count, int64_t records,
+                                     const double* __restrict__ gathered, double* __restrict__ density,
+                                     double* __restrict__ screen) {
+    const uint32_t runs = *head_count;
+    for (uint32_t hd = blockIdx.x * blockDim.x + threadIdx.x; hd < runs; hd += gridDim.x * blockDim.x) {
+        const int64_t j = heads[hd];
+        const uint32_t node = keys[j];
+        double d = density[node], s = screen[node];
+        for (int64_t k = j;; k += kRun) {
+            const int m = run_length(keys, k, records, node);
+            double w[kRun];
 #pragma unroll
-        for (int t = 0; t < kRun; ++t) w[t] = t < m ? gathered[k + t] : 0.0;
+            for (int t = 0; t < kRun; ++t) w[t] = t < m ? gathered[k + t] : 0.0;
 #pragma unroll
-        for (int t = 0; t < kRun; ++t)
-            if (t < m) {
-                d += 2.0 * w[t];
-                s += w[t];
-            }
-        if (m < kRun) break;
+            for (int t = 0; t < kRun; ++t)
+                if (t < m) {
+                    d += 2.0 * w[t];
+                    s += w[t];
+                }
+            if (m < kRun) break;
+        }
+        density[node] = d;
+        screen[node] = s;
     }
-    density[node] = d;
-    screen[node] = s;
 }
 
 // Pass 2, per sample (capi.mojo:176-209): local density from the pass-1 grid,
@@ -227,36 +246,38 @@ __global__ void splat_vector_weights_kernel(const double* __restrict__ points, c
 }
 
 // Pass 2 (capi.mojo:221-223): V -= n_hat * vector_weight, per node in point order.
-__global__ void splat_vector_kernel(const uint32_t* __restrict__ keys, int64_t records, uint32_t sentinel,
+__global__ void splat_vector_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ heads,
+                                    const uint32_t* __restrict__ head_count, int64_t records,
                                     const double* __restrict__ px, const double* __restrict__ py,
                                     const double* __restrict__ pz, double* __restrict__ vx,
                                     double* __restrict__ vy, double* __restrict__ vz) {
-    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= records) return;
-    const uint32_t node = keys[j];
-    if (node == sentinel || (j > 0 && keys[j - 1] == node)) return;
-    double ax = vx[node], ay = vy[node], az = vz[node];
-    for (int64_t k = j;; k += kRun) {
-        const int m = run_length(keys, k, records, node);
-        double qx[kRun], qy[kRun], qz[kRun];
+    const uint32_t runs = *head_count;
+    for (uint32_t hd = blockIdx.x * blockDim.x + threadIdx.x; hd < runs; hd += gridDim.x * blockDim.x) {
+        const int64_t j = heads[hd];
+        const uint32_t node = keys[j];
+        double ax = vx[node], ay = vy[node], az = vz[node];
+        for (int64_t k = j;; k += kRun) {
+            const int m = run_length(keys, k, records, node);
+            double qx[kRun], qy[kRun], qz[kRun];
 #pragma unroll
-        for (int t = 0; t < kRun; ++t) {
-            qx[t] = t < m ? px[k + t] : 0.0;
-            qy[t] = t < m ? py[k + t] : 0.0;
-            qz[t] = t < m ? pz[k + t] : 0.0;
-        }
-#pragma unroll
-        for (int t = 0; t < kRun; ++t)
-            if (t < m) {  // V -= n_hat * w: the product was rounded by the gather, as here
-                ax -= qx[t];
-                ay -= qy[t];
-                az -= qz[t];
+            for (int t = 0; t < kRun; ++t) {
+                qx[t] = t < m ? px[k + t] : 0.0;
+                qy[t] = t < m ? py[k + t] : 0.0;
+                qz[t] = t < m ? pz[k + t] : 0.0;
             }
-        if (m < kRun) break;
+#pragma unroll
+            for (int t = 0; t < kRun; ++t)
+                if (t < m) {  // V -= n_hat * w: the product was rounded by the gather, as here
+                    ax -= qx[t];
+                    ay -= qy[t];
+                    az -= qz[t];
+                }
+            if (m < kRun) break;
+        }
+        vx[node] = ax;
+        vy[node] = ay;
+        vz[node] = az;
     }
-    vx[node] = ax;
-    vy[node] = ay;
-    vz[node] = az;
 }
 
 __global__ void store_count_kernel(const unsigned long long* __restrict__ src, int64_t* __restrict__ dst) {
@@ -267,6 +288,7 @@ struct SplatWork {
     uint32_t *keys, *keys_alt, *vals, *vals_alt;
     double* weight;
     double *gx, *gy, *gz;  // gathered values in sorted record order
+    uint32_t *flag, *rank, *heads, *head_count;  // run heads in record order
     double* unit_normals;
     unsigned long long* accepted;
 };
@@ -282,6 +304,10 @@ static SplatWork splat_carve(Workspace& w, int64_t count) {
     o.gx = w.take<double>(records);
     o.gy = w.take<double>(records);
     o.gz = w.take<double>(records);
+    o.flag = w.take<uint32_t>(records);
+    o.rank = w.take<uint32_t>(records);
+    o.heads = w.take<uint32_t>(records);
+    o.head_count = w.take<uint32_t>(1);
     o.unit_normals = w.take<double>(count * 3);
     o.accepted = w.take<unsigned long long>(1);
     return o;
@@ -291,6 +317,7 @@ static size_t splat_ws_bytes(int64_t count) {
     return measure([&](Workspace& w) {
         splat_carve(w, count);
         radix_carve<uint32_t>(w, count * 8);
+        scan_carve<uint32_t>(w, count * 8);
     });
 }
 
@@ -343,9 +370,15 @@ extern "C" int pb_splat_f64(const double* points, const double* normals, int64_t
                                       w, s));
     const uint32_t* keys = in_alt ? o.keys_alt : o.keys;
     const uint32_t* vals = in_alt ? o.vals_alt : o.vals;
+    run_head_flags_kernel<<<blocks_for(records, 256), 256, 0, s>>>(keys, records, sentinel, o.flag);
+    PB_CHECK_LAUNCH("run_head_flags_kernel");
+    PB_TRY(exclusive_scan<uint32_t>(o.flag, o.rank, records, o.head_count, w, s));
+    run_heads_kernel<<<blocks_for(records, 256), 256, 0, s>>>(o.flag, o.rank, records, o.heads);
+    PB_CHECK_LAUNCH("run_heads_kernel");
+    const unsigned run_blocks = 8 * kSMs;  // grid-stride over the runs (their count stays on the device)
     gather_weights_kernel<<<blocks_for(records, 256), 256, 0, s>>>(vals, records, o.weight, o.gx);
     PB_CHECK_LAUNCH("gather_weights_kernel");
-    splat_density_kernel<<<blocks_for(records, 256), 256, 0, s>>>(keys, records, sentinel, o.gx, density, screen);
+    splat_density_kernel<<<run_blocks, 256, 0, s>>>(keys, o.heads, o.head_count, records, o.gx, density, screen);
     PB_CHECK_LAUNCH("splat_density_kernel");
     splat_vector_weights_kernel<<<blocks_for(point_count, 256), 256, 0, s>>>(
         points, normals, point_count, n, (int)confidence, samples_per_node, density, o.weight, o.unit_normals);
@@ -353,8 +386,8 @@ extern "C" int pb_splat_f64(const double* points, const double* normals, int64_t
     gather_vectors_kernel<<<blocks_for(records, 256), 256, 0, s>>>(vals, records, o.weight, o.unit_normals, o.gx,
                                                                     o.gy, o.gz);
     PB_CHECK_LAUNCH("gather_vectors_kernel");
-    splat_vector_kernel<<<blocks_for(records, 256), 256, 0, s>>>(keys, records, sentinel, o.gx, o.gy, o.gz, vx, vy,
-                                                                  vz);
+    splat_vector_kernel<<<run_blocks, 256, 0, s>>>(keys, o.heads, o.head_count, records, o.gx, o.gy, o.gz, vx, vy,
+                                                    vz);
     PB_CHECK_LAUNCH("splat_vector_kernel");
     store_count_kernel<<<1, 1, 0, s>>>(o.accepted, accepted);
     PB_CHECK_LAUNCH("store_count_kernel");
