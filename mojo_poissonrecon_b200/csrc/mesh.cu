@@ -53,26 +53,44 @@ __global__ void face_records_kernel(const double* __restrict__ v, int64_t nv, co
     }
 }
 
-// One thread per run of records with the same vertex: the vertex's summed
-// normal (zero-initialised), in face order; referenced[v] = 1.
-__global__ void vertex_sums_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
-                                   int64_t records, uint32_t sentinel, const double* __restrict__ cross,
-                                   double* __restrict__ normals, uint32_t* __restrict__ referenced) {
+// Run heads (first record of each vertex's run, sentinel runs excluded),
+// compacted in record order so the sums take one thread per run, full warps.
+__global__ void head_flags_kernel(const uint32_t* __restrict__ keys, int64_t records, uint32_t sentinel,
+                                  uint32_t* __restrict__ flag) {
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= records) return;
     const uint32_t vert = keys[j];
-    if (vert == sentinel || (j > 0 && keys[j - 1] == vert)) return;
-    double x = 0.0, y = 0.0, z = 0.0;
-    for (int64_t k = j; k < records && keys[k] == vert; ++k) {
-        const int64_t f = vals[k] / 3;
-        x += cross[3 * f];
-        y += cross[3 * f + 1];
-        z += cross[3 * f + 2];
+    flag[j] = vert != sentinel && (j == 0 || keys[j - 1] != vert);
+}
+
+__global__ void heads_kernel(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ rank, int64_t records,
+                             uint32_t* __restrict__ heads) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < records && flag[j]) heads[rank[j]] = (uint32_t)j;
+}
+
+// One thread per run of records with the same vertex: the vertex's summed
+// normal (zero-initialised), in face order; referenced[v] = 1.
+__global__ void vertex_sums_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                                   int64_t records, const uint32_t* __restrict__ heads,
+                                   const uint32_t* __restrict__ head_count, const double* __restrict__ cross,
+                                   double* __restrict__ normals, uint32_t* __restrict__ referenced) {
+    const uint32_t runs = *head_count;
+    for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < runs; h += gridDim.x * blockDim.x) {
+        const int64_t j = heads[h];
+        const uint32_t vert = keys[j];
+        double x = 0.0, y = 0.0, z = 0.0;
+        for (int64_t k = j; k < records && keys[k] == vert; ++k) {
+            const int64_t f = vals[k] / 3;
+            x += cross[3 * f];
+            y += cross[3 * f + 1];
+            z += cross[3 * f + 2];
+        }
+        normals[3 * (int64_t)vert] = x;
+        normals[3 * (int64_t)vert + 1] = y;
+        normals[3 * (int64_t)vert + 2] = z;
+        referenced[vert] = 1;
     }
-    normals[3 * (int64_t)vert] = x;
-    normals[3 * (int64_t)vert + 1] = y;
-    normals[3 * (int64_t)vert + 2] = z;
-    referenced[vert] = 1;
 }
 
 // keep[v] (in place over referenced[v]) and the vertex's length.
@@ -109,6 +127,7 @@ __global__ void store_kept_count_kernel(const uint32_t* __restrict__ total, cons
 
 struct Work {
     uint32_t *keys, *keys_alt, *vals, *vals_alt, *keep, *rank, *total;
+    uint32_t *flag, *head_rank, *heads, *head_count;
     double *cross, *normals, *length;
     int* bad;
 };
@@ -127,6 +146,10 @@ inline Work carve(Workspace& w, int64_t nv, int64_t nf) {
     o.rank = w.take<uint32_t>(nv + 1);
     o.total = w.take<uint32_t>(1);
     o.bad = w.take<int>(1);
+    o.flag = w.take<uint32_t>(records);
+    o.head_rank = w.take<uint32_t>(records);
+    o.heads = w.take<uint32_t>(records);
+    o.head_count = w.take<uint32_t>(1);
     return o;
 }
 
@@ -135,6 +158,7 @@ inline size_t ws_bytes(int64_t nv, int64_t nf) {
         carve(w, nv, nf);
         radix_carve<uint32_t>(w, 3 * nf);
         scan_carve<uint32_t>(w, nv);
+        scan_carve<uint32_t>(w, 3 * nf);
     });
 }
 
@@ -186,9 +210,16 @@ extern "C" int pb_mesh_normals_count_f64(const double* vertices, int64_t vertex_
         Workspace sort_ws = w;
         PB_TRY(radix_sort_pairs<uint32_t>(o.keys, o.vals, o.keys_alt, o.vals_alt, 3 * face_count,
                                           bit_width(sentinel), &in_alt, sort_ws, s));
-        vertex_sums_kernel<<<blocks_for(3 * face_count, kT), kT, 0, s>>>(
-            in_alt ? o.keys_alt : o.keys, in_alt ? o.vals_alt : o.vals, 3 * face_count, sentinel, o.cross,
-            o.normals, o.keep);
+        const uint32_t* keys = in_alt ? o.keys_alt : o.keys;
+        const int64_t records = 3 * face_count;
+        head_flags_kernel<<<blocks_for(records, kT), kT, 0, s>>>(keys, records, sentinel, o.flag);
+        PB_CHECK_LAUNCH("head_flags_kernel");
+        Workspace head_ws = w;
+        PB_TRY(exclusive_scan<uint32_t>(o.flag, o.head_rank, records, o.head_count, head_ws, s));
+        heads_kernel<<<blocks_for(records, kT), kT, 0, s>>>(o.flag, o.head_rank, records, o.heads);
+        PB_CHECK_LAUNCH("heads_kernel");
+        vertex_sums_kernel<<<8 * kSMs, kT, 0, s>>>(keys, in_alt ? o.vals_alt : o.vals, records, o.heads,
+                                                   o.head_count, o.cross, o.normals, o.keep);
         PB_CHECK_LAUNCH("vertex_sums_kernel");
     }
     if (vertex_count) {
