@@ -63,6 +63,20 @@ __device__ __forceinline__ bool inside(int x, int y, int z, int n) {
     return (unsigned)x < (unsigned)n && (unsigned)y < (unsigned)n && (unsigned)z < (unsigned)n;
 }
 
+// Node of this thread on a level of side m, threads flattened over each plane's
+// (x, y) (blockIdx.x) with the plane in blockIdx.y: full warps on 2^k + 1 sides.
+// False past the plane's last node.
+__device__ __forceinline__ bool plane_node(int m, int& x, int& y, int& z) {
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (unsigned)(m * m)) return false;
+    y = (int)(t / (unsigned)m);
+    x = (int)(t - (unsigned)y * m);
+    z = blockIdx.y;
+    return true;
+}
+
+inline dim3 plane_grid(int m, int threads) { return dim3((m * m + threads - 1) / threads, m); }
+
 // ---- Galerkin product A_c = P_s^T A P_s / 8 -----------------------------------
 // One thread per coarse node J streams once over the fine nodes i = 2J + o of
 // J's support (27) and their stencil neighbours j = i + K (7 on level 0, 27
@@ -144,10 +158,9 @@ __device__ __forceinline__ void galerkin_store(const float* acc, float* __restri
 __global__ void __launch_bounds__(128) galerkin7_kernel(const float* __restrict__ D, const float* __restrict__ S,
                                                         Geom gf, float h2, float* __restrict__ cc, int64_t cs,
                                                         Geom gc) {
-    const int xc = blockIdx.x * blockDim.x + threadIdx.x, yc = blockIdx.y * blockDim.y + threadIdx.y;
-    const int zc = blockIdx.z;
     const int cn = gc.n;
-    if (xc >= cn || yc >= cn) return;
+    int xc, yc, zc;
+    if (!plane_node(cn, xc, yc, zc)) return;
     float acc[14];
 #pragma unroll
     for (int k = 0; k < 14; ++k) acc[k] = 0.0f;
@@ -282,9 +295,9 @@ __global__ void __launch_bounds__(128) galerkin_z_kernel(const float* __restrict
 
 // A 7-point level (diagonal D, off-diagonals -h2 inside the grid) as 14 planes.
 __global__ void level7_to_27_kernel(const float* __restrict__ D, Geom g, float h2, float* __restrict__ c, int64_t cs) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
     const int n = g.n;
-    if (x >= n || y >= n) return;
+    int x, y, z;
+    if (!plane_node(n, x, y, z)) return;
     const int64_t p = g.at(x, y, z);
     c[p] = D[p];
 #pragma unroll
@@ -297,9 +310,9 @@ __global__ void level7_to_27_kernel(const float* __restrict__ D, Geom g, float h
 // 1/a_JJ and the prolongation weight s_J of a 27-point level.
 __global__ void level27_finish_kernel(const float* __restrict__ c, int64_t cs, Geom g, float* __restrict__ invD,
                                       float* __restrict__ fac) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
     const int n = g.n;
-    if (x >= n || y >= n) return;
+    int x, y, z;
+    if (!plane_node(n, x, y, z)) return;
     const int64_t p = g.at(x, y, z);
     float off = 0.0f;
 #pragma unroll
@@ -321,8 +334,8 @@ __global__ void level27_finish_kernel(const float* __restrict__ c, int64_t cs, G
 // out-of-grid fine nodes are ghosts holding zero.
 __global__ void __launch_bounds__(256) restrict27_kernel(const float* __restrict__ res, Geom gf,
                                                          float* __restrict__ coarse, Geom gc) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
-    if (x >= gc.n || y >= gc.n) return;
+    int x, y, z;
+    if (!plane_node(gc.n, x, y, z)) return;
     const int64_t p = gf.at(2 * x, 2 * y, 2 * z);
     float s = 0.0f;
 #pragma unroll
@@ -374,9 +387,9 @@ inline Packed packed_of(int n) {
 __global__ void __launch_bounds__(256) pack27_kernel(const float* __restrict__ c, int64_t cs, Geom g, Packed pk,
                                                      __half* __restrict__ h0, __half* __restrict__ h1,
                                                      float* __restrict__ i0, float* __restrict__ i1) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
     const int n = g.n;
-    if (x >= n || y >= n) return;
+    int x, y, z;
+    if (!plane_node(n, x, y, z)) return;
     const int colour = (x + y + z) & 1;
     const int64_t q = pk.at(x >> 1, y, z);
     const int64_t p = g.at(x, y, z);
@@ -725,7 +738,6 @@ __global__ void __launch_bounds__(kC27Threads) coarse27_kernel(const float4* __r
     }
 }
 
-inline dim3 node_grid(int n, dim3 block) { return dim3((n + block.x - 1) / block.x, (n + block.y - 1) / block.y, n); }
 
 }  // namespace pb
 
@@ -761,10 +773,9 @@ extern "C" int pb_galerkin_f32(const float* fine, int64_t fine_n, int fine_is_7p
     const int fn = (int)fine_n, cn = (fn + 1) / 2;
     const Geom gf = geom(fn), gc = geom(cn);
     cudaStream_t s = (cudaStream_t)stream;
-    const dim3 block(32, 4);
     if (fine_is_7pt) {
         const float h2 = (float)(fn - 1) * (float)(fn - 1);
-        galerkin7_kernel<<<node_grid(cn, block), block, 0, s>>>(fine, fine_weights, gf, h2, coarse, padded_size(cn),
+        galerkin7_kernel<<<plane_grid(cn, 128), 128, 0, s>>>(fine, fine_weights, gf, h2, coarse, padded_size(cn),
                                                                 gc);
         PB_CHECK_LAUNCH("galerkin7_kernel");
         return PB_OK;
@@ -797,8 +808,7 @@ extern "C" int pb_galerkin_f32(const float* fine, int64_t fine_n, int fine_is_7p
 // 14 planes of a 7-point level (diagonal D, off-diagonals -(n-1)^2).
 extern "C" int pb_level27_from7_f32(const float* D, int64_t n, float* coef, void* stream) {
     if (!level_side_ok(n) || !D || !coef) return fail(PB_ERR_INVALID, "level27 from 7: bad args");
-    const dim3 block(32, 4);
-    level7_to_27_kernel<<<node_grid((int)n, block), block, 0, (cudaStream_t)stream>>>(
+    level7_to_27_kernel<<<plane_grid((int)n, 128), 128, 0, (cudaStream_t)stream>>>(
         D, geom((int)n), (float)(n - 1) * (float)(n - 1), coef, padded_size((int)n));
     PB_CHECK_LAUNCH("level7_to_27_kernel");
     return PB_OK;
@@ -807,8 +817,7 @@ extern "C" int pb_level27_from7_f32(const float* D, int64_t n, float* coef, void
 // invD = 1 / diagonal and the prolongation weights of a 27-point level.
 extern "C" int pb_level27_finish_f32(const float* coef, int64_t n, float* invD, float* weights, void* stream) {
     if (!level_side_ok(n) || !coef || !invD || !weights) return fail(PB_ERR_INVALID, "level27 finish: bad args");
-    const dim3 block(32, 4);
-    level27_finish_kernel<<<node_grid((int)n, block), block, 0, (cudaStream_t)stream>>>(
+    level27_finish_kernel<<<plane_grid((int)n, 128), 128, 0, (cudaStream_t)stream>>>(
         coef, padded_size((int)n), geom((int)n), invD, weights);
     PB_CHECK_LAUNCH("level27_finish_kernel");
     return PB_OK;
@@ -904,8 +913,7 @@ extern "C" int pb_packed27_size(int64_t n, int64_t* coupling_bytes, int64_t* inv
 extern "C" int pb_pack27_f32(const float* coef, int64_t n, void* h0, void* h1, float* inv0, float* inv1,
                              void* stream) {
     if (!level_side_ok(n) || !coef || !h0 || !h1 || !inv0 || !inv1) return fail(PB_ERR_INVALID, "pack27: bad args");
-    const dim3 block(32, 8);
-    pack27_kernel<<<node_grid((int)n, block), block, 0, (cudaStream_t)stream>>>(
+    pack27_kernel<<<plane_grid((int)n, 256), 256, 0, (cudaStream_t)stream>>>(
         coef, padded_size((int)n), geom((int)n), packed_of((int)n), (__half*)h0, (__half*)h1, inv0, inv1);
     PB_CHECK_LAUNCH("pack27_kernel");
     return PB_OK;
@@ -943,12 +951,11 @@ extern "C" int pb_residual_restrict27p_f32(const float* e, const float* rhs, con
         return fail(PB_ERR_INVALID, "residual_restrict27p: bad args");
     cudaStream_t s = (cudaStream_t)stream;
     const int fn = (int)n, cn = (fn + 1) / 2;
-    const dim3 block(32, 8);
     residual27p_kernel<<<dim3((fn * fn + 255) / 256, fn), 256, 0, s>>>(e, rhs, (const __half*)h0, (const __half*)h1,
                                                                      inv0, inv1, weights, geom(fn), packed_of(fn),
                                                                      res);
     PB_CHECK_LAUNCH("residual27p_kernel");
-    restrict27_kernel<<<node_grid(cn, block), block, 0, s>>>(res, geom(fn), coarse_rhs, geom(cn));
+    restrict27_kernel<<<plane_grid(cn, 256), 256, 0, s>>>(res, geom(fn), coarse_rhs, geom(cn));
     PB_CHECK_LAUNCH("restrict27_kernel");
     return PB_OK;
 }
