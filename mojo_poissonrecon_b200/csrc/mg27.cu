@@ -77,13 +77,14 @@ __device__ __forceinline__ bool plane_node(int m, int& x, int& y, int& z) {
 
 inline dim3 plane_grid(int m, int threads) { return dim3((m * m + threads - 1) / threads, m); }
 
-// ---- Galerkin product A_c = P_s^T A P_s / 8 -----------------------------------
+// ---- Galerkin product A_c = P_s^T A P_s / 8 from level 0 ------------------------
 // One thread per coarse node J streams once over the fine nodes i = 2J + o of
-// J's support (27) and their stencil neighbours j = i + K (7 on level 0, 27
-// below), and scatters the product p_iJ a_ij s_j into the stored entries
-// A_c[J, J+m] (m = 0 or forward) whose column support holds j, with weight
-// P(d - 2m), d = o + K.  Every index and weight is resolved at compile time,
-// so the 14 sums stay in registers.
+// J's support (27) and their 7-point stencil neighbours j = i + K, and
+// scatters the product p_iJ a_ij s_j into the stored entries A_c[J, J+m]
+// (m = 0 or forward) whose column support holds j, with weight P(d - 2m),
+// d = o + K.  Every index and weight is resolved at compile time, so the 14
+// sums stay in registers.  (From a 27-point level the product is separable:
+// see the x, y, z stages below.)
 __device__ __forceinline__ void scatter14(float v, int dx, int dy, int dz, float* acc) {
 #pragma unroll
     for (int mz = -1; mz <= 1; ++mz)
@@ -99,13 +100,12 @@ __device__ __forceinline__ void scatter14(float v, int dx, int dy, int dz, float
             }
 }
 
-// The sums for one coarse node.  FINE7: `fc` is the level-0 diagonal D
-// (couplings -h2 to in-grid face neighbours); otherwise `fc` holds the fine
-// level's 14 planes.  S: the fine level's prolongation weights.  INTERIOR:
-// every i and j of J lies in the grid (no bounds tests).
-template <bool FINE7, bool INTERIOR>
-__device__ __forceinline__ void galerkin_sums(const float* __restrict__ fc, int64_t fs, const float* __restrict__ S,
-                                              const Geom& gf, float h2, int xc, int yc, int zc, float* acc) {
+// The sums for one coarse node below level 0: `D` is the level-0 diagonal
+// (couplings -h2 to in-grid face neighbours), S its prolongation weights.
+// INTERIOR: every i and j of J lies in the grid (no bounds tests).
+template <bool INTERIOR>
+__device__ __forceinline__ void galerkin7_sums(const float* __restrict__ D, const float* __restrict__ S,
+                                               const Geom& gf, float h2, int xc, int yc, int zc, float* acc) {
     const int fn = gf.n;
 #pragma unroll
     for (int oz = -1; oz <= 1; ++oz)
@@ -123,21 +123,14 @@ __device__ __forceinline__ void galerkin_sums(const float* __restrict__ fc, int6
                     for (int ky = -1; ky <= 1; ++ky)
 #pragma unroll
                         for (int kx = -1; kx <= 1; ++kx) {
-                            if (FINE7 && (kx != 0) + (ky != 0) + (kz != 0) > 1) continue;
+                            if ((kx != 0) + (ky != 0) + (kz != 0) > 1) continue;  // 7-point stencil
                             if (!INTERIOR && !inside(xi + kx, yi + ky, zi + kz, fn)) continue;
-                            float a;
-                            if (kx == 0 && ky == 0 && kz == 0)
-                                a = fc[pi];
-                            else if (FINE7)
-                                a = -h2;
-                            else
-                                a = coupling(fc, fs, gf, pi, kx, ky, kz);
+                            const float a = (kx == 0 && ky == 0 && kz == 0) ? D[pi] : -h2;
                             scatter14(si * a * S[pi + offset_of(gf, kx, ky, kz)], ox + kx, oy + ky, oz + kz, acc);
                         }
             }
 }
 
-template <bool FINE7>
 __device__ __forceinline__ void galerkin_store(const float* acc, float* __restrict__ cc, int64_t cs, const Geom& gc,
                                                int xc, int yc, int zc) {
     const int64_t p = gc.at(xc, yc, zc);
@@ -165,10 +158,10 @@ __global__ void __launch_bounds__(128) galerkin7_kernel(const float* __restrict_
 #pragma unroll
     for (int k = 0; k < 14; ++k) acc[k] = 0.0f;
     if (xc >= 1 && yc >= 1 && zc >= 1 && xc <= cn - 2 && yc <= cn - 2 && zc <= cn - 2)
-        galerkin_sums<true, true>(D, 0, S, gf, h2, xc, yc, zc, acc);
+        galerkin7_sums<true>(D, S, gf, h2, xc, yc, zc, acc);
     else
-        galerkin_sums<true, false>(D, 0, S, gf, h2, xc, yc, zc, acc);
-    galerkin_store<true>(acc, cc, cs, gc, xc, yc, zc);
+        galerkin7_sums<false>(D, S, gf, h2, xc, yc, zc, acc);
+    galerkin_store(acc, cc, cs, gc, xc, yc, zc);
 }
 
 // ---- separable product for a 27-point fine level ---------------------------------
