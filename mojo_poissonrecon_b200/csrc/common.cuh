@@ -42,6 +42,29 @@ __host__ __device__ __forceinline__ int64_t grid_index(int64_t x, int64_t y, int
     return (z * n + y) * n + x;
 }
 
+// Unsigned 32-bit division by an invariant divisor d as a multiply-high and
+// shifts (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994, round-up variant): with l = ceil(log2 d) and
+// m = floor(2^32 (2^l - d) / d) + 1, n / d = (t + ((n - t) >> 1)) >> (l - 1)
+// where t = mulhi(m, n), exact for every 32-bit n and 2 <= d < 2^32.
+struct FastDiv {
+    uint32_t d = 1, m = 0, s = 0;
+    FastDiv() = default;
+    explicit FastDiv(uint32_t divisor) : d(divisor) {
+        if (d >= 2) {
+            int l = 0;
+            while ((1ull << l) < d) ++l;
+            m = (uint32_t)(((1ull << 32) * ((1ull << l) - d)) / d + 1);
+            s = (uint32_t)(l - 1);
+        }
+    }
+    __device__ __forceinline__ uint32_t div(uint32_t n) const {
+        if (d == 1) return n;
+        const uint32_t t = __umulhi(m, n);
+        return (t + ((n - t) >> 1)) >> s;
+    }
+};
+
 inline unsigned blocks_for(int64_t items, int threads) {
     int64_t b = (items + threads - 1) / threads;
     return (unsigned)(b < 1 ? 1 : b);

@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(kT) sign_bits_kernel(const double* __restrict_
 
 // active cells (corners on both sides, capi.mojo:946-960) as bits, and the
 // popcount of each 32-cell word (scanned in place into the word's first id).
-__global__ void __launch_bounds__(kT) cell_words_kernel(const uint32_t* __restrict__ bits, uint32_t n,
+__global__ void __launch_bounds__(kT) cell_words_kernel(const uint32_t* __restrict__ bits, uint32_t n, FastDiv dc,
                                                         uint32_t cells3, uint32_t* __restrict__ active,
                                                         uint32_t* __restrict__ counts) {
     const uint32_t c = n - 1, nn = n * n, lane = threadIdx.x & 31;
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(kT) cell_words_kernel(const uint32_t* __restri
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i - lane < cells3; i += stride) {
         bool a = false;
         if (i < cells3) {
-            const uint32_t ci = (uint32_t)i, x = ci % c, t = ci / c, y = t % c, z = t / c;
+            const uint32_t ci = (uint32_t)i, t = dc.div(ci), x = ci - t * c, z = dc.div(t), y = t - z * c;
             const uint32_t i0 = (z * n + y) * n + x;
             const uint32_t below = bit_at(bits, i0) + bit_at(bits, i0 + 1) + bit_at(bits, i0 + n) +
                                    bit_at(bits, i0 + n + 1) + bit_at(bits, i0 + nn) + bit_at(bits, i0 + nn + 1) +
@@ -399,41 +399,47 @@ __global__ void __launch_bounds__(kT) cell_words_kernel(const uint32_t* __restri
 }
 
 // Edge `local` of sweep s (capi.mojo:1090-1128): its lower node; sweep order z, y, x.
-__device__ __forceinline__ void sweep_edge(int s, uint32_t local, uint32_t c, uint32_t& x, uint32_t& y, uint32_t& z) {
-    const uint32_t cm1 = c - 1;
+struct SideDiv {  // the cell count per axis c and c - 1, as invariant divisors
+    uint32_t c;
+    FastDiv dc, dm;
+};
+
+__device__ __forceinline__ void sweep_edge(int s, uint32_t local, const SideDiv& sd, uint32_t& x, uint32_t& y,
+                                           uint32_t& z) {
+    const uint32_t c = sd.c, cm1 = c - 1;
     if (s == 0) {  // x-edges: z, y in [1, c), x in [0, c)
-        x = local % c;
-        const uint32_t t = local / c;
-        y = 1 + t % cm1;
-        z = 1 + t / cm1;
+        const uint32_t t = sd.dc.div(local), u = sd.dm.div(t);
+        x = local - t * c;
+        y = 1 + (t - u * cm1);
+        z = 1 + u;
     } else if (s == 1) {  // y-edges: z in [1, c), y in [0, c), x in [1, c)
-        x = 1 + local % cm1;
-        const uint32_t t = local / cm1;
-        y = t % c;
-        z = 1 + t / c;
+        const uint32_t t = sd.dm.div(local), u = sd.dc.div(t);
+        x = 1 + (local - t * cm1);
+        y = t - u * c;
+        z = 1 + u;
     } else {  // z-edges: z in [0, c), y, x in [1, c)
-        x = 1 + local % cm1;
-        const uint32_t t = local / cm1;
-        y = 1 + t % cm1;
-        z = t / cm1;
+        const uint32_t t = sd.dm.div(local), u = sd.dm.div(t);
+        x = 1 + (local - t * cm1);
+        y = 1 + (t - u * cm1);
+        z = u;
     }
 }
 
 // Sign-changing edges of the three sweeps as bits (word w of sweep s at
 // s * words + w) and per-word popcounts.  An interior edge that changes sign
 // lies on four active cells, so it always yields a quad.
-__global__ void __launch_bounds__(kT) edge_words_kernel(const uint32_t* __restrict__ bits, uint32_t n,
+__global__ void __launch_bounds__(kT) edge_words_kernel(const uint32_t* __restrict__ bits, uint32_t n, SideDiv sd,
                                                         uint32_t per_sweep, uint32_t words,
                                                         uint32_t* __restrict__ fwords, uint32_t* __restrict__ counts) {
     const int s = blockIdx.y;
-    const uint32_t c = n - 1, lane = threadIdx.x & 31;
+    const uint32_t lane = threadIdx.x & 31;
     const uint32_t step = s == 0 ? 1u : (s == 1 ? n : n * n);
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e - lane < per_sweep; e += stride) {
         bool a = false;
         if (e < per_sweep) {
             uint32_t x, y, z;
-            sweep_edge(s, (uint32_t)e, c, x, y, z);
+            sweep_edge(s, (uint32_t)e, sd, x, y, z);
             const uint32_t i0 = (z * n + y) * n + x;
             a = bit_at(bits, i0) != bit_at(bits, i0 + step);
         }
@@ -452,7 +458,7 @@ __global__ void store_counts_kernel(const uint32_t* __restrict__ totals, int64_t
 
 // One thread per 32-cell word: each active cell's vertex at id = its rank.
 __global__ void __launch_bounds__(kT) vertex_words_kernel(const double* __restrict__ field,
-                                                          const double* __restrict__ density, uint32_t n,
+                                                          const double* __restrict__ density, uint32_t n, FastDiv dc,
                                                           IsoArg iso_arg, const uint32_t* __restrict__ active,
                                                           const uint32_t* __restrict__ first, uint32_t cell_words,
                                                           double* __restrict__ vertices,
@@ -468,7 +474,7 @@ __global__ void __launch_bounds__(kT) vertex_words_kernel(const double* __restri
     while (m) {
         const uint32_t b = __ffs(m) - 1;
         m &= m - 1;
-        const uint32_t ci = 32 * w + b, x = ci % c, t = ci / c, y = t % c, z = t / c;
+        const uint32_t ci = 32 * w + b, t = dc.div(ci), x = ci - t * c, z = dc.div(t), y = t - z * c;
         cell_vertex(field, density, n, x, y, z, iso, cells_d, vertices + 3 * (int64_t)id, vertex_density + id);
         ++id;
     }
@@ -481,7 +487,7 @@ __device__ __forceinline__ int64_t cell_id(const uint32_t* __restrict__ active, 
 
 // One thread per 32-edge word: each sign-changing edge's two triangles at
 // quad = its rank (capi.mojo:1040-1071).
-__global__ void __launch_bounds__(kT) face_words_kernel(const uint32_t* __restrict__ bits, uint32_t n,
+__global__ void __launch_bounds__(kT) face_words_kernel(const uint32_t* __restrict__ bits, uint32_t n, SideDiv sd,
                                                         uint32_t words, const uint32_t* __restrict__ fwords,
                                                         const uint32_t* __restrict__ ffirst,
                                                         const uint32_t* __restrict__ active,
@@ -498,7 +504,7 @@ __global__ void __launch_bounds__(kT) face_words_kernel(const uint32_t* __restri
         const uint32_t b = __ffs(m) - 1;
         m &= m - 1;
         uint32_t x, y, z;
-        sweep_edge(s, 32 * w + b, c, x, y, z);
+        sweep_edge(s, 32 * w + b, sd, x, y, z);
         const bool reverse = bit_at(bits, (z * n + y) * n + x) != 0;
         uint32_t q[4];
         if (s == 0) {
@@ -651,13 +657,17 @@ extern "C" int pb_extract_count_f64(const double* field, int64_t n, const double
     const IsoArg ia{0.0, iso};
     fast::sign_bits_kernel<<<fast::grid_for(L.nodes), fast::kT, 0, s>>>(field, L.nodes, ia, L.bits);
     PB_CHECK_LAUNCH("sign_bits_kernel");
-    fast::cell_words_kernel<<<fast::grid_for(L.cells3), fast::kT, 0, s>>>(L.bits, L.n, L.cells3, L.active, L.first);
+    const FastDiv dc(L.n - 1);
+    const fast::SideDiv sd{L.n - 1, dc, FastDiv(L.n - 2)};
+    fast::cell_words_kernel<<<fast::grid_for(L.cells3), fast::kT, 0, s>>>(L.bits, L.n, dc, L.cells3, L.active,
+                                                                           L.first);
     PB_CHECK_LAUNCH("cell_words_kernel");
     Workspace scan_ws = L.scratch();
     PB_TRY(exclusive_scan<uint32_t>(L.first, L.first, L.cell_words, L.totals, scan_ws, s));
     if (L.per_sweep) {
-        fast::edge_words_kernel<<<dim3(fast::grid_for(L.per_sweep), 3), fast::kT, 0, s>>>(L.bits, L.n, L.per_sweep,
-                                                                                           L.words, L.fwords, L.ffirst);
+        fast::edge_words_kernel<<<dim3(fast::grid_for(L.per_sweep), 3), fast::kT, 0, s>>>(L.bits, L.n, sd,
+                                                                                           L.per_sweep, L.words,
+                                                                                           L.fwords, L.ffirst);
         PB_CHECK_LAUNCH("edge_words_kernel");
         Workspace scan_ws2 = L.scratch();
         PB_TRY(exclusive_scan<uint32_t>(L.ffirst, L.ffirst, 3 * (int64_t)L.words, L.totals + 1, scan_ws2, s));
@@ -686,12 +696,13 @@ extern "C" int pb_extract_emit_f64(const double* field, const double* density, i
     const IsoArg ia{0.0, iso};
     if (vertices) {
         fast::vertex_words_kernel<<<(L.cell_words + fast::kT - 1) / fast::kT, fast::kT, 0, s>>>(
-            field, density, L.n, ia, L.active, L.first, L.cell_words, vertices, vertex_density);
+            field, density, L.n, FastDiv(L.n - 1), ia, L.active, L.first, L.cell_words, vertices, vertex_density);
         PB_CHECK_LAUNCH("vertex_words_kernel");
     }
     if (faces && L.per_sweep) {
         fast::face_words_kernel<<<dim3((L.words + fast::kT - 1) / fast::kT, 3), fast::kT, 0, s>>>(
-            L.bits, L.n, L.words, L.fwords, L.ffirst, L.active, L.first, faces);
+            L.bits, L.n, fast::SideDiv{L.n - 1, FastDiv(L.n - 1), FastDiv(L.n - 2)}, L.words, L.fwords, L.ffirst,
+            L.active, L.first, faces);
         PB_CHECK_LAUNCH("face_words_kernel");
     }
     return PB_OK;

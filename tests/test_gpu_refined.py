@@ -154,3 +154,27 @@ def test_refined_mesh_matches_fp64_mesh():
     b = mpr.reconstruct(pts, nrm, depth=7, confidence=True, tol=1e-8, precision="fp32_refined")
     assert abs(a.faces.shape[0] - b.faces.shape[0]) <= 0.001 * a.faces.shape[0]
     assert b.iso_value == pytest.approx(a.iso_value, rel=1e-6)
+
+
+def test_engine_graphs_replay_new_inputs():
+    """An engine captures its prologue and iteration graphs on the first solve
+    and replays them afterwards: a second system solved on the same engine
+    gives the same field, bit for bit, as that system on a fresh engine."""
+    from mojo_poissonrecon_b200 import _native as nat
+    from mojo_poissonrecon_b200 import solver32
+
+    n = 65
+    rng = np.random.default_rng(11)
+    systems = []
+    for _ in range(2):
+        screen = torch.from_numpy(rng.random((n, n, n)) * (rng.random((n, n, n)) < 0.1)).cuda()
+        rhs = torch.from_numpy(rng.normal(size=(n, n, n))).cuda()
+        systems.append((rhs, screen))
+    ws = nat.Workspace(torch.device("cuda"))
+    solver32.clear_engines()
+    solver32.solve_refined(*systems[0], 4.0, ws)  # captures the graphs
+    replayed, stats = solver32.solve_refined(*systems[1], 4.0, ws)
+    assert stats.relative_residual <= 1e-8
+    solver32.clear_engines()
+    fresh, _ = solver32.solve_refined(*systems[1], 4.0, ws)
+    assert torch.equal(replayed, fresh)
