@@ -8,26 +8,29 @@ flexible conjugate gradients:
     while ||r|| > tol * ||b||:               evaluated on the device
         z = V-cycle on A e = r, e = 0        FP32
         p = z - beta p;  x += alpha p;  r = b - A x                 FP64 (pb_fcg_direction_f64,
-                                                                         pb_fcg_update_f64)
+                                                                         pb_fcg_update_f64;
+                                                                         p stored in FP32)
 
 One iteration touches the same buffers every time, so the engine captures it
 once as the body of a CUDA graph WHILE node whose condition a device kernel
 sets from ||r||^2 (pb_loop_condition); a solve is then one graph launch with
-no host synchronisation per iteration.  Engines (hierarchy, vectors, graph)
-are cached per device, grid side and point weight and reused across solves.
+no host synchronisation per iteration.  The prologue (level set-up, x0 and its
+residual, ||b||) is captured once as a second graph.  Engines (hierarchy,
+vectors, graphs) are cached per device, grid side, point weight and slot and
+reused across solves.
 
 Defect correction (``precision="fp32_defect"``): x += V(r), one FP32 V-cycle
 per FP64 residual, eager launches.
 
 The FP32 cycle: level 0 is the reference's operator with its red-black
 Gauss-Seidel smoother (core.py:141-193; the reference runs 3 sweeps each way,
-the preconditioner level0_sweeps(n)); the coarser
-levels are Galerkin operators with screening-scaled transfers (mg27.cu),
-smoothed by COARSE_SWEEPS sweeps each way (on levels of side > 9 with their
-couplings packed per colour in FP16), which cut the cycles needed for a
-given residual 2-4x against the reference's rediscretised hierarchy.  Levels
-of side <= 9 run in a single launch from shared memory, the 3^3 level solved exactly with its
-inverse (built once per set-up).  Convergence is always measured with the
+the preconditioner level0_sweeps(n)); the coarser levels are Galerkin
+operators with screening-scaled transfers (mg27.cu), smoothed by
+COARSE_SWEEPS sweeps each way (on levels of side > 9 with their couplings
+packed per colour in FP16), which cut the cycles needed for a given residual
+2-4x against the reference's rediscretised hierarchy.  Levels of side <= 9
+run in a single launch from shared memory, the 3^3 level solved exactly with
+its inverse (built once per set-up).  Convergence is always measured with the
 reference's FP64 operator.
 """
 
