@@ -32,12 +32,19 @@ def _numpy(a) -> np.ndarray:
     return np.asarray(a)
 
 
+_PLY_TYPES = {np.dtype("u1"): "uchar", np.dtype("i1"): "char", np.dtype("u2"): "ushort", np.dtype("i2"): "short",
+              np.dtype("u4"): "uint", np.dtype("i4"): "int", np.dtype("f4"): "float", np.dtype("f8"): "double"}
+
+
 def write_ply(path, mesh, *, binary: bool = True, coordinates: str = "float", density: bool = True,
-              comment: str | None = None) -> None:
+              properties: dict | None = None, comment: str | None = None) -> None:
     """Write `mesh` (vertices (V, 3), faces (F, 3), density (V,)) to `path`.
 
     coordinates: "float" or "double" for x, y, z (and the density `value`).
     density: write each vertex's density as a `value` property.
+    properties: further per-vertex scalars {name: (V,) array}, written after
+    them in the array's own type (uint8, int8, (u)int16, (u)int32, float32,
+    float64; e.g. colours as uint8 "red", "green", "blue").
     Raises ValueError on malformed arrays or face indices outside [0, V)."""
     if coordinates not in ("float", "double"):
         raise ValueError("coordinates must be 'float' or 'double'")
@@ -49,6 +56,16 @@ def write_ply(path, mesh, *, binary: bool = True, coordinates: str = "float", de
         raise ValueError("density must have one value per vertex")
     if nf and (faces.min() < 0 or faces.max() >= nv):
         raise ValueError("face indices must lie in [0, vertex count)")
+    extra = []
+    for name, values_k in (properties or {}).items():
+        arr = _numpy(values_k).reshape(-1)
+        if arr.dtype not in _PLY_TYPES:
+            raise ValueError(f"property {name!r}: unsupported type {arr.dtype}")
+        if arr.shape[0] != nv:
+            raise ValueError(f"property {name!r} must have one value per vertex")
+        if name in ("x", "y", "z", "value") or not name.isidentifier():
+            raise ValueError(f"property name {name!r} is reserved or not a plain identifier")
+        extra.append((name, arr))
     ctype = "f4" if coordinates == "float" else "f8"
 
     header = ["ply", "format " + ("binary_little_endian" if binary else "ascii") + " 1.0",
@@ -62,6 +79,7 @@ def write_ply(path, mesh, *, binary: bool = True, coordinates: str = "float", de
     header.extend(f"property {coordinates} {axis}" for axis in "xyz")
     if values is not None:
         header.append(f"property {coordinates} value")
+    header.extend(f"property {_PLY_TYPES[arr.dtype]} {name}" for name, arr in extra)
     header.append(f"element face {nf}")
     header.append("property list uchar int vertex_indices")
     header.append("end_header")
@@ -70,10 +88,13 @@ def write_ply(path, mesh, *, binary: bool = True, coordinates: str = "float", de
     fields = [("x", "<" + ctype), ("y", "<" + ctype), ("z", "<" + ctype)]
     if values is not None:
         fields.append(("value", "<" + ctype))
+    fields.extend((name, arr.dtype.newbyteorder("<")) for name, arr in extra)
     vrec = np.empty(nv, dtype=fields)
     vrec["x"], vrec["y"], vrec["z"] = vertices[:, 0], vertices[:, 1], vertices[:, 2]
     if values is not None:
         vrec["value"] = values
+    for name, arr in extra:
+        vrec[name] = arr
     frec = np.empty(nf, dtype=[("n", "u1"), ("v", "<i4", (3,))])
     frec["n"] = 3
     frec["v"] = faces
@@ -84,11 +105,14 @@ def write_ply(path, mesh, *, binary: bool = True, coordinates: str = "float", de
         if binary:
             f.write(vrec.tobytes())
             f.write(frec.tobytes())
-        else:  # shortest round-tripping decimal of each stored value
-            cols = np.column_stack([vertices] + ([values] if values is not None else [])).astype(ctype)
-            vfmt = " ".join(["%.9g" if coordinates == "float" else "%.17g"] * len(fields))
+        else:  # shortest round-tripping decimal of each stored value, integers as integers
+            cfmt = "%.9g" if coordinates == "float" else "%.17g"
+            fmts = [cfmt] * (3 + (values is not None))
+            fmts += ["%d" if arr.dtype.kind in "iu" else ("%.9g" if arr.dtype == np.float32 else "%.17g")
+                     for _, arr in extra]
             if nv:
-                np.savetxt(f, cols, fmt=vfmt)
+                rows = zip(*([vrec[name] for name, _ in fields]))
+                f.write("".join(" ".join(fm % v for fm, v in zip(fmts, row)) + "\n" for row in rows).encode("ascii"))
             if nf:
                 np.savetxt(f, np.column_stack([np.full(nf, 3), faces]), fmt="%d")
 

@@ -28,6 +28,34 @@ def test_round_trip(tmp_path, binary, coordinates):
     assert any(c.startswith("iso_value 0.123456789") for c in back["comments"])
 
 
+@pytest.mark.parametrize("binary", [True, False])
+def test_vertex_properties(tmp_path, binary):
+    """Per-vertex colours (uint8) and a float32 scalar round-trip in their own
+    types, after the density."""
+    mesh = _mesh(30, 20, seed=3)
+    rng = np.random.default_rng(4)
+    colours = {c: rng.integers(0, 256, 30).astype(np.uint8) for c in ("red", "green", "blue")}
+    quality = rng.random(30).astype(np.float32)
+    path = tmp_path / "c.ply"
+    write_ply(path, mesh, binary=binary, properties={**colours, "quality": quality})
+    head = path.read_bytes().split(b"end_header")[0].decode()
+    assert "property uchar red" in head and "property float quality" in head
+    assert head.index("property float value") < head.index("property uchar red")
+    back = read_ply(path)
+    for c, v in colours.items():
+        assert back["properties"][c].dtype == np.uint8 and np.array_equal(back["properties"][c], v)
+    assert np.array_equal(back["properties"]["quality"], quality)
+    assert np.array_equal(back["faces"], mesh.faces)
+
+
+def test_vertex_properties_rejected(tmp_path):
+    mesh = _mesh(5, 3)
+    for bad in ({"red": np.zeros(4, np.uint8)}, {"x": np.zeros(5)}, {"bad name": np.zeros(5)},
+                {"flag": np.zeros(5, bool)}):
+        with pytest.raises(ValueError):
+            write_ply(tmp_path / "m.ply", mesh, properties=bad)
+
+
 def test_header_and_sizes(tmp_path):
     mesh = _mesh(5, 4)
     path = tmp_path / "m.ply"
