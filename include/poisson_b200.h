@@ -88,6 +88,21 @@ int pb_splat_f64(const double *points, const double *normals, int64_t point_coun
                  int64_t confidence, double *density, double *vx, double *vy, double *vz,
                  double *screen, double samples_per_node, int64_t *accepted,
                  void *workspace, size_t workspace_bytes, void *stream);
+/* Auxiliary attribute interpolation (no counterpart in the reference, which
+ * lists it among upstream PoissonRecon features it leaves out, README.md:31-36):
+ * per-sample attributes (point_count x channels, row-major FP64) of unit-cube
+ * samples splatted with the samples' pass-1 weights w, summed per node in
+ * sample order: grids (channels + 1 planes of n^3, overwritten) get sum w a_c
+ * and, last, sum w.  Then the values at mesh vertices (world coordinates, `map`
+ * = the (min x, y, z, width) of pb_prepare_points_f64): the ratio of the
+ * trilinear interpolants of sum w a_c and sum w over the vertex's cell, 0
+ * where no weight reaches it.  1 <= channels <= 64. */
+size_t pb_splat_attributes_workspace_size(int64_t point_count);
+int pb_splat_attributes_f64(const double *points, const double *normals, int64_t point_count, int64_t n,
+                            int64_t confidence, const double *attributes, int64_t channels, double *grids,
+                            void *workspace, size_t workspace_bytes, void *stream);
+int pb_sample_attributes_f64(const double *vertices, int64_t vertex_count, const double *map, int64_t n,
+                             const double *grids, int64_t channels, double *out, void *stream);
 
 /* mpr_assemble_f64 (_lib.py:24; capi.mojo:228-279):
  * rhs = -div(V) + point_weight * screen * (n-1)^2 * target_value. Bit-exact. */

@@ -17,6 +17,7 @@ from .core import (
     reconstruct_mesh,
     solve_screened_poisson,
 )
+from .attributes import interpolate_attributes
 from .ply import read_ply, write_ply
 
 __version__ = "0.1.0"
@@ -27,6 +28,7 @@ __all__ = [
     "build",
     "build_octree",
     "extract_isosurface",
+    "interpolate_attributes",
     "oriented_points_from_mesh",
     "reconstruct",
     "read_ply",

@@ -33,6 +33,9 @@ _SIGNATURES = {
     "pb_octree_emit": ([I, I, P, I, P, P, P, P, P, P, P, S, P], C),
     "pb_splat_workspace_size": ([I, I], S),
     "pb_splat_f64": ([P, P, I, I, I, P, P, P, P, P, F, P, P, S, P], C),
+    "pb_splat_attributes_workspace_size": ([I], S),
+    "pb_splat_attributes_f64": ([P, P, I, I, I, P, I, P, P, S, P], C),
+    "pb_sample_attributes_f64": ([P, I, P, I, P, I, P, P], C),
     "pb_assemble_f64": ([P, P, P, P, P, I, F, F, P], C),
     "pb_relax_f64": ([P, P, P, I, F, I, P], C),
     "pb_residual_workspace_size": ([I], S),

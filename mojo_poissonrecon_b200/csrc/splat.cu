@@ -280,6 +280,67 @@ __global__ void splat_vector_kernel(const uint32_t* __restrict__ keys, const uin
     }
 }
 
+// ---- auxiliary attributes (upstream PoissonRecon's colour interpolation) --------
+// Each sample's k attributes are splatted with its pass-1 weights w (the
+// screening weights), per node in record order: planes 0 .. k-1 of `grids`
+// hold sum w a_c, plane k holds sum w.  One thread per run, one channel at a
+// time (deterministic sums).
+__global__ void attribute_runs_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                                      const uint32_t* __restrict__ heads, const uint32_t* __restrict__ head_count,
+                                      int64_t records, const double* __restrict__ weight,
+                                      const double* __restrict__ attributes, int channels, int64_t plane,
+                                      double* __restrict__ grids) {
+    const uint32_t runs = *head_count;
+    for (uint32_t hd = blockIdx.x * blockDim.x + threadIdx.x; hd < runs; hd += gridDim.x * blockDim.x) {
+        const int64_t j = heads[hd];
+        const uint32_t node = keys[j];
+        for (int c = 0; c <= channels; ++c) {
+            double sum = 0.0;
+            for (int64_t k = j; k < records && keys[k] == node; ++k) {
+                const uint32_t r = vals[k];
+                const double w = weight[r];
+                sum += c < channels ? w * attributes[(int64_t)(r >> 3) * channels + c] : w;
+            }
+            grids[c * plane + node] = sum;
+        }
+    }
+}
+
+// Per vertex (world coordinates, mapped to the unit cube by `map` = (min x, y,
+// z, width)): the ratio of the trilinear interpolants of sum w a_c and sum w
+// over its cell (zero where no sample's weight reaches the cell).
+__global__ void sample_attributes_kernel(const double* __restrict__ vertices, int64_t count,
+                                         const double* __restrict__ map, int64_t n, const double* __restrict__ grids,
+                                         int channels, double* __restrict__ out) {
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= count) return;
+    const int64_t res = n - 1, plane = n * n * n;
+    int64_t ix[3];
+    double f[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double u = (vertices[3 * v + a] - map[a]) / map[3];
+        pass2_cell(u, res, ix[a], f[a]);
+    }
+    double den = 0.0;
+    for (int c = 0; c <= channels; ++c) {
+        double num = 0.0;
+        for (int dz = 0; dz < 2; ++dz) {
+            const double wz = dz == 1 ? f[2] : 1.0 - f[2];
+            for (int dy = 0; dy < 2; ++dy) {
+                const double wy = dy == 1 ? f[1] : 1.0 - f[1];
+                for (int dx = 0; dx < 2; ++dx) {
+                    const double wx = dx == 1 ? f[0] : 1.0 - f[0];
+                    num += grids[c * plane + grid_index(ix[0] + dx, ix[1] + dy, ix[2] + dz, n)] * wx * wy * wz;
+                }
+            }
+        }
+        if (c == channels) den = num;
+        else out[v * channels + c] = num;
+    }
+    for (int c = 0; c < channels; ++c) out[v * channels + c] = den > 0.0 ? out[v * channels + c] / den : 0.0;
+}
+
 __global__ void store_count_kernel(const unsigned long long* __restrict__ src, int64_t* __restrict__ dst) {
     *dst = (int64_t)*src;
 }
@@ -391,5 +452,100 @@ extern "C" int pb_splat_f64(const double* points, const double* normals, int64_t
     PB_CHECK_LAUNCH("splat_vector_kernel");
     store_count_kernel<<<1, 1, 0, s>>>(o.accepted, accepted);
     PB_CHECK_LAUNCH("store_count_kernel");
+    return PB_OK;
+}
+
+namespace pb {
+
+struct AttrWork {
+    uint32_t *keys, *keys_alt, *vals, *vals_alt, *flag, *rank, *heads, *head_count;
+    double* weight;
+    unsigned long long* accepted;
+};
+
+static AttrWork attr_carve(Workspace& w, int64_t count) {
+    AttrWork o;
+    const int64_t records = count * 8;
+    o.keys = w.take<uint32_t>(records);
+    o.keys_alt = w.take<uint32_t>(records);
+    o.vals = w.take<uint32_t>(records);
+    o.vals_alt = w.take<uint32_t>(records);
+    o.flag = w.take<uint32_t>(records);
+    o.rank = w.take<uint32_t>(records);
+    o.heads = w.take<uint32_t>(records);
+    o.head_count = w.take<uint32_t>(1);
+    o.weight = w.take<double>(records);
+    o.accepted = w.take<unsigned long long>(1);
+    return o;
+}
+
+static size_t attr_ws_bytes(int64_t count) {
+    return measure([&](Workspace& w) {
+        attr_carve(w, count);
+        radix_carve<uint32_t>(w, count * 8);
+        scan_carve<uint32_t>(w, count * 8);
+    });
+}
+
+}  // namespace pb
+
+extern "C" size_t pb_splat_attributes_workspace_size(int64_t point_count) {
+    return attr_ws_bytes(point_count < 1 ? 1 : point_count);
+}
+
+// Auxiliary attributes of unit-cube samples (points, normals as for
+// pb_splat_f64; attributes: point_count x channels, row-major): grids (channels
+// + 1 planes of n^3, overwritten) get sum w a_c per node and, in the last
+// plane, sum w, with w the samples' pass-1 weights, summed in sample order.
+extern "C" int pb_splat_attributes_f64(const double* points, const double* normals, int64_t point_count, int64_t n,
+                                       int64_t confidence, const double* attributes, int64_t channels,
+                                       double* grids, void* workspace, size_t workspace_bytes, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    if (n < 2 || n * n * n >= (int64_t)0x7FFFFFFF) return fail(PB_ERR_INVALID, "splat attributes: bad n");
+    if (point_count < 0 || point_count * 8 >= (int64_t)0xFFFFFFFFll || channels < 1 || channels > 64 || !grids)
+        return fail(PB_ERR_INVALID, "splat attributes: bad sizes");
+    PB_CHECK_CUDA(cudaMemsetAsync(grids, 0, sizeof(double) * (size_t)(channels + 1) * (size_t)(n * n * n), s),
+                  "splat attributes zero");
+    if (point_count == 0) return PB_OK;
+    if (!points || !normals || !attributes) return fail(PB_ERR_INVALID, "splat attributes: null input");
+    const size_t need = attr_ws_bytes(point_count);
+    if (!workspace || workspace_bytes < need)
+        return fail(PB_ERR_WORKSPACE, "splat attributes: workspace needs %zu bytes", need);
+    Workspace w(workspace, workspace_bytes);
+    AttrWork o = attr_carve(w, point_count);
+    const int64_t records = point_count * 8;
+    const uint32_t sentinel = (uint32_t)(n * n * n);
+    PB_CHECK_CUDA(cudaMemsetAsync(o.accepted, 0, sizeof(unsigned long long), s), "splat attributes accepted");
+    splat_records_kernel<<<blocks_for(records, 256), 256, 0, s>>>(points, normals, point_count, n, (int)confidence,
+                                                                  o.keys, o.vals, o.weight, o.accepted);
+    PB_CHECK_LAUNCH("splat_records_kernel");
+    bool in_alt = false;
+    PB_TRY(radix_sort_pairs<uint32_t>(o.keys, o.vals, o.keys_alt, o.vals_alt, records, bit_width(sentinel), &in_alt,
+                                      w, s));
+    const uint32_t* keys = in_alt ? o.keys_alt : o.keys;
+    const uint32_t* vals = in_alt ? o.vals_alt : o.vals;
+    run_head_flags_kernel<<<blocks_for(records, 256), 256, 0, s>>>(keys, records, sentinel, o.flag);
+    PB_CHECK_LAUNCH("run_head_flags_kernel");
+    PB_TRY(exclusive_scan<uint32_t>(o.flag, o.rank, records, o.head_count, w, s));
+    run_heads_kernel<<<blocks_for(records, 256), 256, 0, s>>>(o.flag, o.rank, records, o.heads);
+    PB_CHECK_LAUNCH("run_heads_kernel");
+    attribute_runs_kernel<<<8 * kSMs, 256, 0, s>>>(keys, vals, o.heads, o.head_count, records, o.weight, attributes,
+                                                   (int)channels, n * n * n, grids);
+    PB_CHECK_LAUNCH("attribute_runs_kernel");
+    return PB_OK;
+}
+
+// Attribute values at mesh vertices (world coordinates; map = the (min x, y, z,
+// width) that took the samples to the unit cube): out (vertex_count x
+// channels) from the grids of pb_splat_attributes_f64.
+extern "C" int pb_sample_attributes_f64(const double* vertices, int64_t vertex_count, const double* map, int64_t n,
+                                        const double* grids, int64_t channels, double* out, void* stream) {
+    if (n < 2 || vertex_count < 0 || channels < 1 || channels > 64 || !map || !grids ||
+        (vertex_count && (!vertices || !out)))
+        return fail(PB_ERR_INVALID, "sample attributes: bad args");
+    if (!vertex_count) return PB_OK;
+    sample_attributes_kernel<<<blocks_for(vertex_count, 256), 256, 0, (cudaStream_t)stream>>>(
+        vertices, vertex_count, map, n, grids, (int)channels, out);
+    PB_CHECK_LAUNCH("sample_attributes_kernel");
     return PB_OK;
 }
