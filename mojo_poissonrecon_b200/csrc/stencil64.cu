@@ -12,14 +12,26 @@ namespace pb {
 // ---- assemble (capi.mojo:228-279) -------------------------------------------
 __global__ void assemble_kernel(const double* __restrict__ vx, const double* __restrict__ vy,
                                 const double* __restrict__ vz, const double* __restrict__ screen,
-                                double* __restrict__ rhs, int64_t n, double point_weight, double target) {
+                                double* __restrict__ rhs, int64_t n, FastDiv dn, double point_weight,
+                                double target) {
     const int64_t total = n * n * n;
+    const bool small = total <= 0xFFFFFFFFll;  // coordinates by 32-bit invariant division
     const double h_inv = (double)(n - 1);
     const double h_inv2 = h_inv * h_inv;
     const double half_h = 0.5 * h_inv;
     for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t x = idx % n, y = (idx / n) % n, z = idx / (n * n);
+        int64_t x, y, z;
+        if (small) {
+            const uint32_t i32 = (uint32_t)idx, row = dn.div(i32), zz = dn.div(row);
+            x = i32 - row * (uint32_t)n;
+            y = row - zz * (uint32_t)n;
+            z = zz;
+        } else {
+            x = idx % n;
+            y = (idx / n) % n;
+            z = idx / (n * n);
+        }
         const int64_t sy = n, sz = n * n;
         double div = 0.0;
         if (x == 0) div += (vx[idx + 1] - vx[idx]) * h_inv;
@@ -237,8 +249,8 @@ extern "C" int pb_assemble_f64(const double* vx, const double* vy, const double*
                                int64_t n, double point_weight, double target_value, void* stream) {
     PB_TRY(check_n(n, "assemble"));
     if (!vx || !vy || !vz || !screen || !rhs) return fail(PB_ERR_INVALID, "assemble: null buffer");
-    assemble_kernel<<<stride_blocks(n * n * n, 256), 256, 0, (cudaStream_t)stream>>>(vx, vy, vz, screen, rhs, n,
-                                                                                     point_weight, target_value);
+    assemble_kernel<<<stride_blocks(n * n * n, 256), 256, 0, (cudaStream_t)stream>>>(
+        vx, vy, vz, screen, rhs, n, FastDiv((uint32_t)n), point_weight, target_value);
     PB_CHECK_LAUNCH("assemble_kernel");
     return PB_OK;
 }
