@@ -81,6 +81,59 @@ def galerkin(A, s, n):
     return ((Ps.T @ A @ Ps) / 8.0).tocsr()
 
 
+def _wt1(d):
+    return 1.0 if d == 0 else (0.5 if abs(d) == 1 else 0.0)
+
+
+def galerkin_separable(A, s, n):
+    """P^T (S A S) P / 8 for a 27-point A contracted one axis at a time (x, then
+    y, then z), as csrc/mg27.cu's galerkin_x/y/z kernels do: each stage maps
+    fine positions 2M + a and offsets d to coarse offsets m with weights
+    P(a) P(a + d - 2m), keeping the other two axes' offsets.  Returns the
+    coarse operator's 14 planes (plane 0 the diagonal)."""
+    cn = (n + 1) // 2
+    st = np.zeros((n, n, n, 3, 3, 3))  # st[z, y, x, dz+1, dy+1, dx+1] = s_i a_ij s_j
+    coo = A.tocoo()
+    z, y, x = coords(n)
+    for i, j, a in zip(coo.row, coo.col, coo.data):
+        d = (z[j] - z[i], y[j] - y[i], x[j] - x[i])
+        if max(abs(v) for v in d) <= 1:
+            st[z[i], y[i], x[i], d[0] + 1, d[1] + 1, d[2] + 1] = s[i] * a * s[j]
+    b1 = np.zeros((n, n, cn, 3, 3, 3))  # [z, y, I, dz, dy, m]
+    for a in (-1, 0, 1):
+        xi = 2 * np.arange(cn) + a
+        ok = (xi >= 0) & (xi < n)
+        for dx in (-1, 0, 1):
+            for m in (-1, 0, 1):
+                w = _wt1(a) * _wt1(a + dx - 2 * m)
+                if w:
+                    b1[:, :, ok, :, :, m + 1] += w * st[:, :, xi[ok], :, :, dx + 1]
+    b2 = np.zeros((n, cn, cn, 3, 3, 3))  # [z, J, I, dz, my, m]
+    for b in (-1, 0, 1):
+        yj = 2 * np.arange(cn) + b
+        ok = (yj >= 0) & (yj < n)
+        for dy in (-1, 0, 1):
+            for my in (-1, 0, 1):
+                w = _wt1(b) * _wt1(b + dy - 2 * my)
+                if w:
+                    b2[:, ok, :, :, my + 1, :] += w * b1[:, yj[ok], :, :, dy + 1, :]
+    c = np.zeros((cn, cn, cn, 3, 3, 3))  # [K, J, I, mz, my, m]
+    for cc in (-1, 0, 1):
+        zf = 2 * np.arange(cn) + cc
+        ok = (zf >= 0) & (zf < n)
+        for dz in (-1, 0, 1):
+            for mz in (-1, 0, 1):
+                w = _wt1(cc) * _wt1(cc + dz - 2 * mz)
+                if w:
+                    c[ok, :, :, mz + 1, :, :] += w * b2[zf[ok], :, :, dz + 1, :, :]
+    c /= 8.0
+    out = np.zeros((14, cn, cn, cn))
+    out[0] = c[..., 1, 1, 1]
+    for (kx, ky, kz) in forward_offsets():
+        out[fwd_index(kx, ky, kz)] = c[..., kz + 1, ky + 1, kx + 1]
+    return out
+
+
 def planes(A, n):
     """14 dense (n, n, n) planes: the diagonal, then a(J, J+K) for forward K."""
     out = np.zeros((14, n, n, n))

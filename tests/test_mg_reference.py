@@ -29,6 +29,29 @@ def test_planes_round_trip():
         assert s.min() >= 0.0 and s.max() <= 1.0
 
 
+@pytest.mark.parametrize("n", [9, 17])
+def test_separable_galerkin_equals_direct_product(n):
+    """The x, y, z stages of the 27-point Galerkin product (as the GPU runs
+    them) equal the direct sparse product P_s^T A P_s / 8, boundary rows
+    included, for a realistic 27-point level (the Galerkin level below a
+    7-point one with shell screening) and for a random symmetric one."""
+    rng = np.random.default_rng(n)
+    fine = 2 * n - 1
+    screen = rng.random((fine, fine, fine)) * (rng.random((fine, fine, fine)) < 0.2) * 50.0
+    ops, ws, sizes = mg.hierarchy(screen, 4.0)
+    A, s = ops[1], ws[1]
+    assert sizes[1] == n
+    cn = (n + 1) // 2
+    want = mg.planes(mg.galerkin(A, s, n), cn)
+    got = mg.galerkin_separable(A, s, n)
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+    R = mg.from_planes(rng.normal(size=(14, n, n, n)) * (np.arange(14) > 0)[:, None, None, None], n)
+    R = R + R.T
+    s2 = rng.random(n ** 3)
+    want = mg.planes(mg.galerkin(R, s2, n), cn)
+    assert np.abs(mg.galerkin_separable(R, s2, n) - want).max() <= 1e-12 * np.abs(want).max()
+
+
 def _reference_factors(oracle, screen, rhs, cycles):
     """Residual ratios of the reference's rediscretised V(3,3) cycle (oracle)."""
     L = oracle.lib()
