@@ -20,9 +20,15 @@
 // streams, no ordering between them) race on the array and may return wrong
 // counts: order such calls on one stream or synchronise between them.
 //
-// The first call on each device looks up the array's device address with
-// cudaGetSymbolAddress while that device is current; make that first call
-// before any stream capture.
+// The first call on each device (and CUDA context) looks up the array's device
+// address with cudaGetSymbolAddress while that device is current; make that
+// first call before any stream capture.  The address is cached per (device,
+// context): a call made under another context of the same device (one the
+// caller created and made current with the driver API) looks it up again for
+// that context.  cudaDeviceReset unloads the library's device memory; do not
+// call this entry point on a device after resetting it in the same process.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "common.cuh"
@@ -84,20 +90,48 @@ __global__ void __launch_bounds__(kThreads) sum_tiles_kernel(const long long* __
     }
 }
 
-// Device address of g_tile_counts on the current device, looked up once per device.
+typedef CUresult (*CtxGetCurrent)(CUcontext*);
+
+// The driver's cuCtxGetCurrent, fetched through the runtime (the library does
+// not link libcuda directly).
+static CtxGetCurrent ctx_get_current() {
+    static CtxGetCurrent fn = [] {
+        void* ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            return reinterpret_cast<CtxGetCurrent>(ptr);
+        return (CtxGetCurrent) nullptr;
+    }();
+    return fn;
+}
+
+// Device address of g_tile_counts on the current device, looked up once per
+// device and context.  A thread with no current context gets the device's
+// primary context from the runtime's first symbol lookup.
 static int scratch_address(long long** out) {
     static std::mutex mu;
     static long long* addresses[kMaxDevices] = {};
+    static CUcontext contexts[kMaxDevices] = {};
     int dev = 0;
     PB_CHECK_CUDA(cudaGetDevice(&dev), "dual count (no alloc): cudaGetDevice");
     if (dev < 0 || dev >= kMaxDevices) return fail(PB_ERR_DEVICE, "dual count (no alloc): device index %d", dev);
+    CtxGetCurrent get = ctx_get_current();
+    if (!get) return fail(PB_ERR_CUDA, "dual count (no alloc): cuCtxGetCurrent is unavailable");
     std::lock_guard<std::mutex> lock(mu);
-    if (!addresses[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_tile_counts);
-        if (e != cudaSuccess || !p) return cuda_fail(e, "dual count (no alloc): cudaGetSymbolAddress");
-        addresses[dev] = static_cast<long long*>(p);
+    CUcontext ctx = nullptr;
+    if (get(&ctx) != CUDA_SUCCESS) return fail(PB_ERR_CUDA, "dual count (no alloc): cuCtxGetCurrent failed");
+    if (ctx && addresses[dev] && contexts[dev] == ctx) {
+        *out = addresses[dev];
+        return PB_OK;
     }
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_tile_counts);
+    if (e != cudaSuccess || !p) return cuda_fail(e, "dual count (no alloc): cudaGetSymbolAddress");
+    if (!ctx && (get(&ctx) != CUDA_SUCCESS || !ctx))
+        return fail(PB_ERR_CUDA, "dual count (no alloc): no current context after the symbol lookup");
+    addresses[dev] = static_cast<long long*>(p);
+    contexts[dev] = ctx;
     *out = addresses[dev];
     return PB_OK;
 }
@@ -112,9 +146,15 @@ extern "C" int pb_dual_vertex_count_f64_noalloc(const double* field, int64_t n, 
     using namespace pb::noalloc;
     if (!field || !count) return fail(PB_ERR_INVALID, "dual count (no alloc): null buffer");
     if (n < 2) return fail(PB_ERR_INVALID, "dual count (no alloc): n must be >= 2 (got %lld)", (long long)n);
+    // n is bounded before the cell count is formed, so the product cannot overflow.
+    if (n > 4097)
+        return fail(PB_ERR_INVALID,
+                    "dual count (no alloc): n = %lld exceeds the fixed scratch (n <= 513); use "
+                    "pb_dual_vertices_f64 with a workspace for larger grids",
+                    (long long)n);
     const int64_t cells = n - 1;
     const int64_t tiles = (cells * cells * cells + kTile - 1) / kTile;
-    if (n > 4097 || tiles > kMaxTiles)
+    if (tiles > kMaxTiles)
         return fail(PB_ERR_INVALID,
                     "dual count (no alloc): n = %lld needs %lld tile slots but the fixed scratch holds %lld "
                     "(n <= 513); use pb_dual_vertices_f64 with a workspace for larger grids",

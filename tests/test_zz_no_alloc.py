@@ -66,7 +66,10 @@ def test_noalloc_count_equals_workspace_count_on_consecutive_calls(L):
 def test_noalloc_count_rejects_grids_beyond_its_scratch(L):
     field = torch.zeros(8, dtype=torch.float64, device="cuda")  # never read: rejected before launch
     count = torch.zeros(1, dtype=torch.int64, device="cuda")
-    status = L.pb_dual_vertex_count_f64_noalloc(field.data_ptr(), 1025, 0.0, count.data_ptr(),
-                                                torch.cuda.current_stream().cuda_stream)
-    assert status == 1
-    assert "n <= 513" in L.pb_last_error().decode()
+    # 514 is the first side past the limit (65,918 tiles of 2048 cells against 65,536
+    # slots); 1025 and 1 << 40 are far past it (the latter would overflow n^3).
+    for n in (514, 1025, 1 << 40):
+        status = L.pb_dual_vertex_count_f64_noalloc(field.data_ptr(), n, 0.0, count.data_ptr(),
+                                                    torch.cuda.current_stream().cuda_stream)
+        assert status == 1, n
+        assert "n <= 513" in L.pb_last_error().decode(), n
