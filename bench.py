@@ -65,6 +65,8 @@ def parse_args():
     ap.add_argument("--workload", choices=("torus", "batch", "serving", "deep"), default="torus",
                     help="torus: the default line; batch: 256 uneven clouds; serving: Poisson arrivals; "
                          "deep: depth 10")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the autotuner (built-in launch shapes); by default it runs before the warm-up")
     ap.add_argument("--lanes", type=int, default=4)
     ap.add_argument("--duration", type=float, default=10.0, help="serving: seconds of arrivals")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
@@ -155,6 +157,13 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     dev_p, dev_n = host_p.to(dev), host_n.to(dev)
     common = dict(depth=args.depth, confidence=True, point_weight=4.0, tol=TOL)
     lib = _native.lib()
+    tuning = None
+    if not args.no_tune:  # before any engine captures its launch shapes
+        from mojo_poissonrecon_b200 import tune
+
+        found = tune.autotune((1 << args.depth) + 1, device=dev, write=False)
+        tuning = {k: {"chosen": v["best"], "default_us": round(v["default_s"] * 1e6, 1),
+                      "tuned_us": round(v["best_s"] * 1e6, 1)} for k, v in found.items()}
 
     def barrier():
         if dist is not None:
@@ -333,6 +342,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         "kernels": kernel_table,
         "gpu_launches": int(launches),
         "clocks": clock_info,
+        "tuning": tuning,
     }
     return result
 
@@ -412,25 +422,36 @@ def read_profile_traffic(path):
 
 # ---- CPU baselines (the oracle: test infrastructure, timed only here) -------------
 
-def cpu_sample(pts, nrm, depth: int, threaded: bool, full: bool):
-    """Seconds per reconstruction of the workload on the host.  full=False times
-    the set-up and 3 V-cycles and extrapolates to the cycle count the FP64
-    solve needs (the cycle count comes from a GPU or earlier CPU run)."""
+def cpu_sample(pts, nrm, depth: int, threaded: bool, full: bool, cycles: int | None = None,
+               budget_s: float = 60.0):
+    """Seconds per reconstruction of the workload on the host, and how they were
+    taken.  full=True times one whole reconstruction.  full=False first times
+    the set-up with 1 and with 3 V-cycles; if set-up + `cycles` V-cycles +
+    extraction fits `budget_s` it then times the whole reconstruction,
+    otherwise it extrapolates to `cycles` V-cycles (the count the FP64 GPU
+    solve, which is bit-identical to the oracle cycle for cycle, needed to
+    reach the tolerance)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pipeline as oracle
 
     if not os.path.exists(os.path.join(ROOT, "oracle", "liboracle_mpr.so")):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-s"], check=True)
-    keep = oracle.valid_rows(pts, nrm)
-    t0 = time.perf_counter()
+
+    def whole():
+        t0 = time.perf_counter()
+        mesh = oracle.reconstruct(pts, nrm, depth=depth, confidence=True, point_weight=4.0, tol=TOL, max_cycles=200,
+                                  threaded=threaded, octree=False)
+        return time.perf_counter() - t0, mesh
+
     if full:
-        oracle.reconstruct(pts, nrm, depth=depth, confidence=True, point_weight=4.0, tol=TOL, max_cycles=200,
-                           threaded=threaded, octree=False)
-        return time.perf_counter() - t0, "full reconstruction"
+        dt, _ = whole()
+        return dt, "full reconstruction"
+    t0 = time.perf_counter()
+    keep = oracle.valid_rows(pts, nrm)
     unit, _, _ = oracle.normalize(pts[keep], 1.1)
     t_a = time.perf_counter()
-    sol = oracle.solve(unit, nrm[keep], depth=depth, confidence=True, point_weight=4.0, cycles=1,
-                       threaded=threaded, octree=False)
+    oracle.solve(unit, nrm[keep], depth=depth, confidence=True, point_weight=4.0, cycles=1, threaded=threaded,
+                 octree=False)
     t_b = time.perf_counter()
     sol3 = oracle.solve(unit, nrm[keep], depth=depth, confidence=True, point_weight=4.0, cycles=3,
                         threaded=threaded, octree=False)
@@ -440,9 +461,14 @@ def cpu_sample(pts, nrm, depth: int, threaded: bool, full: bool):
     t_d = time.perf_counter()
     oracle.extract(sol3.field, sol3.iso_value, sol3.density, threaded)
     extract_s = time.perf_counter() - t_d
-    cycles = 31  # V-cycles the FP64 solve of this workload needs to reach 1e-8 (measured)
-    total = (t_a - t0) + setup + cycles * per_cycle + extract_s
-    return total, f"set-up + 1 and 3 V-cycles timed, extrapolated to {cycles} cycles + extraction"
+    if cycles is None:
+        raise ValueError("cpu_sample needs the cycle count to extrapolate")
+    estimate = (t_a - t0) + setup + cycles * per_cycle + extract_s
+    if estimate <= budget_s:
+        dt, _ = whole()
+        return dt, f"full reconstruction (set-up + V-cycles to rel-res {TOL:g} + extraction, timed whole)"
+    return estimate, (f"set-up + 1 and 3 V-cycles timed, extrapolated to the {cycles} V-cycles the bit-identical "
+                      f"FP64 solve needs for rel-res {TOL:g}, + extraction")
 
 
 def run_reference(args) -> dict:
@@ -453,23 +479,21 @@ def run_reference(args) -> dict:
     pts, nrm = workload(args.points)
     threads = int(oracle.lib(True).mpr_oracle_threads())
     first, how = cpu_sample(pts, nrm, args.depth, True, True)
+    # every step is a whole reconstruction; the warm-up and step counts are cut
+    # to what fits a few minutes (the first timing counts as a warm-up)
     budget = 180.0
-    full = first * (args.steps + args.warmup) <= budget
-    times = []
-    for k in range(args.warmup + args.steps):
-        if k == 0:
-            dt = first
-        else:
-            dt, how = cpu_sample(pts, nrm, args.depth, True, full)
-        if k >= args.warmup:
+    runs = max(1, min(args.warmup + args.steps, int(budget // max(first, 1e-3))))
+    warm = min(args.warmup, runs - 1)
+    times = [first] if warm == 0 else []
+    for k in range(1, runs):
+        dt, how = cpu_sample(pts, nrm, args.depth, True, True)
+        if k >= warm:
             times.append(dt)
-        if not full and k >= args.warmup:
-            break
-    per = statistics.mean(times) if times else first
+    per = statistics.mean(times)
     value = 1.0 / per
     return {
         "metric": METRIC, "impl": "reference", "value": round(value, 5), "unit": "recons/s", "n_gpus": args.gpus,
-        "steps": len(times), "warmup": args.warmup, "ms_per_step": round(per * 1e3, 1), "higher_is_better": True,
+        "steps": len(times), "warmup": warm, "ms_per_step": round(per * 1e3, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (same seeded torus)",
         "config": {"workload": WORKLOAD, "points": args.points, "depth": args.depth, "precision": "fp64", "tol": TOL},
         "cpu_baseline": {"value": round(value, 5), "unit": "recons/s", "cores": threads, "kind": "port",
@@ -500,32 +524,47 @@ def warm_lanes(lanes: int, depths, cloud) -> None:
 
 def run_batch(args) -> dict:
     """256 clouds, sizes log-uniform 1k-200k, depths uniform in {5,6,7,8},
-    random ellipsoids and tori; all submitted at once to a Server."""
+    random ellipsoids and tori.  value: batch.reconstruct_many (one grouped
+    launch per solver step across the clouds, host arrays in, meshes out),
+    timed with CUDA events around whole calls after a warm-up call; beside it
+    the same clouds through a 4-lane Server (one reconstruction per lane)."""
     import torch
 
-    from mojo_poissonrecon_b200 import serve, workloads
+    from mojo_poissonrecon_b200 import batch, serve, workloads
 
     clouds = workloads.batch_clouds(256, seed=3)
     total_points = sum(len(p) for p, _, _ in clouds)
-    warm_lanes(args.lanes, sorted({d for _, _, d in clouds}), clouds[0][:2])
-    serve.reconstruct_batch(clouds[:8], lanes=args.lanes)
-    results = {}
-    for lanes in (1, args.lanes):
+    batch.reconstruct_many(clouds[:16], tol=TOL)  # loads the modules, sets kernel attributes
+    times = []
+    meshes = None
+    for k in range(max(1, args.warmup) + max(1, args.steps)):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        meshes = batch.reconstruct_many(clouds, tol=TOL)
+        e1.record()
+        torch.cuda.synchronize()
+        if k >= max(1, args.warmup):
+            times.append(e0.elapsed_time(e1) / 1e3)
+    per = statistics.median(times)
+    lanes = {}
+    if args.lanes > 0:
+        warm_lanes(args.lanes, sorted({d for _, _, d in clouds}), clouds[0][:2])
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        with serve.Server(lanes=lanes) as server:
+        with serve.Server(lanes=args.lanes) as server:
             futures = [server.submit(p, n, depth=d) for p, n, d in clouds]
             out = [f.result() for f in futures]
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
-        service = [t.service_ms for _, t in out]
-        results[lanes] = {"recons_per_s": round(len(clouds) / wall, 2), "wall_s": round(wall, 3),
-                          "service_p50_ms": round(statistics.median(service), 3),
-                          "service_p99_ms": round(float(np.percentile(service, 99)), 3)}
-    best = results[args.lanes]
+        lanes = {"lanes": args.lanes, "recons_per_s": round(len(clouds) / wall, 2), "wall_s": round(wall, 3),
+                 "service_p99_ms": round(float(np.percentile([t.service_ms for _, t in out], 99)), 3)}
     return {"metric": METRIC, "workload": "batch: 256 uneven clouds (1k-200k points, depths 5-8, ellipsoids/tori)",
-            "value": best["recons_per_s"], "unit": "recons/s", "n_gpus": 1, "precision": "fp32_refined",
-            "tol": TOL, "points_total": total_points, "lanes": args.lanes, "by_lanes": results,
+            "value": round(len(clouds) / per, 2), "unit": "recons/s", "n_gpus": 1, "precision": "fp32_refined",
+            "tol": TOL, "points_total": total_points, "ms_per_batch": round(per * 1e3, 1),
+            "batches_timed": len(times), "timing": "CUDA events around each reconstruct_many call (host arrays in, "
+                                                  "host meshes out), median", "faces_total":
+                int(sum(m.faces.shape[0] for m in meshes)), "server_lanes": lanes,
             "data": "synthetic (workloads.batch_clouds, seed 3)"}
 
 
@@ -670,7 +709,8 @@ def main():
         if rank == 0 and result is not None:
             if world == 1 and not args.no_cpu_baseline and not args.profile:
                 pts, nrm = workload(args.points)
-                per, how = cpu_sample(pts, nrm, args.depth, False, False)
+                per, how = cpu_sample(pts, nrm, args.depth, False, False,
+                                      cycles=result["accuracy"].get("fp64_cycles"))
                 result["cpu_baseline"] = {"value": round(1.0 / per, 5), "unit": "recons/s", "cores": 1,
                                           "kind": "port",
                                           "sample": how + " (serial oracle/mpr_oracle.c, the reference's "
