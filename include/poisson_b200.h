@@ -173,8 +173,9 @@ int pb_dual_vertices_f64_isoptr(const double *field, const double *density, int6
  * the reference: its count mode writes into the caller's scratch buffer.
  * Scratch is a fixed 512 KiB array in the library's device memory, so
  * n <= 513; larger grids get PB_ERR_INVALID.  The first call on a device
- * looks the array up (make it before any stream capture); calls that overlap
- * on the GPU share the array and race. */
+ * (and on each further context of it) looks the array up: make it before any
+ * stream capture.  Calls that overlap on the GPU share the array and race.
+ * Do not call it on a device after cudaDeviceReset in the same process. */
 int pb_dual_vertex_count_f64_noalloc(const double *field, int64_t n, double iso, int64_t *count,
                                      void *stream);
 
@@ -342,6 +343,102 @@ int pb_coarse27_image_f32(int64_t count, const int64_t *sizes, const float *cons
  * correction. */
 int pb_coarse27_cycle_f32(int64_t count, const int64_t *sizes, const float *image, const float *rhs, float *e,
                           int64_t pre, int64_t post, int64_t inner, void *stream);
+
+/* ---- batches of clouds: one grouped launch per solver step ------------------
+ * No counterpart in the reference, which solves one cloud at a time and level
+ * by level (core.py:141-193, driven per cycle at :270-287).  A grouped launch
+ * runs one step of the FP32 V-cycle or of FCG(1) over many (cloud, level)
+ * grids of any side at once.  The caller describes the grids once:
+ * pb_batch_describe writes `count` descriptors (pb_batch_desc_bytes(count)
+ * bytes, 64-byte aligned, host memory) from, per grid, its cloud index, side,
+ * PB_BATCH_PTRS operand pointers (kind-specific order below, unused slots
+ * NULL) and 4 kind-specific integers (aux, may be NULL: zeros), and reports
+ * the launch's total blocks.  The caller copies the descriptors to device
+ * memory it owns (64-byte aligned) and pb_batch_launch queues the step over
+ * them as often as needed, inside a captured graph too.
+ *
+ * Per-cloud state, indexed by the cloud index: flags int[4] (first step,
+ * iterations done, active, unused), scalars double[8] (as pb_fcg_*), loop
+ * control double[2] (target ||r||^2, iteration cap).  Every block of a cloud
+ * whose active flag is 0 returns at once, so converged clouds stay as they
+ * are while the others iterate.
+ *
+ * Operands per kind (p = padded FP32 level arrays, d = dense):
+ *   SWEEP / SWEEP_ZERO     e_in (ignored from zero), e_out, rhs, 1/D, status word;
+ *                          z_chunk <= 0: whole planes per block (sides 2^k + 1 >= 33)
+ *   PROLONG32              coarse, fine, weights               (pb_prolong_fac_f32)
+ *   RESIDUAL_RESTRICT32    e, rhs, D, weights, coarse rhs      (pb_residual_restrict_f32)
+ *   RELAX27P / _ZERO       e_prev, e_next, rhs, h0, h1, inv0, inv1   (pb_relax27p_f32)
+ *   RESIDUAL27P            e, rhs, h0, h1, inv0, inv1, weights, res
+ *   RESTRICT27             fine res, coarse rhs (side = the fine side)
+ *   COARSE27               image, rhs, e; aux = pre, post, inner; one block per
+ *                          grid, every grid of the launch of the same first side
+ *                          (pass it as first_side to pb_batch_launch)
+ *   FCG_DIRECTION          z, p0, p1, r32, screen (d), partials; aux[0] = point
+ *                          weight as the bits of a double
+ *   FCG_DIRECTION_FINISH   partials, the cloud's scalars; aux[0] = the cloud's
+ *                          pb_batch_fcg_blocks(n, 0)
+ *   FCG_UPDATE             z, p0, p1, x0, x1, b, screen, r32, the cloud's scalars,
+ *                          partials; aux[0] = point weight bits
+ *   FCG_SUM                partials, the cloud's scalars + 4; aux[0] =
+ *                          pb_batch_fcg_blocks(n, 1)
+ * Partials: pb_batch_fcg_partials(n) doubles per cloud. */
+enum {
+    PB_BATCH_SWEEP = 0,
+    PB_BATCH_SWEEP_ZERO = 1,
+    PB_BATCH_PROLONG32 = 2,
+    PB_BATCH_RESIDUAL_RESTRICT32 = 3,
+    PB_BATCH_RELAX27P = 4,
+    PB_BATCH_RELAX27P_ZERO = 5,
+    PB_BATCH_RESIDUAL27P = 6,
+    PB_BATCH_RESTRICT27 = 7,
+    PB_BATCH_COARSE27 = 8,
+    PB_BATCH_FCG_DIRECTION = 9,
+    PB_BATCH_FCG_DIRECTION_FINISH = 10,
+    PB_BATCH_FCG_UPDATE = 11,
+    PB_BATCH_FCG_SUM = 12,
+    PB_BATCH_PTRS = 12
+};
+size_t pb_batch_desc_bytes(int64_t count);
+int64_t pb_batch_fcg_partials(int64_t n);
+int64_t pb_batch_fcg_blocks(int64_t n, int64_t pass);
+int pb_batch_describe(int kind, int64_t count, const int64_t *clouds, const int64_t *sides,
+                      const void *const *ptrs, const int64_t *aux, int64_t z_chunk, void *desc_host,
+                      size_t desc_bytes, int64_t *blocks);
+int pb_batch_launch(int kind, const void *desc_device, int64_t count, int64_t blocks, const int *flags,
+                    int64_t first_side, void *stream);
+/* End of one batch iteration (the last launch of a captured WHILE body, as
+ * pb_loop_condition for one cloud): for every active cloud, count the
+ * iteration, clear its first-step flag, record scal[4] in
+ * history[cloud*max_iter + iteration-1] (history may be NULL) and keep it
+ * active while scal[4] > ctrl[0] and fewer than min(max_iter, ctrl[1])
+ * iterations ran; the loop continues while any cloud is active. */
+int pb_batch_loop_condition(unsigned long long handle, const double *scal, const double *ctrl, int *flags,
+                            int64_t clouds, int64_t max_iter, double *history, void *stream);
+
+/* ---- launch parameters chosen by an autotuner (no counterpart in the reference,
+ * whose launch shape is the fixed GRID_Z_CHUNK / PARALLEL_GRID_THRESHOLD of
+ * capi.mojo:9-10) ----------------------------------------------------------------
+ * A host-side table per (parameter, grid side n); a launcher reads it when it
+ * chooses its launch shape and uses its built-in choice where no value is set.
+ *   SWEEP_Z_CHUNK          planes per block of pb_sweep_tma_f32 when its z_chunk <= 0
+ *   RESTRICT_PLANES        coarse planes per block of pb_residual_restrict_f32 (default 4)
+ *   PROLONG_PLANES         fine planes per block of pb_prolong_fac_f32
+ *   FCG_DIRECTION_PLANES   planes per block of pb_fcg_direction_f64 (default 24, at least 8)
+ *   FCG_UPDATE_PLANES      planes per block of pb_fcg_update_f64 (default 24, at least 8)
+ * The same values apply to the grouped launches described after they are set.
+ * value 0 clears an entry.  Results do not depend on these values. */
+enum {
+    PB_TUNE_SWEEP_Z_CHUNK = 0,
+    PB_TUNE_RESTRICT_PLANES = 1,
+    PB_TUNE_PROLONG_PLANES = 2,
+    PB_TUNE_FCG_DIRECTION_PLANES = 3,
+    PB_TUNE_FCG_UPDATE_PLANES = 4,
+    PB_TUNE_PARAMS = 5
+};
+int pb_tune_set(int64_t param, int64_t n, int64_t value);
+int64_t pb_tune_get(int64_t param, int64_t n);
+int pb_tune_clear(void);
 
 /* ---- host-orchestration helpers (core.py steps done on the device) ---------- */
 

@@ -92,6 +92,15 @@ _SIGNATURES = {
     "pb_coarse27_image_size": ([I, P], S),
     "pb_coarse27_image_f32": ([I, P, P, P, P, P, P, S, P], C),
     "pb_coarse27_cycle_f32": ([I, P, P, P, P, I, I, I, P], C),
+    "pb_batch_desc_bytes": ([I], S),
+    "pb_batch_fcg_partials": ([I], I),
+    "pb_batch_fcg_blocks": ([I, I], I),
+    "pb_batch_describe": ([C, I, P, P, P, P, I, P, S, P], C),
+    "pb_batch_launch": ([C, P, I, I, P, I, P], C),
+    "pb_batch_loop_condition": ([ctypes.c_ulonglong, P, P, P, I, I, P, P], C),
+    "pb_tune_set": ([I, I, I], C),
+    "pb_tune_get": ([I, I], I),
+    "pb_tune_clear": ([], C),
 }
 
 LIBRARY_PATH = _build.LIBRARY

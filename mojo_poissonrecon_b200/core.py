@@ -20,7 +20,7 @@ import numpy as np
 import torch
 
 from . import _native as nat
-from . import solver
+from . import _sync, solver
 from ._convert import f64, i64
 
 MAX_DEPTH = 10
@@ -145,6 +145,7 @@ def _host_all(tensors, device_out: bool) -> list:
             out.append(h)
         else:
             out.append(t.cpu())
+    _sync.wait("result copies")
     torch.cuda.current_stream().synchronize()
     return [h.numpy() for h in out]
 
@@ -161,6 +162,7 @@ def _prepare(ctx: _Context, points: torch.Tensor, normals: torch.Tensor, scale: 
     ctx.check(ctx.lib.pb_prepare_points_f64(points.data_ptr(), normals.data_ptr(), count, scale, out_p.data_ptr(),
                                             out_n.data_ptr(), kept.data_ptr(), fmap.data_ptr(), ptr, size,
                                             ctx.stream), "prepare points")
+    _sync.wait("prepare points")
     k = int(kept.item())
     return out_p[:k], out_n[:k], k, fmap
 
@@ -340,6 +342,7 @@ def _extract_device(ctx: _Context, field: torch.Tensor, density: torch.Tensor, i
         counts = torch.empty(2, dtype=torch.int64, device=ctx.device)
         ctx.check(L.pb_extract_count_f64(field.data_ptr(), n, iso.data_ptr(), counts.data_ptr(), ptr, size,
                                          ctx.stream), "extract count")
+        _sync.wait("extract count")
         nv, nf = (int(v) for v in counts.cpu())
         vertices = torch.empty((nv, 3), dtype=torch.float64, device=ctx.device)
         vdens = torch.empty(nv, dtype=torch.float64, device=ctx.device)

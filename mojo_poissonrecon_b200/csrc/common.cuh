@@ -17,6 +17,10 @@ int cuda_fail(cudaError_t err, const char* where);
 // Counts every kernel this library launches (read by pb_launch_count()).
 void count_launch();
 
+// The autotuned value of a launch parameter (PB_TUNE_*) for grid side n, or
+// `fallback` when none is set (pb_tune_set).
+int64_t tuned(int param, int64_t n, int64_t fallback);
+
 #define PB_CHECK_LAUNCH(where)                                   \
     do {                                                         \
         ::pb::count_launch();                                    \

@@ -26,12 +26,16 @@
 // direction, and the residual is recomputed from x in FP64 every iteration,
 // so the rounding perturbs alpha and beta by ~1e-7 relative and never the
 // measured residual.
+#include "batch.cuh"
 #include "common.cuh"
 
 namespace pb {
 namespace fcg {
 
-constexpr int kTZ = 24, kThreads = 256;  // pass 1: 256 (x, y) columns per block; both passes 24 planes deep (measured: 16 -> 24, pass 1 82 -> 78 us)
+// pass 1: 256 (x, y) columns per block; both passes kTZ planes deep unless the
+// autotuner chose otherwise (measured: 16 -> 24, pass 1 82 -> 78 us).  Partial
+// sums are sized for the shallowest depth a launch may use, kMinTZ.
+constexpr int kTZ = 24, kMinTZ = 8, kThreads = 256;
 
 // Pass 2 tile: 32 x 8 nodes per block, kTZ planes deep.
 constexpr int kUX = 32, kUY = 8, kUThreads = kUX * kUY;
@@ -80,18 +84,16 @@ __device__ __forceinline__ int64_t block_index() {
 // registers; the ghosts of the padded z are zero, so the 6-neighbour sum needs
 // no tests.  Compiled for 4 resident blocks per SM (64 registers), which keeps
 // more loads in flight than the occupancy-first default.
-__global__ void __launch_bounds__(kThreads, 4) direction_sums_kernel(const float* __restrict__ z, Pad g,
-                                                                     const float* __restrict__ p0,
-                                                                     const float* __restrict__ p1,
-                                                                     const float* __restrict__ r32,
-                                                                     const double* __restrict__ screen, double pw,
-                                                                     const int* __restrict__ flags,
-                                                                     double* __restrict__ part) {
+__device__ __forceinline__ void direction_sums_body(const float* __restrict__ z, Pad g, const float* __restrict__ p0,
+                                                    const float* __restrict__ p1, const float* __restrict__ r32,
+                                                    const double* __restrict__ screen, double pw,
+                                                    const int* __restrict__ flags, double* __restrict__ part, int tz,
+                                                    int bx, int by, int64_t block) {
     __shared__ double shared[4][32];
     const int n = g.n;
-    const unsigned t = blockIdx.x * kThreads + threadIdx.x;  // flattened over the plane's (x, y): full warps
+    const unsigned t = bx * kThreads + threadIdx.x;  // flattened over the plane's (x, y): full warps
     const int y = t < (unsigned)(n * n) ? (int)(t / (unsigned)n) : n, x = (int)(t - (unsigned)y * n);
-    const int z0 = blockIdx.y * kTZ, z1 = min(n, z0 + kTZ);
+    const int z0 = by * tz, z1 = min(n, z0 + tz);
     const double h = (double)(n - 1), h2 = h * h;
     const bool first = flags[0] != 0;
     const float* __restrict__ pp = (flags[1] & 1) ? p1 : p0;
@@ -123,14 +125,24 @@ __global__ void __launch_bounds__(kThreads, 4) direction_sums_kernel(const float
     block_sums<4>(v, shared);
     if (lin_tid() == 0)
 #pragma unroll
-        for (int k = 0; k < 4; ++k) part[4 * block_index() + k] = v[k];
+        for (int k = 0; k < 4; ++k) part[4 * block + k] = v[k];
+}
+
+__global__ void __launch_bounds__(kThreads, 4) direction_sums_kernel(const float* __restrict__ z, Pad g,
+                                                                     const float* __restrict__ p0,
+                                                                     const float* __restrict__ p1,
+                                                                     const float* __restrict__ r32,
+                                                                     const double* __restrict__ screen, double pw,
+                                                                     const int* __restrict__ flags,
+                                                                     double* __restrict__ part, int tz) {
+    direction_sums_body(z, g, p0, p1, r32, screen, pw, flags, part, tz, blockIdx.x, blockIdx.y, block_index());
 }
 
 // Sums pass 1's partials (fixed order) and forms the step's scalars:
 //   scal[0] (p, Ap) (the previous direction's on entry)   scal[1] beta
 //   scal[2] alpha   scal[3] (p, r)
-__global__ void direction_finish_kernel(const double* __restrict__ part, int blocks, const int* __restrict__ flags,
-                                        double* __restrict__ scal) {
+__device__ __forceinline__ void direction_finish_body(const double* __restrict__ part, int blocks,
+                                                      const int* __restrict__ flags, double* __restrict__ scal) {
     __shared__ double shared[4][32];
     double v[4] = {0.0, 0.0, 0.0, 0.0};
     for (int b = threadIdx.x; b < blocks; b += blockDim.x)
@@ -148,6 +160,11 @@ __global__ void direction_finish_kernel(const double* __restrict__ part, int blo
     scal[1] = beta;
     scal[2] = pap > 0.0 ? prn / pap : 0.0;
     scal[3] = prn;
+}
+
+__global__ void direction_finish_kernel(const double* __restrict__ part, int blocks, const int* __restrict__ flags,
+                                        double* __restrict__ scal) {
+    direction_finish_body(part, blocks, flags, scal);
 }
 
 // Halo node of thread tid for a tile at (bx, by): rows by - 1 and by + kUY,
@@ -185,17 +202,19 @@ struct Halo {
 // registers (about 7 global loads per node instead of 23 with every neighbour
 // formed from memory).  Nodes outside the domain hold 0 and
 // the neighbour sum adds x-, x+, y-, y+, z-, z+ in that order.
-__global__ void __launch_bounds__(kUThreads) update_residual_kernel(
-    const float* __restrict__ z, Pad g, float* p0, float* p1, double* x0, double* x1, const double* __restrict__ b,
-    const double* __restrict__ screen, double pw, const double* __restrict__ scal, const int* __restrict__ flags,
-    float* __restrict__ r32, double* __restrict__ part) {
+__device__ __forceinline__ void update_residual_body(const float* __restrict__ z, Pad g, float* p0, float* p1,
+                                                     double* x0, double* x1, const double* __restrict__ b,
+                                                     const double* __restrict__ screen, double pw,
+                                                     const double* __restrict__ scal, const int* __restrict__ flags,
+                                                     float* __restrict__ r32, double* __restrict__ part, int tz,
+                                                     int tile_x, int tile_y, int tile_z, int64_t block) {
     __shared__ double tiles[2][kUY + 2][kUX + 2];  // by plane parity: one barrier per plane
     __shared__ double shared[1][32];
     const int n = g.n;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kUX + tx;
-    const int bx = blockIdx.x * kUX, by = blockIdx.y * kUY;
+    const int bx = tile_x * kUX, by = tile_y * kUY;
     const int x = bx + tx, y = by + ty;
-    const int z0 = blockIdx.z * kTZ, z1 = min(n, z0 + kTZ);
+    const int z0 = tile_z * tz, z1 = min(n, z0 + tz);
     const double h = (double)(n - 1), h2 = h * h;
     const int odd = flags[1] & 1;
     const bool first = flags[0] != 0;
@@ -270,16 +289,28 @@ __global__ void __launch_bounds__(kUThreads) update_residual_kernel(
         hc += g.plane;
     }
     block_sums<1>(v, shared);
-    if (lin_tid() == 0) part[block_index()] = v[0];
+    if (lin_tid() == 0) part[block] = v[0];
+}
+
+__global__ void __launch_bounds__(kUThreads) update_residual_kernel(
+    const float* __restrict__ z, Pad g, float* p0, float* p1, double* x0, double* x1, const double* __restrict__ b,
+    const double* __restrict__ screen, double pw, const double* __restrict__ scal, const int* __restrict__ flags,
+    float* __restrict__ r32, double* __restrict__ part, int tz) {
+    update_residual_body(z, g, p0, p1, x0, x1, b, screen, pw, scal, flags, r32, part, tz, blockIdx.x, blockIdx.y,
+                         blockIdx.z, block_index());
 }
 
 // out[0] = sum over blocks of part[b] (fixed order).
-__global__ void sum_kernel(const double* __restrict__ part, int blocks, double* __restrict__ out) {
+__device__ __forceinline__ void sum_body(const double* __restrict__ part, int blocks, double* __restrict__ out) {
     __shared__ double shared[1][32];
     double v[1] = {0.0};
     for (int b = threadIdx.x; b < blocks; b += blockDim.x) v[0] += part[b];
     block_sums<1>(v, shared);
     if (threadIdx.x == 0) out[0] = v[0];
+}
+
+__global__ void sum_kernel(const double* __restrict__ part, int blocks, double* __restrict__ out) {
+    sum_body(part, blocks, out);
 }
 
 // End of one iteration: record ||r||^2, count it, clear the first-step flag
@@ -299,19 +330,181 @@ __global__ void loop_kernel(cudaGraphConditionalHandle handle, int use_handle, c
     if (use_handle) cudaGraphSetConditional(handle, more ? 1u : 0u);
 }
 
-static dim3 flat_grid_of(int n) { return dim3((n * n + kThreads - 1) / kThreads, (n + kTZ - 1) / kTZ); }
-static dim3 tile_grid_of(int n) { return dim3((n + kUX - 1) / kUX, (n + kUY - 1) / kUY, (n + kTZ - 1) / kTZ); }
+static int direction_planes(int n) {
+    const int64_t tz = tuned(PB_TUNE_FCG_DIRECTION_PLANES, n, kTZ);
+    return tz < kMinTZ ? kMinTZ : (int)tz;
+}
+static int update_planes(int n) {
+    const int64_t tz = tuned(PB_TUNE_FCG_UPDATE_PLANES, n, kTZ);
+    return tz < kMinTZ ? kMinTZ : (int)tz;
+}
+static dim3 flat_grid_of(int n, int tz) { return dim3((n * n + kThreads - 1) / kThreads, (n + tz - 1) / tz); }
+static dim3 tile_grid_of(int n, int tz) {
+    return dim3((n + kUX - 1) / kUX, (n + kUY - 1) / kUY, (n + tz - 1) / tz);
+}
 static unsigned count(dim3 g) { return g.x * g.y * g.z; }
-static unsigned blocks_of(int n) {
-    const unsigned a = count(flat_grid_of(n)), t = count(tile_grid_of(n));
+static unsigned blocks_of(int n) {  // the most either pass can launch (kMinTZ planes per block)
+    const unsigned a = count(flat_grid_of(n, kMinTZ)), t = count(tile_grid_of(n, kMinTZ));
     return a > t ? a : t;
 }
-static Pad pad_of(int n) {
+__host__ __device__ inline Pad pad_of(int n) {
     const int P = ((n + 5) + 7) & ~7;
     return Pad{n, P, (int64_t)(n + 2) * P};
 }
 
+// ---- grouped launches over a batch of clouds (batch.cuh) --------------------------
+// Per cloud c: flags + 4c (first step, iterations, active), scal + 8c, its own
+// partial-sum area.  The point weight travels as the bits of a double in aux[0].
+
+__device__ __forceinline__ double aux_double(int64_t bits) { return __longlong_as_double((long long)bits); }
+
+// ptr[0] z, ptr[1] p0, ptr[2] p1, ptr[3] r32, ptr[4] screen, ptr[5] partials.
+__global__ void __launch_bounds__(kThreads, 4) direction_sums_grouped_kernel(const batch::GridDesc* __restrict__ descs,
+                                                                             int count, const int* __restrict__ flags) {
+    int bx, by, bz;
+    const batch::GridDesc& d = batch::locate(descs, count, blockIdx.x, bx, by, bz);
+    if (!batch::cloud_active(flags, d.cloud)) return;
+    direction_sums_body((const float*)d.ptr[0], pad_of((int)d.n), (const float*)d.ptr[1], (const float*)d.ptr[2],
+                        (const float*)d.ptr[3], (const double*)d.ptr[4], aux_double(d.aux[0]),
+                        flags + d.cloud * batch::kFlagStride, (double*)d.ptr[5], (int)d.aux[1], bx, by,
+                        bx + d.gx * (int64_t)by);
+}
+
+// One block per cloud: ptr[0] partials, ptr[1] the cloud's scalars; aux[0] pass-1 blocks.
+__global__ void direction_finish_grouped_kernel(const batch::GridDesc* __restrict__ descs, int count,
+                                                const int* __restrict__ flags) {
+    int bx, by, bz;
+    const batch::GridDesc& d = batch::locate(descs, count, blockIdx.x, bx, by, bz);
+    if (!batch::cloud_active(flags, d.cloud)) return;
+    direction_finish_body((const double*)d.ptr[0], (int)d.aux[0], flags + d.cloud * batch::kFlagStride,
+                          (double*)d.ptr[1]);
+}
+
+// ptr[0] z, ptr[1] p0, ptr[2] p1, ptr[3] x0, ptr[4] x1, ptr[5] b, ptr[6] screen, ptr[7] r32, ptr[8] the
+// cloud's scalars, ptr[9] partials.
+__global__ void __launch_bounds__(kUThreads) update_residual_grouped_kernel(const batch::GridDesc* __restrict__ descs,
+                                                                            int count, const int* __restrict__ flags) {
+    int bx, by, bz;
+    const batch::GridDesc& d = batch::locate(descs, count, blockIdx.x, bx, by, bz);
+    if (!batch::cloud_active(flags, d.cloud)) return;
+    update_residual_body((const float*)d.ptr[0], pad_of((int)d.n), (float*)d.ptr[1], (float*)d.ptr[2],
+                         (double*)d.ptr[3], (double*)d.ptr[4], (const double*)d.ptr[5], (const double*)d.ptr[6],
+                         aux_double(d.aux[0]), (const double*)d.ptr[8], flags + d.cloud * batch::kFlagStride,
+                         (float*)d.ptr[7], (double*)d.ptr[9], (int)d.aux[1], bx, by, bz,
+                         bx + d.gx * ((int64_t)by + d.gy * bz));
+}
+
+// One block per cloud: ptr[0] partials, ptr[1] output (the cloud's scal + 4); aux[0] blocks.
+__global__ void sum_grouped_kernel(const batch::GridDesc* __restrict__ descs, int count,
+                                   const int* __restrict__ flags) {
+    int bx, by, bz;
+    const batch::GridDesc& d = batch::locate(descs, count, blockIdx.x, bx, by, bz);
+    if (!batch::cloud_active(flags, d.cloud)) return;
+    sum_body((const double*)d.ptr[0], (int)d.aux[0], (double*)d.ptr[1]);
+}
+
+// End of one batch iteration, every active cloud: record ||r||^2, count the
+// iteration, clear the first-step flag, and keep the cloud active while
+// ||r||^2 > target2 and fewer than min(max_iter, cap) iterations have run.  The
+// WHILE condition (inside a graph) continues while any cloud is active.
+__global__ void __launch_bounds__(1024) loop_batch_kernel(cudaGraphConditionalHandle handle, int use_handle,
+                                                          const double* __restrict__ scal,
+                                                          const double* __restrict__ ctrl, int* __restrict__ flags,
+                                                          int clouds, int max_iter, double* __restrict__ history) {
+    int any = 0;
+    for (int c = threadIdx.x; c < clouds; c += blockDim.x) {
+        int* f = flags + (int64_t)c * batch::kFlagStride;
+        if (!f[batch::kFlagActive]) continue;
+        const int it = f[batch::kFlagIter] + 1;
+        f[batch::kFlagIter] = it;
+        f[batch::kFlagFirst] = 0;
+        const double r2 = scal[(int64_t)c * batch::kScalStride + 4];
+        if (history && it <= max_iter) history[(int64_t)c * max_iter + it - 1] = r2;
+        const double* ct = ctrl + (int64_t)c * batch::kCtrlStride;
+        const bool more = r2 > ct[0] && it < max_iter && (double)it < ct[1];
+        f[batch::kFlagActive] = more ? 1 : 0;
+        any |= more ? 1 : 0;
+    }
+    any = __syncthreads_or(any);
+    if (use_handle && threadIdx.x == 0) cudaGraphSetConditional(handle, any ? 1u : 0u);
+}
+
 }  // namespace fcg
+
+namespace batch {
+
+int describe_fcg_direction(GridDesc& d) {
+    const int n = (int)d.n;
+    for (int k = 0; k < 6; ++k)
+        if (!d.ptr[k]) return fail(PB_ERR_INVALID, "batch fcg direction: bad args");
+    if (n < 2 || n > 4097 || d.ptr[1] == d.ptr[2]) return fail(PB_ERR_INVALID, "batch fcg direction: bad args");
+    const int tz = fcg::direction_planes(n);
+    const dim3 g = fcg::flat_grid_of(n, tz);
+    d.gx = g.x;
+    d.gy = g.y;
+    d.gz = 1;
+    d.aux[1] = tz;
+    return PB_OK;
+}
+
+int describe_fcg_update(GridDesc& d) {
+    const int n = (int)d.n;
+    for (int k = 0; k < 10; ++k)
+        if (!d.ptr[k]) return fail(PB_ERR_INVALID, "batch fcg update: bad args");
+    if (n < 2 || n > 4097 || d.ptr[1] == d.ptr[2] || d.ptr[3] == d.ptr[4])
+        return fail(PB_ERR_INVALID, "batch fcg update: bad args");
+    const int tz = fcg::update_planes(n);
+    const dim3 g = fcg::tile_grid_of(n, tz);
+    d.gx = g.x;
+    d.gy = g.y;
+    d.gz = g.z;
+    d.aux[1] = tz;
+    return PB_OK;
+}
+
+int describe_fcg_reduce(GridDesc& d) {
+    if (!d.ptr[0] || !d.ptr[1] || d.aux[0] < 1) return fail(PB_ERR_INVALID, "batch fcg reduce: bad args");
+    d.gx = d.gy = d.gz = 1;
+    return PB_OK;
+}
+
+// Partial-sum doubles one cloud of side n needs (both FCG passes).
+int64_t fcg_partials(int n) { return (int64_t)fcg::blocks_of(n) * 4; }
+int64_t fcg_direction_blocks(int n) { return fcg::count(fcg::flat_grid_of(n, fcg::direction_planes(n))); }
+int64_t fcg_update_blocks(int n) { return fcg::count(fcg::tile_grid_of(n, fcg::update_planes(n))); }
+
+int launch_fcg(int kind, const GridDesc* descs, int count, int64_t blocks, const int* flags, cudaStream_t s) {
+    switch (kind) {
+        case 0:
+            fcg::direction_sums_grouped_kernel<<<(unsigned)blocks, fcg::kThreads, 0, s>>>(descs, count, flags);
+            PB_CHECK_LAUNCH("direction_sums_grouped_kernel");
+            return PB_OK;
+        case 1:
+            fcg::direction_finish_grouped_kernel<<<(unsigned)blocks, 1024, 0, s>>>(descs, count, flags);
+            PB_CHECK_LAUNCH("direction_finish_grouped_kernel");
+            return PB_OK;
+        case 2:
+            fcg::update_residual_grouped_kernel<<<(unsigned)blocks, dim3(fcg::kUX, fcg::kUY), 0, s>>>(descs, count,
+                                                                                                      flags);
+            PB_CHECK_LAUNCH("update_residual_grouped_kernel");
+            return PB_OK;
+        case 3:
+            fcg::sum_grouped_kernel<<<(unsigned)blocks, 1024, 0, s>>>(descs, count, flags);
+            PB_CHECK_LAUNCH("sum_grouped_kernel");
+            return PB_OK;
+    }
+    return fail(PB_ERR_INVALID, "batch fcg: unknown kind %d", kind);
+}
+
+int launch_loop_batch(unsigned long long handle, const double* scal, const double* ctrl, int* flags, int clouds,
+                      int max_iter, double* history, cudaStream_t s) {
+    fcg::loop_batch_kernel<<<1, 1024, 0, s>>>((cudaGraphConditionalHandle)handle, handle != 0, scal, ctrl, flags,
+                                              clouds, max_iter, history);
+    PB_CHECK_LAUNCH("loop_batch_kernel");
+    return PB_OK;
+}
+
+}  // namespace batch
 }  // namespace pb
 
 using namespace pb;
@@ -340,9 +533,10 @@ extern "C" int pb_fcg_direction_f64(const float* z, const float* p0, const float
     PB_TRY(fcg_check(n, workspace_bytes, workspace));
     double* part = (double*)workspace;
     cudaStream_t s = (cudaStream_t)stream;
-    const dim3 grid = flat_grid_of((int)n);
+    const int tz = direction_planes((int)n);
+    const dim3 grid = flat_grid_of((int)n, tz);
     direction_sums_kernel<<<grid, kThreads, 0, s>>>(z, pad_of((int)n), p0, p1, r32, screen, point_weight,
-                                                          flags, part);
+                                                          flags, part, tz);
     PB_CHECK_LAUNCH("fcg direction_sums_kernel");
     direction_finish_kernel<<<1, 1024, 0, s>>>(part, (int)count(grid), flags, scal);
     PB_CHECK_LAUNCH("fcg direction_finish_kernel");
@@ -362,9 +556,10 @@ extern "C" int pb_fcg_update_f64(const float* z, float* p0, float* p1, double* x
     PB_TRY(fcg_check(n, workspace_bytes, workspace));
     double* part = (double*)workspace;
     cudaStream_t s = (cudaStream_t)stream;
-    const dim3 grid = tile_grid_of((int)n);
+    const int tz = update_planes((int)n);
+    const dim3 grid = tile_grid_of((int)n, tz);
     update_residual_kernel<<<grid, dim3(kUX, kUY), 0, s>>>(z, pad_of((int)n), p0, p1, x0, x1, b, screen,
-                                                           point_weight, scal, flags, r32, part);
+                                                           point_weight, scal, flags, r32, part, tz);
     PB_CHECK_LAUNCH("fcg update_residual_kernel");
     sum_kernel<<<1, 1024, 0, s>>>(part, (int)count(grid), scal + 4);
     PB_CHECK_LAUNCH("fcg sum_kernel");

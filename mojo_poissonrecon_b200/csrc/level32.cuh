@@ -23,7 +23,7 @@ struct Geom {
 };
 
 __host__ __device__ inline int pitch_of(int n) { return ((n + 5) + 7) & ~7; }
-inline Geom geom(int n) { return Geom{n, pitch_of(n), (int64_t)(n + 2) * pitch_of(n)}; }
-inline int64_t padded_size(int n) { return (int64_t)(n + 2) * geom(n).plane; }
+__host__ __device__ inline Geom geom(int n) { return Geom{n, pitch_of(n), (int64_t)(n + 2) * pitch_of(n)}; }
+__host__ __device__ inline int64_t padded_size(int n) { return (int64_t)(n + 2) * geom(n).plane; }
 
 }  // namespace pb

@@ -34,6 +34,7 @@
 // plane k(K) at J-K (symmetry).  Ghost entries are zero.
 #include <cuda_fp16.h>
 
+#include "batch.cuh"
 #include "common.cuh"
 #include "level32.cuh"
 
@@ -325,10 +326,11 @@ __global__ void level27_finish_kernel(const float* __restrict__ c, int64_t cs, G
 // ---- 27-point smoothing, residual, transfers ------------------------------------
 // coarse[J] = sum_o w(o)/64 res[2J+o], w = prod (2 on the axis, 1 off it);
 // out-of-grid fine nodes are ghosts holding zero.
-__global__ void __launch_bounds__(256) restrict27_kernel(const float* __restrict__ res, Geom gf,
-                                                         float* __restrict__ coarse, Geom gc) {
-    int x, y, z;
-    if (!plane_node(gc.n, x, y, z)) return;
+__device__ __forceinline__ void restrict27_body(const float* __restrict__ res, Geom gf, float* __restrict__ coarse,
+                                                Geom gc, int bx, int by) {
+    const unsigned t = bx * blockDim.x + threadIdx.x;
+    if (t >= (unsigned)(gc.n * gc.n)) return;
+    const int y = (int)(t / (unsigned)gc.n), x = (int)(t - (unsigned)y * gc.n), z = by;
     const int64_t p = gf.at(2 * x, 2 * y, 2 * z);
     float s = 0.0f;
 #pragma unroll
@@ -339,6 +341,11 @@ __global__ void __launch_bounds__(256) restrict27_kernel(const float* __restrict
             for (int dx = -1; dx <= 1; ++dx)
                 s += res[p + offset_of(gf, dx, dy, dz)] * (float)((dx ? 1 : 2) * (dy ? 1 : 2) * (dz ? 1 : 2));
     coarse[gc.at(x, y, z)] = s * (1.0f / 64.0f);
+}
+
+__global__ void __launch_bounds__(256) restrict27_kernel(const float* __restrict__ res, Geom gf,
+                                                         float* __restrict__ coarse, Geom gc) {
+    restrict27_body(res, gf, coarse, gc, blockIdx.x, blockIdx.y);
 }
 
 // ---- packed 27-point levels: per-colour FP16 couplings --------------------------
@@ -369,7 +376,7 @@ struct Packed {
     __host__ __device__ __forceinline__ int64_t at(int i, int y, int z) const { return ((int64_t)z * n + y) * Pc + i; }
 };
 
-inline Packed packed_of(int n) {
+__host__ __device__ inline Packed packed_of(int n) {
     Packed p;
     p.n = n;
     p.Pc = (n + 1) / 2;
@@ -422,12 +429,12 @@ __device__ __forceinline__ void load_couplings(const __half* __restrict__ h, int
 // when COLOUR == 1 (updated by pass 0), everything else from `prev` (zero when
 // ZERO).
 template <int COLOUR, bool ZERO>
-__global__ void __launch_bounds__(256) relax27p_kernel(const float* __restrict__ prev, float* next,
-                                                       const float* __restrict__ rhs, const __half* __restrict__ h,
-                                                       const float* __restrict__ inv, Geom g, Packed pk) {
+__device__ __forceinline__ void relax27p_body(const float* __restrict__ prev, float* next,
+                                              const float* __restrict__ rhs, const __half* __restrict__ h,
+                                              const float* __restrict__ inv, Geom g, Packed pk, int bx, int by) {
     // threads flattened over the plane's compact (i, y) nodes: full warps on odd rows
-    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int n = g.n, z = blockIdx.y;
+    const unsigned t = bx * blockDim.x + threadIdx.x;
+    const int n = g.n, z = by;
     if (t >= (unsigned)(pk.Pc * n)) return;
     const int y = (int)(t / (unsigned)pk.Pc), i = (int)(t - (unsigned)y * pk.Pc);
     const int x = 2 * i + ((y + z + COLOUR) & 1);
@@ -452,15 +459,21 @@ __global__ void __launch_bounds__(256) relax27p_kernel(const float* __restrict__
     next[p] = inv[q] * rhs[p] + s;
 }
 
+template <int COLOUR, bool ZERO>
+__global__ void __launch_bounds__(256) relax27p_kernel(const float* __restrict__ prev, float* next,
+                                                       const float* __restrict__ rhs, const __half* __restrict__ h,
+                                                       const float* __restrict__ inv, Geom g, Packed pk) {
+    relax27p_body<COLOUR, ZERO>(prev, next, rhs, h, inv, g, pk, blockIdx.x, blockIdx.y);
+}
+
 // res = s (rhs - A e) on a packed level, one thread per node.
-__global__ void __launch_bounds__(256) residual27p_kernel(const float* __restrict__ e, const float* __restrict__ rhs,
-                                                          const __half* __restrict__ h0,
-                                                          const __half* __restrict__ h1,
-                                                          const float* __restrict__ i0, const float* __restrict__ i1,
-                                                          const float* __restrict__ fac, Geom g, Packed pk,
-                                                          float* __restrict__ res) {
-    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;  // flattened over the plane's (x, y)
-    const int n = g.n, z = blockIdx.y;
+__device__ __forceinline__ void residual27p_body(const float* __restrict__ e, const float* __restrict__ rhs,
+                                                 const __half* __restrict__ h0, const __half* __restrict__ h1,
+                                                 const float* __restrict__ i0, const float* __restrict__ i1,
+                                                 const float* __restrict__ fac, Geom g, Packed pk,
+                                                 float* __restrict__ res, int bx, int by) {
+    const unsigned t = bx * blockDim.x + threadIdx.x;  // flattened over the plane's (x, y)
+    const int n = g.n, z = by;
     if (t >= (unsigned)(n * n)) return;
     const int y = (int)(t / (unsigned)n), x = (int)(t - (unsigned)y * n);
     const int colour = (x + y + z) & 1;
@@ -480,6 +493,15 @@ __global__ void __launch_bounds__(256) residual27p_kernel(const float* __restric
             }
     const float inv = colour ? i1[q] : i0[q];
     res[p] = fac[p] * (rhs[p] - (e[p] - s) / inv);
+}
+
+__global__ void __launch_bounds__(256) residual27p_kernel(const float* __restrict__ e, const float* __restrict__ rhs,
+                                                          const __half* __restrict__ h0,
+                                                          const __half* __restrict__ h1,
+                                                          const float* __restrict__ i0, const float* __restrict__ i1,
+                                                          const float* __restrict__ fac, Geom g, Packed pk,
+                                                          float* __restrict__ res) {
+    residual27p_body(e, rhs, h0, h1, i0, i1, fac, g, pk, res, blockIdx.x, blockIdx.y);
 }
 
 // ---- exact solve on the 3^3 level -----------------------------------------------
@@ -646,10 +668,9 @@ __device__ void cube_relax(const float* cf, const float* invD, const float* rhs,
         }
 }
 
-__global__ void __launch_bounds__(kC27Threads) coarse27_kernel(const float4* __restrict__ image, CoarseLayout lay,
-                                                               const float* __restrict__ rhs0,
-                                                               float* __restrict__ e0, Geom g0, int pre, int post,
-                                                               int inner) {
+__device__ __forceinline__ void coarse27_body(const float4* __restrict__ image, const CoarseLayout& lay,
+                                              const float* __restrict__ rhs0, float* __restrict__ e0, Geom g0,
+                                              int pre, int post, int inner) {
     extern __shared__ float4 smem4[];
     float* sm = reinterpret_cast<float*>(smem4);
     const int tid = threadIdx.x;
@@ -729,6 +750,63 @@ __global__ void __launch_bounds__(kC27Threads) coarse27_kernel(const float4* __r
         unflatten(tid, n, x, y, z);
         e0[g0.at(x, y, z)] = sm[lay.e[0] + cube_at(x, y, z, n)];
     }
+}
+
+__global__ void __launch_bounds__(kC27Threads) coarse27_kernel(const float4* __restrict__ image, CoarseLayout lay,
+                                                               const float* __restrict__ rhs0,
+                                                               float* __restrict__ e0, Geom g0, int pre, int post,
+                                                               int inner) {
+    coarse27_body(image, lay, rhs0, e0, g0, pre, post, inner);
+}
+
+// ---- grouped launches (batch.cuh) ----------------------------------------------------
+
+// relax27p: ptr[0] e_prev (null: from zero), ptr[1] e_next, ptr[2] rhs, ptr[3] h0, ptr[4] h1, ptr[5] inv0,
+// ptr[6] inv1.  Colour COLOUR of every grid.
+template <int COLOUR, bool ZERO>
+__global__ void __launch_bounds__(256) relax27p_grouped_kernel(const batch::GridDesc* __restrict__ descs, int count,
+                                                               const int* __restrict__ flags) {
+    int bx, by, bz;
+    const batch::GridDesc& d = batch::locate(descs, count, blockIdx.x, bx, by, bz);
+    if (!batch::cloud_active(flags, d.cloud)) return;
+    const int n = (int)d.n;
+    relax27p_body<COLOUR, ZERO>((const float*)d.ptr[0], (float*)d.ptr[1], (const float*)d.ptr[2],
+                                (const __half*)d.ptr[3 + COLOUR], (const float*)d.ptr[5 + COLOUR], geom(n),
+                                packed_of(n), bx, by);
+}
+
+// residual27p: ptr[0] e, ptr[1] rhs, ptr[2] h0, ptr[3] h1, ptr[4] inv0, ptr[5] inv1, ptr[6] weights, ptr[7] res.
+__global__ void __launch_bounds__(256) residual27p_grouped_kernel(const batch::GridDesc* __restrict__ descs,
+                                                                  int count, const int* __restrict__ flags) {
+    int bx, by, bz;
+    const batch::GridDesc& d = batch::locate(descs, count, blockIdx.x, bx, by, bz);
+    if (!batch::cloud_active(flags, d.cloud)) return;
+    const int n = (int)d.n;
+    residual27p_body((const float*)d.ptr[0], (const float*)d.ptr[1], (const __half*)d.ptr[2],
+                     (const __half*)d.ptr[3], (const float*)d.ptr[4], (const float*)d.ptr[5], (const float*)d.ptr[6],
+                     geom(n), packed_of(n), (float*)d.ptr[7], bx, by);
+}
+
+// restrict27: ptr[0] fine residual, ptr[1] coarse rhs; d.n is the fine side.
+__global__ void __launch_bounds__(256) restrict27_grouped_kernel(const batch::GridDesc* __restrict__ descs, int count,
+                                                                 const int* __restrict__ flags) {
+    int bx, by, bz;
+    const batch::GridDesc& d = batch::locate(descs, count, blockIdx.x, bx, by, bz);
+    if (!batch::cloud_active(flags, d.cloud)) return;
+    const int n = (int)d.n;
+    restrict27_body((const float*)d.ptr[0], geom(n), (float*)d.ptr[1], geom((n + 1) / 2), bx, by);
+}
+
+// coarse27: one block per cloud; ptr[0] image, ptr[1] rhs, ptr[2] e; d.n the first level's side (9, 5 or 3
+// levels below it); aux[0..2] pre, post, inner.  Every grid of one launch has the same side.
+__global__ void __launch_bounds__(kC27Threads) coarse27_grouped_kernel(const batch::GridDesc* __restrict__ descs,
+                                                                       int count, const int* __restrict__ flags,
+                                                                       CoarseLayout lay) {
+    int bx, by, bz;
+    const batch::GridDesc& d = batch::locate(descs, count, blockIdx.x, bx, by, bz);
+    if (!batch::cloud_active(flags, d.cloud)) return;
+    coarse27_body((const float4*)d.ptr[0], lay, (const float*)d.ptr[1], (float*)d.ptr[2], geom((int)d.n),
+                  (int)d.aux[0], (int)d.aux[1], (int)d.aux[2]);
 }
 
 
@@ -952,3 +1030,99 @@ extern "C" int pb_residual_restrict27p_f32(const float* e, const float* rhs, con
     PB_CHECK_LAUNCH("restrict27_kernel");
     return PB_OK;
 }
+
+// ---- grouped launches (batch.cuh) ----------------------------------------------------
+
+namespace pb {
+namespace batch {
+
+int describe_relax27p(GridDesc& d, bool zero) {
+    const int n = (int)d.n;
+    if (!level_side_ok(n) || (!zero && !d.ptr[0]) || !d.ptr[1] || !d.ptr[2] || !d.ptr[3] || !d.ptr[4] || !d.ptr[5] ||
+        !d.ptr[6] || d.ptr[0] == d.ptr[1])
+        return fail(PB_ERR_INVALID, "batch relax27p: bad args");
+    const Packed pk = packed_of(n);
+    d.gx = (pk.Pc * n + 255) / 256;
+    d.gy = n;
+    d.gz = 1;
+    return PB_OK;
+}
+
+int launch_relax27p(const GridDesc* descs, int count, int64_t blocks, bool zero, const int* flags, cudaStream_t s) {
+    if (zero) {
+        relax27p_grouped_kernel<0, true><<<(unsigned)blocks, 256, 0, s>>>(descs, count, flags);
+        PB_CHECK_LAUNCH("relax27p_grouped_kernel");
+        relax27p_grouped_kernel<1, true><<<(unsigned)blocks, 256, 0, s>>>(descs, count, flags);
+    } else {
+        relax27p_grouped_kernel<0, false><<<(unsigned)blocks, 256, 0, s>>>(descs, count, flags);
+        PB_CHECK_LAUNCH("relax27p_grouped_kernel");
+        relax27p_grouped_kernel<1, false><<<(unsigned)blocks, 256, 0, s>>>(descs, count, flags);
+    }
+    PB_CHECK_LAUNCH("relax27p_grouped_kernel");
+    return PB_OK;
+}
+
+int describe_residual27p(GridDesc& d) {
+    const int n = (int)d.n;
+    for (int k = 0; k < 8; ++k)
+        if (!d.ptr[k]) return fail(PB_ERR_INVALID, "batch residual27p: bad args");
+    if (!level_side_ok(n) || n < 5) return fail(PB_ERR_INVALID, "batch residual27p: bad side");
+    d.gx = (n * n + 255) / 256;
+    d.gy = n;
+    d.gz = 1;
+    return PB_OK;
+}
+
+int launch_residual27p(const GridDesc* descs, int count, int64_t blocks, const int* flags, cudaStream_t s) {
+    residual27p_grouped_kernel<<<(unsigned)blocks, 256, 0, s>>>(descs, count, flags);
+    PB_CHECK_LAUNCH("residual27p_grouped_kernel");
+    return PB_OK;
+}
+
+int describe_restrict27(GridDesc& d) {
+    const int n = (int)d.n;
+    if (!level_side_ok(n) || n < 5 || !d.ptr[0] || !d.ptr[1]) return fail(PB_ERR_INVALID, "batch restrict27: bad args");
+    const int cn = (n + 1) / 2;
+    d.gx = (cn * cn + 255) / 256;
+    d.gy = cn;
+    d.gz = 1;
+    return PB_OK;
+}
+
+int launch_restrict27(const GridDesc* descs, int count, int64_t blocks, const int* flags, cudaStream_t s) {
+    restrict27_grouped_kernel<<<(unsigned)blocks, 256, 0, s>>>(descs, count, flags);
+    PB_CHECK_LAUNCH("restrict27_grouped_kernel");
+    return PB_OK;
+}
+
+int describe_coarse27(GridDesc& d) {
+    const int n = (int)d.n;
+    if (!level_side_ok(n) || n > kC27N || !d.ptr[0] || !d.ptr[1] || !d.ptr[2] ||
+        (reinterpret_cast<uintptr_t>(d.ptr[0]) & 15))
+        return fail(PB_ERR_INVALID, "batch coarse27: bad args");
+    if (d.aux[0] < 0 || d.aux[1] < 0 || d.aux[2] < 0 || d.aux[0] > 64 || d.aux[1] > 64 || d.aux[2] > 64)
+        return fail(PB_ERR_INVALID, "batch coarse27: sweep counts must be in [0, 64]");
+    d.gx = d.gy = d.gz = 1;
+    return PB_OK;
+}
+
+int launch_coarse27(const GridDesc* descs, int count, int64_t blocks, int first_side, const int* flags,
+                    cudaStream_t s) {
+    int sz[kC27MaxLevels];
+    int levels = 0;
+    for (int m = first_side; levels < kC27MaxLevels; m = (m + 1) / 2) {
+        sz[levels++] = m;
+        if (m == 3) break;
+    }
+    if (sz[levels - 1] != 3) return fail(PB_ERR_INVALID, "batch coarse27: first side must be 9, 5 or 3");
+    const CoarseLayout lay = coarse_layout(levels, sz);
+    const size_t smem = (size_t)lay.total * sizeof(float);
+    PB_CHECK_CUDA(cudaFuncSetAttribute(coarse27_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                  "batch coarse27 smem");
+    coarse27_grouped_kernel<<<(unsigned)blocks, kC27Threads, smem, s>>>(descs, count, flags, lay);
+    PB_CHECK_LAUNCH("coarse27_grouped_kernel");
+    return PB_OK;
+}
+
+}  // namespace batch
+}  // namespace pb

@@ -2,6 +2,9 @@
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "common.cuh"
 
@@ -22,6 +25,17 @@ int fail(int code, const char* fmt, ...) {
 
 int cuda_fail(cudaError_t err, const char* where) {
     return fail(PB_ERR_CUDA, "%s: %s (%s)", where, cudaGetErrorString(err), cudaGetErrorName(err));
+}
+
+// Launch parameters chosen by the autotuner, per (parameter, grid side); read
+// by the host launchers, which fall back to their built-in choice when unset.
+static std::mutex g_tune_mu;
+static std::map<std::pair<int64_t, int64_t>, int64_t> g_tune;
+
+int64_t tuned(int param, int64_t n, int64_t fallback) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune.find({(int64_t)param, n});
+    return it == g_tune.end() ? fallback : it->second;
 }
 
 }  // namespace pb
@@ -46,5 +60,22 @@ extern "C" int pb_init(int device) {
     if (prop.major != 10)
         return pb::fail(PB_ERR_DEVICE, "pb_init: device %d is sm_%d%d; this library is built for sm_100a", device,
                         prop.major, prop.minor);
+    return PB_OK;
+}
+
+extern "C" int pb_tune_set(int64_t param, int64_t n, int64_t value) {
+    if (param < 0 || param >= PB_TUNE_PARAMS || n < 2 || n > 4097 || value < 0 || value > 4097)
+        return pb::fail(PB_ERR_INVALID, "tune set: bad parameter, side or value");
+    std::lock_guard<std::mutex> lock(pb::g_tune_mu);
+    if (value == 0) pb::g_tune.erase({param, n});
+    else pb::g_tune[{param, n}] = value;
+    return PB_OK;
+}
+
+extern "C" int64_t pb_tune_get(int64_t param, int64_t n) { return pb::tuned((int)param, n, 0); }
+
+extern "C" int pb_tune_clear(void) {
+    std::lock_guard<std::mutex> lock(pb::g_tune_mu);
+    pb::g_tune.clear();
     return PB_OK;
 }

@@ -8,6 +8,7 @@
 // equals the reference's Neumann sum over in-grid neighbours, and the degree
 // term lives in the stored diagonal D = (deg + pw*screen) * (n-1)^2.  The
 // coarse levels are Galerkin operators (mg27.cu).
+#include "batch.cuh"
 #include "common.cuh"
 #include "level32.cuh"
 
@@ -125,16 +126,14 @@ constexpr int kRrFX = 2 * kRrCX + 8, kRrFY = 2 * kRrCY + 1;  // 136 x 9 fine nod
 constexpr int kRrGroups = kRrFX / 4;                            // float4 groups per ring row
 constexpr int kRrThreads = 256;
 
-__global__ void __launch_bounds__(kRrThreads) residual_restrict32_kernel(const float* __restrict__ e,
-                                                                          const float* __restrict__ rhs,
-                                                                          const float* __restrict__ D,
-                                                                          const float* __restrict__ w, Geom gf,
-                                                                          float h2, float* __restrict__ coarse,
-                                                                          Geom gc) {
+__device__ __forceinline__ void residual_restrict32_body(const float* __restrict__ e, const float* __restrict__ rhs,
+                                                         const float* __restrict__ D, const float* __restrict__ w,
+                                                         Geom gf, float h2, float* __restrict__ coarse, Geom gc,
+                                                         int cz, int bx, int by, int bz) {
     __shared__ __align__(16) float ring[kRrRing][kRrFY][kRrFX];
     const int fn = gf.n, cn = gc.n;
-    const int xc0 = blockIdx.x * kRrCX, yc0 = blockIdx.y * kRrCY;
-    const int zc0 = blockIdx.z * kRrCZ, zc1 = min(cn, zc0 + kRrCZ);
+    const int xc0 = bx * kRrCX, yc0 = by * kRrCY;
+    const int zc0 = bz * cz, zc1 = min(cn, zc0 + cz);
     const int fx0 = 2 * xc0 - 4, fy0 = 2 * yc0 - 1;
     const int tid = threadIdx.x;
     auto fine_plane = [&](int f) {  // s-weighted residual of fine plane f over the tile region
@@ -195,6 +194,27 @@ __global__ void __launch_bounds__(kRrThreads) residual_restrict32_kernel(const f
         // 2zc+3, whose slots (mod 5) differ from the three read here, and the one
         // after it rewrites these only after all threads pass its first barrier
     }
+}
+
+__global__ void __launch_bounds__(kRrThreads) residual_restrict32_kernel(const float* __restrict__ e,
+                                                                          const float* __restrict__ rhs,
+                                                                          const float* __restrict__ D,
+                                                                          const float* __restrict__ w, Geom gf,
+                                                                          float h2, float* __restrict__ coarse,
+                                                                          Geom gc, int cz) {
+    residual_restrict32_body(e, rhs, D, w, gf, h2, coarse, gc, cz, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Grouped (batch.cuh): ptr[0] e, ptr[1] rhs, ptr[2] D, ptr[3] weights, ptr[4] coarse rhs.
+__global__ void __launch_bounds__(kRrThreads) residual_restrict32_grouped_kernel(
+    const batch::GridDesc* __restrict__ descs, int count, const int* __restrict__ flags) {
+    int bx, by, bz;
+    const batch::GridDesc& d = batch::locate(descs, count, blockIdx.x, bx, by, bz);
+    if (!batch::cloud_active(flags, d.cloud)) return;
+    const int n = (int)d.n;
+    residual_restrict32_body((const float*)d.ptr[0], (const float*)d.ptr[1], (const float*)d.ptr[2],
+                             (const float*)d.ptr[3], geom(n), (float)((n - 1) * (n - 1)), (float*)d.ptr[4],
+                             geom((n + 1) / 2), (int)d.aux[0], bx, by, bz);
 }
 
 
@@ -260,10 +280,38 @@ extern "C" int pb_residual_restrict_f32(const float* e, const float* rhs, const 
         return fail(PB_ERR_INVALID, "residual_restrict: bad args");
     const int cn = (int)((n + 1) / 2);
     const float h2 = (float)((n - 1) * (n - 1));
-    const dim3 grid((cn + kRrCX - 1) / kRrCX, (cn + kRrCY - 1) / kRrCY, (cn + kRrCZ - 1) / kRrCZ);
+    const int cz = (int)tuned(PB_TUNE_RESTRICT_PLANES, n, kRrCZ);
+    const dim3 grid((cn + kRrCX - 1) / kRrCX, (cn + kRrCY - 1) / kRrCY, (cn + cz - 1) / cz);
     residual_restrict32_kernel<<<grid, kRrThreads, 0, (cudaStream_t)stream>>>(e, rhs, D, weights, geom((int)n), h2,
-                                                                              coarse_rhs, geom(cn));
+                                                                              coarse_rhs, geom(cn), cz);
     PB_CHECK_LAUNCH("residual_restrict32_kernel");
     return PB_OK;
 }
 
+
+// ---- grouped launches (batch.cuh) ----------------------------------------------------
+
+namespace pb {
+namespace batch {
+
+int describe_residual_restrict32(GridDesc& d) {
+    const int n = (int)d.n;
+    if (n < 3 || n > 4097 || !d.ptr[0] || !d.ptr[1] || !d.ptr[2] || !d.ptr[3] || !d.ptr[4])
+        return fail(PB_ERR_INVALID, "batch residual_restrict32: bad args");
+    const int cn = (n + 1) / 2;
+    d.gx = (cn + kRrCX - 1) / kRrCX;
+    d.gy = (cn + kRrCY - 1) / kRrCY;
+    const int cz = (int)tuned(PB_TUNE_RESTRICT_PLANES, n, kRrCZ);
+    d.gz = (cn + cz - 1) / cz;
+    d.aux[0] = cz;
+    return PB_OK;
+}
+
+int launch_residual_restrict32(const GridDesc* descs, int count, int64_t blocks, const int* flags, cudaStream_t s) {
+    residual_restrict32_grouped_kernel<<<(unsigned)blocks, kRrThreads, 0, s>>>(descs, count, flags);
+    PB_CHECK_LAUNCH("residual_restrict32_grouped_kernel");
+    return PB_OK;
+}
+
+}  // namespace batch
+}  // namespace pb

@@ -17,6 +17,7 @@
 // outstanding copies (also bounded).
 #include <cuda.h>
 
+#include "batch.cuh"
 #include "common.cuh"
 
 namespace pb {
@@ -110,21 +111,21 @@ __device__ __forceinline__ float4 lds4(const float* p) { return *reinterpret_cas
 // s = (br + t) & 1 in both phases.
 constexpr int kThreads = 352;  // 19 box rows x 18 groups = 342 work items, one per thread
 
+// The sweep of tile (bx, by) and z chunk bz; the maps may live in kernel
+// parameters (single grid) or in global memory (grouped launches).
 template <bool ZERO_IN, int SLOTS>
-__global__ void __launch_bounds__(kThreads, PB_SWEEP_MIN_BLOCKS)
-    sweep_kernel(const __grid_constant__ CUtensorMap map_e, const __grid_constant__ CUtensorMap map_rhs,
-                    const __grid_constant__ CUtensorMap map_invD, Params p) {
+__device__ __forceinline__ void sweep_body(const CUtensorMap* map_e, const CUtensorMap* map_rhs,
+                                           const CUtensorMap* map_invD, const Params& p, int bx, int by, int bz) {
     constexpr int TY = kTY;
     using G = Geo2<TY, SLOTS>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const uint32_t raw = saddr(smem_raw);
     typename G::Smem& S = *reinterpret_cast<typename G::Smem*>(smem_raw + (((raw + 127u) & ~127u) - raw));
     const int n = p.n;
-    const int bx = blockIdx.x, by = blockIdx.y;
     const int x0 = bx * kTX, y0 = by * TY;
     const int W = (bx == p.ntx - 1 ? n : x0 + kTX) - x0;
     const int H = (by == p.nty - 1 ? n : y0 + TY) - y0;
-    const int zb = blockIdx.z * p.z_chunk;
+    const int zb = bz * p.z_chunk;
     const int ze = min(n, zb + p.z_chunk);
     const int zfirst = zb - 2, zlast = ze + 1;
     const int tid = threadIdx.x;
@@ -141,9 +142,9 @@ __global__ void __launch_bounds__(kThreads, PB_SWEEP_MIN_BLOCKS)
     auto issue = [&](int z) {
         const int s = slot_of(z);
         bar_expect(&S.bar[s], bytes);
-        if (!ZERO_IN) load_box(S.slot[s][0], &map_e, x0, y0 - 1, z + 1, &S.bar[s]);
-        load_box(S.slot[s][1], &map_rhs, x0, y0 - 1, z + 1, &S.bar[s]);
-        load_box(S.slot[s][2], &map_invD, x0, y0 - 1, z + 1, &S.bar[s]);
+        if (!ZERO_IN) load_box(S.slot[s][0], map_e, x0, y0 - 1, z + 1, &S.bar[s]);
+        load_box(S.slot[s][1], map_rhs, x0, y0 - 1, z + 1, &S.bar[s]);
+        load_box(S.slot[s][2], map_invD, x0, y0 - 1, z + 1, &S.bar[s]);
     };
     int issued = zfirst;
     if (tid == 0)
@@ -247,6 +248,35 @@ __global__ void __launch_bounds__(kThreads, PB_SWEEP_MIN_BLOCKS)
     }
 }
 
+template <bool ZERO_IN, int SLOTS>
+__global__ void __launch_bounds__(kThreads, PB_SWEEP_MIN_BLOCKS)
+    sweep_kernel(const __grid_constant__ CUtensorMap map_e, const __grid_constant__ CUtensorMap map_rhs,
+                 const __grid_constant__ CUtensorMap map_invD, Params p) {
+    sweep_body<ZERO_IN, SLOTS>(&map_e, &map_rhs, &map_invD, p, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Grouped: one launch over the level-0 sweeps of many clouds (batch.cuh).
+// Descriptor operands: map[0..2] = e_in, rhs, 1/D; ptr[0] = e_out, ptr[1] =
+// status word; aux[0] = z chunk.
+template <bool ZERO_IN, int SLOTS>
+__global__ void __launch_bounds__(kThreads, PB_SWEEP_MIN_BLOCKS)
+    sweep_grouped_kernel(const batch::GridDesc* __restrict__ descs, int count, const int* __restrict__ flags) {
+    int bx, by, bz;
+    const batch::GridDesc& d = batch::locate(descs, count, blockIdx.x, bx, by, bz);
+    if (!batch::cloud_active(flags, d.cloud)) return;
+    Params p;
+    p.n = (int)d.n;
+    p.P = ((p.n + 5) + 7) & ~7;
+    p.plane = (int64_t)(p.n + 2) * p.P;
+    p.ntx = (int)d.gx;
+    p.nty = (int)d.gy;
+    p.z_chunk = (int)d.aux[0];
+    p.h2 = (float)((p.n - 1) * (p.n - 1));
+    p.e_out = (float*)d.ptr[0];
+    p.status = (int*)d.ptr[1];
+    sweep_body<ZERO_IN, SLOTS>(&d.map[0], &d.map[1], &d.map[2], p, bx, by, bz);
+}
+
 typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -293,19 +323,18 @@ static int make_map(CUtensorMap* map, const float* base, int n, int P, int rows)
 // written.
 constexpr int kProTX = 32, kProTY = 8, kProTZ = 16;
 
-__global__ void __launch_bounds__(kProTX* kProTY) prolong_add32_kernel(const float* __restrict__ c,
-                                                                       float* __restrict__ f,
-                                                                       const float* __restrict__ w, int n, int P,
-                                                                       int cn, int cP, int tz, int row) {
+__device__ __forceinline__ void prolong_add32_body(const float* __restrict__ c, float* __restrict__ f,
+                                                   const float* __restrict__ w, int n, int P, int cn, int cP, int tz,
+                                                   int row, int bx, int by) {
     // threads flattened over the plane's (float4 group, y), `row` threads per y:
     // the group count on short rows (full warps), a whole number of warps on
     // long ones (a warp's coarse reads stay on one row)
-    const unsigned t = blockIdx.x * (kProTX * kProTY) + threadIdx.x;
+    const unsigned t = bx * (kProTX * kProTY) + threadIdx.x;
     const int groups = (n + 3) / 4;
     const int y = (int)(t / (unsigned)row), k = (int)(t - (unsigned)y * row);
     if (y >= n || k >= groups) return;
     const int x = 4 * k;
-    const int z0 = blockIdx.y * tz, z1 = min(n, z0 + tz);
+    const int z0 = by * tz, z1 = min(n, z0 + tz);
     const int ya = y >> 1, yb = min(ya + 1, cn - 1);
     const float ty = (y & 1) ? 0.5f : 0.f;
     const int64_t cplane = (int64_t)(cn + 2) * cP;
@@ -345,6 +374,26 @@ __global__ void __launch_bounds__(kProTX* kProTY) prolong_add32_kernel(const flo
     }
 }
 
+__global__ void __launch_bounds__(kProTX* kProTY) prolong_add32_kernel(const float* __restrict__ c,
+                                                                       float* __restrict__ f,
+                                                                       const float* __restrict__ w, int n, int P,
+                                                                       int cn, int cP, int tz, int row) {
+    prolong_add32_body(c, f, w, n, P, cn, cP, tz, row, blockIdx.x, blockIdx.y);
+}
+
+// Grouped (batch.cuh): ptr[0] = coarse, ptr[1] = fine, ptr[2] = weights;
+// aux[0] = planes per block, aux[1] = threads per row.
+__global__ void __launch_bounds__(kProTX* kProTY) prolong_add32_grouped_kernel(const batch::GridDesc* __restrict__ descs,
+                                                                               int count,
+                                                                               const int* __restrict__ flags) {
+    int bx, by, bz;
+    const batch::GridDesc& d = batch::locate(descs, count, blockIdx.x, bx, by, bz);
+    if (!batch::cloud_active(flags, d.cloud)) return;
+    const int n = (int)d.n, cn = (n + 1) / 2;
+    prolong_add32_body((const float*)d.ptr[0], (float*)d.ptr[1], (const float*)d.ptr[2], n, ((n + 5) + 7) & ~7, cn,
+                       ((cn + 5) + 7) & ~7, (int)d.aux[0], (int)d.aux[1], bx, by);
+}
+
 }  // namespace pb
 
 using namespace pb;
@@ -370,6 +419,7 @@ extern "C" int pb_sweep_tma_f32(const float* e_in, float* e_out, const float* rh
     prm.ntx = (N - 1) / kTX > 0 ? (N - 1) / kTX : 1;
     prm.nty = (N - 1) / kTY > 0 ? (N - 1) / kTY : 1;
     const int tiles = prm.ntx * prm.nty;
+    if (z_chunk <= 0) z_chunk = tuned(PB_TUNE_SWEEP_Z_CHUNK, n, 0);
     if (z_chunk <= 0) {
         // c chunks per tile: minimise waves x (planes per chunk + the 4 planes a
         // chunk loads beyond its range), waves = ceil(tiles c / (2 blocks x 148
@@ -421,10 +471,79 @@ extern "C" int pb_prolong_fac_f32(const float* coarse, float* fine, const float*
     const int gxy = (row * n + kProTX * kProTY - 1) / (kProTX * kProTY);
     // planes per block: as many as keep at least 4 blocks per SM, at most kProTZ
     const int64_t fill = (int64_t)gxy * n / (4 * kSMs);
-    const int tz = fill < 1 ? 1 : (fill > kProTZ ? kProTZ : (int)fill);
+    const int tz = (int)tuned(PB_TUNE_PROLONG_PLANES, n, fill < 1 ? 1 : (fill > kProTZ ? kProTZ : fill));
     const dim3 grid(gxy, (n + tz - 1) / tz);
     prolong_add32_kernel<<<grid, kProTX * kProTY, 0, (cudaStream_t)stream>>>(coarse, fine, weights, n, pitch_for(n),
                                                                               cn, pitch_for(cn), tz, row);
     PB_CHECK_LAUNCH("prolong_add32_kernel");
     return PB_OK;
 }
+
+// ---- grouped launches (batch.cuh) ----------------------------------------------------
+
+namespace pb {
+namespace batch {
+
+// Level-0 sweep of one grid: ptr[0] e_in (ignored from zero), ptr[1] e_out,
+// ptr[2] rhs, ptr[3] 1/D, ptr[4] status word; z_chunk <= 0: whole planes.
+int describe_sweep(GridDesc& d, bool zero_in, int64_t z_chunk) {
+    using namespace pb::tma;
+    const int N = (int)d.n;
+    if (N < 33 || N > 4097 || ((N - 1) & (N - 2)))
+        return fail(PB_ERR_INVALID, "batch sweep: side must be 2^k + 1 >= 33 (got %d)", N);
+    const float* e_in = (const float*)d.ptr[0];
+    const float* rhs = (const float*)d.ptr[2];
+    const float* invD = (const float*)d.ptr[3];
+    if ((!zero_in && !e_in) || !d.ptr[1] || !rhs || !invD || !d.ptr[4] || e_in == d.ptr[1])
+        return fail(PB_ERR_INVALID, "batch sweep: bad operands");
+    const int P = pitch_for(N);
+    PB_TRY(make_map(&d.map[0], zero_in ? rhs : e_in, N, P, kBoxY));
+    PB_TRY(make_map(&d.map[1], rhs, N, P, kBoxY));
+    PB_TRY(make_map(&d.map[2], invD, N, P, kBoxY));
+    const int zc = z_chunk <= 0 || z_chunk > N ? N : (int)z_chunk;
+    d.gx = (N - 1) / kTX > 0 ? (N - 1) / kTX : 1;
+    d.gy = (N - 1) / kTY > 0 ? (N - 1) / kTY : 1;
+    d.gz = (N + zc - 1) / zc;
+    d.aux[0] = zc;
+    d.ptr[0] = d.ptr[1];  // e_out, as the grouped kernel reads it
+    d.ptr[1] = d.ptr[4];  // status
+    return PB_OK;
+}
+
+int launch_sweep(const GridDesc* descs, int count, int64_t blocks, bool zero_in, const int* flags, cudaStream_t s) {
+    using namespace pb::tma;
+    const size_t smem = sizeof(Geo2<kTY, kSlots>::Smem) + 128;
+    auto go = [&](auto kernel) -> int {
+        PB_CHECK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                      "batch sweep smem");
+        kernel<<<(unsigned)blocks, kThreads, smem, s>>>(descs, count, flags);
+        PB_CHECK_LAUNCH("sweep_grouped_kernel");
+        return PB_OK;
+    };
+    return zero_in ? go(sweep_grouped_kernel<true, kSlots>) : go(sweep_grouped_kernel<false, kSlots>);
+}
+
+// fine += s * trilinear(coarse): ptr[0] coarse, ptr[1] fine, ptr[2] weights.
+int describe_prolong32(GridDesc& d) {
+    const int n = (int)d.n;
+    if (n < 3 || n > 4097 || !d.ptr[0] || !d.ptr[1] || !d.ptr[2]) return fail(PB_ERR_INVALID, "batch prolong: bad args");
+    const int groups = (n + 3) / 4;
+    const int row = groups < 64 ? groups : (groups + 31) / 32 * 32;
+    const int gxy = (row * n + kProTX * kProTY - 1) / (kProTX * kProTY);
+    const int tz = (int)tuned(PB_TUNE_PROLONG_PLANES, n, n < kProTZ ? n : kProTZ);
+    d.gx = gxy;
+    d.gy = (n + tz - 1) / tz;
+    d.gz = 1;
+    d.aux[0] = tz;
+    d.aux[1] = row;
+    return PB_OK;
+}
+
+int launch_prolong32(const GridDesc* descs, int count, int64_t blocks, const int* flags, cudaStream_t s) {
+    prolong_add32_grouped_kernel<<<(unsigned)blocks, kProTX * kProTY, 0, s>>>(descs, count, flags);
+    PB_CHECK_LAUNCH("prolong_add32_grouped_kernel");
+    return PB_OK;
+}
+
+}  // namespace batch
+}  // namespace pb

@@ -44,6 +44,7 @@ import threading
 import torch
 
 from . import _native as nat
+from . import _sync
 from .solver import SolveStats, level_sizes, norm
 
 COARSE_N = 9  # levels of this side or smaller: one single-block launch
@@ -120,13 +121,25 @@ class Level32:
                 if t is not None] + list(self.packed or ())
 
 
+def galerkin_scratch_bytes(n: int, levels=None) -> int:
+    """Bytes of the Galerkin products' scratch for a hierarchy of side n."""
+    lib = nat.lib()
+    sizes = level_sizes(n) if levels is None else [lv.n for lv in levels]
+    first_seven = sizes[0] >= TMA_MIN_N
+    fine27 = [m for i, m in enumerate(sizes[:-1]) if not (i == 0 and first_seven)]
+    need = max([lib.pb_galerkin_workspace_size(m, 0) for m in fine27], default=0)
+    one_plane = max([27 * 4 * 3 * ((m + 1) // 2) * (m + (m + 1) // 2) for m in fine27], default=0)
+    return int(min(need, max(GALERKIN_SCRATCH, one_plane)))
+
+
 class Hierarchy32:
     """FP32 preconditioner levels.  Level 0 is the reference's operator (its
     red-black sweeps staged by TMA); the levels below are Galerkin operators
     P_s^T A P_s / 8 built on the device by `setup` (mg27.cu), down to 3^3,
     which is solved exactly with its inverse."""
 
-    def __init__(self, n: int, device: torch.device, z_chunk: int = 0, coarse_sweeps: int | None = None):
+    def __init__(self, n: int, device: torch.device, z_chunk: int = 0, coarse_sweeps: int | None = None,
+                 galerkin_ws: torch.Tensor | None = None):
         self.status = torch.zeros(1, dtype=torch.int32, device=device)
         self.lib = nat.lib()
         self.device = device
@@ -139,12 +152,13 @@ class Hierarchy32:
             if not lv.seven:
                 lv.pack(device, self.lib)
         self.inverse = torch.zeros(27 * 27, dtype=torch.float32, device=device)  # of the 3^3 level
-        # scratch of the separable Galerkin products (27-point fine levels), at most GALERKIN_SCRATCH bytes
-        fine27 = [lv.n for lv in self.levels[:-1] if not lv.seven]
-        need = max([self.lib.pb_galerkin_workspace_size(m, 0) for m in fine27], default=0)
-        one_plane = max([27 * 4 * 3 * ((m + 1) // 2) * (m + (m + 1) // 2) for m in fine27], default=0)
-        size = min(need, max(GALERKIN_SCRATCH, one_plane))
-        self.galerkin_ws = torch.empty((size + 3) // 4, dtype=torch.float32, device=device)
+        # scratch of the separable Galerkin products (27-point fine levels), at most GALERKIN_SCRATCH bytes;
+        # hierarchies set up one after another on one stream may share one (galerkin_ws)
+        size = galerkin_scratch_bytes(n, self.levels)
+        if galerkin_ws is not None and galerkin_ws.numel() * 4 >= size:
+            self.galerkin_ws = galerkin_ws
+        else:
+            self.galerkin_ws = torch.empty((size + 3) // 4, dtype=torch.float32, device=device)
         # levels of side <= COARSE_N: one block from their image (couplings, 1/diagonal, weights, inverse)
         tail = self.levels[self.first_coarse:]
         k = len(tail)
@@ -255,6 +269,24 @@ class Hierarchy32:
         return src
 
 
+_TUNED: set = set()
+
+
+def apply_tuning(lib, n: int, device: torch.device) -> None:
+    """Load the autotuner's cached launch parameters for side n on this GPU
+    (tune.py) into the library's table, once per (device, side); skipped when
+    MPR_B200_TUNE=0."""
+    import os
+
+    key = (device.index, n)
+    if key in _TUNED or os.environ.get("MPR_B200_TUNE", "1") == "0":
+        return
+    from . import tune
+
+    tune.apply(lib, tune.gpu_name(device), n)
+    _TUNED.add(key)
+
+
 class RefinedEngine:
     """FCG(1) state for one grid side and point weight, reused across solves.
 
@@ -266,6 +298,7 @@ class RefinedEngine:
         self.pw = float(point_weight)
         self.device = device
         self.lib = nat.lib()
+        apply_tuning(self.lib, n, device)  # before any launch shape is captured
         # Graph capture needs a stream other than the legacy default stream;
         # the engine's buffers are allocated on it and it runs every solve.
         self.stream = torch.cuda.Stream(device=device)
@@ -399,6 +432,7 @@ class RefinedEngine:
         self.screen.copy_(screen)
         self.b.copy_(rhs)
         self._run_prologue()
+        _sync.wait("solver prologue")
         both = torch.cat([self.norm2, self.bnorm]).cpu()
         stats.rhs_norm = float(both[1])
         r = math.sqrt(max(float(both[0]), 0.0))
@@ -423,6 +457,7 @@ class RefinedEngine:
                     self._start()
                     self._capture()
                 nat.check(L.pb_graph_launch(self.exec, s), "graph launch")
+            _sync.wait("solver iterations")
             tail = torch.cat([self.flags[1:2].to(torch.float64), self.scal[4:5]]).cpu()
             it = int(tail[0])
             if not EAGER_LOOP:

@@ -77,3 +77,66 @@ def test_build_entry_compiles_sm100a():
 
     assert buildlib.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
     assert os.path.exists(buildlib.build())
+
+
+def _describe(lib, kind, sides, ptrs, aux=None, clouds=None):
+    import numpy as np
+
+    count = len(sides)
+    clouds = np.arange(count, dtype=np.int64) if clouds is None else np.asarray(clouds, np.int64)
+    sides = np.asarray(sides, np.int64)
+    p = np.zeros((count, 12), np.uint64)
+    for i, row in enumerate(ptrs):
+        p[i, :len(row)] = row
+    a = np.zeros((count, 4), np.int64) if aux is None else np.asarray(aux, np.int64)
+    nbytes = int(lib.pb_batch_desc_bytes(count))
+    raw = np.zeros(nbytes + 64, np.uint8)
+    off = (-raw.ctypes.data) % 64
+    blocks = ctypes.c_int64(-1)
+    status = lib.pb_batch_describe(kind, count, clouds.ctypes.data, sides.ctypes.data, p.ctypes.data, a.ctypes.data,
+                                   0, raw[off:].ctypes.data, nbytes, ctypes.byref(blocks))
+    return status, blocks.value
+
+
+def test_batch_descriptors_count_blocks_on_the_host():
+    """pb_batch_describe (no GPU needed for the non-TMA kinds): a grouped
+    launch's blocks are the sum of each grid's own launch grid."""
+    from mojo_poissonrecon_b200 import _native
+
+    lib = _native.lib()
+    fake = [0x1000 * (k + 1) for k in range(12)]
+    # packed relaxation: grid ((Pc*n + 255)/256, n), Pc = (n+1)/2
+    sides = [17, 33, 65, 129]
+    status, blocks = _describe(lib, 4, sides, [fake[:7]] * 4)
+    assert status == 0, lib.pb_last_error()
+    assert blocks == sum(((n + 1) // 2 * n + 255) // 256 * n for n in sides)
+    # residual + restriction of level 0: (cn/64, cn/4, cn/4) coarse tiles
+    status, blocks = _describe(lib, 3, [257, 33], [fake[:5]] * 2)
+    assert status == 0
+    assert blocks == sum(-(-c // 64) * -(-c // 4) * -(-c // 4) for c in (129, 17))
+    # FCG pass 2: (n/32, n/8, n/24) tiles; pass-1 blocks match pb_batch_fcg_blocks
+    status, blocks = _describe(lib, 11, [257], [fake[:10]])
+    assert status == 0 and blocks == lib.pb_batch_fcg_blocks(257, 1) == 9 * 33 * 11
+    status, blocks = _describe(lib, 9, [65, 257], [fake[:6]] * 2)
+    assert blocks == lib.pb_batch_fcg_blocks(65, 0) + lib.pb_batch_fcg_blocks(257, 0)
+    # one block per cloud for the reductions and the coarse cycle
+    status, blocks = _describe(lib, 10, [65, 257, 33], [fake[:2]] * 3, aux=[[5, 0, 0, 0]] * 3)
+    assert status == 0 and blocks == 3
+    status, blocks = _describe(lib, 8, [9, 9], [fake[:3]] * 2, aux=[[1, 1, 1, 0]] * 2)
+    assert status == 0 and blocks == 2
+    assert lib.pb_batch_fcg_partials(257) >= 4 * lib.pb_batch_fcg_blocks(257, 0)
+
+
+def test_batch_descriptors_reject_bad_grids():
+    from mojo_poissonrecon_b200 import _native
+
+    lib = _native.lib()
+    fake = [0x1000 * (k + 1) for k in range(12)]
+    assert _describe(lib, 4, [17], [fake[:6]])[0] == 1  # a missing operand
+    assert _describe(lib, 4, [18], [fake[:7]])[0] == 1  # not 2^k + 1
+    assert _describe(lib, 8, [9, 5], [fake[:3]] * 2, aux=[[1, 1, 1, 0]] * 2)[0] == 1  # mixed coarse sides
+    assert b"same side" in lib.pb_last_error()
+    assert _describe(lib, 8, [9], [fake[:3]], aux=[[65, 1, 1, 0]])[0] == 1  # sweep count out of range
+    assert _describe(lib, 99, [9], [fake])[0] == 1
+    assert _describe(lib, 4, [17], [fake[:7]], clouds=[-1])[0] == 1
+    assert lib.pb_batch_launch(4, None, 1, 1, None, 0, None) == 1

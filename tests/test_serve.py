@@ -1,5 +1,7 @@
 """Continuous batching: admission by HBM footprint, overlap of requests that
-arrive while others run, and identical results alone and in the mix."""
+arrive while others run, batches formed from whatever is queued, host-side
+failure handling (deadlines, cancellation, allocator refusal, one bad request
+in a batch), and identical results alone and in the mix."""
 
 import threading
 import time
@@ -37,7 +39,7 @@ class FakeGPU:
 def make_server(lanes, budget, delay=0.05):
     ref = []
     fake = FakeGPU(ref, delay)
-    server = serve.Server(lanes=lanes, budget_bytes=budget, runner=fake)
+    server = serve.Server(lanes=lanes, budget_bytes=budget, runner=fake, max_batch=1)
     ref.append(server)
     return server, fake
 
@@ -86,13 +88,208 @@ def test_failures_are_reported_and_serving_continues():
             raise ValueError("bad request")
         return kw["tag"]
 
-    server = serve.Server(lanes=1, budget_bytes=1 << 40, runner=runner)
+    server = serve.Server(lanes=1, budget_bytes=1 << 40, runner=runner, max_batch=1)
     bad = server.submit(np.zeros((1, 3)), np.ones((1, 3)), depth=5, tag="bad")
     good = server.submit(np.zeros((1, 3)), np.ones((1, 3)), depth=5, tag="good")
     with pytest.raises(ValueError):
         bad.result(timeout=10)
     assert good.result(timeout=10)[0] == "good"
     server.close()
+
+
+class FakeBatchGPU:
+    """Stands in for the batched device path: records every batch's tags."""
+
+    def __init__(self, delay=0.05, fail_tag=None, oom_batches=0):
+        self.lock = threading.Lock()
+        self.batches = []
+        self.delay = delay
+        self.fail_tag = fail_tag
+        self.oom_batches = oom_batches
+
+    def __call__(self, items):
+        tags = [kw["tag"] for _, _, kw in items]
+        with self.lock:
+            self.batches.append(tags)
+            oom = self.oom_batches > 0 and len(items) > 1
+            if oom:
+                self.oom_batches -= 1
+        if oom:
+            raise MemoryError("simulated device allocation refusal")
+        if self.fail_tag in tags:
+            raise ValueError("one request of the batch is bad")
+        time.sleep(max(kw.get("sleep", self.delay) for _, _, kw in items))
+        return tags
+
+
+def cloud():
+    return np.zeros((10, 3)), np.ones((10, 3))
+
+
+def test_queued_requests_form_the_next_batch():
+    fake = FakeBatchGPU(delay=0.3)
+    server = serve.Server(lanes=1, budget_bytes=1 << 40, batch_runner=fake, max_batch=8)
+    first = server.submit(*cloud(), depth=6, tag=0)
+    time.sleep(0.1)  # the first batch (one request) is on the "device"
+    rest = [server.submit(*cloud(), depth=6 + (k % 2), tag=k) for k in range(1, 6)]
+    assert first.result(timeout=10)[0] == 0
+    assert [f.result(timeout=10)[0] for f in rest] == [1, 2, 3, 4, 5]
+    server.close()
+    assert fake.batches == [[0], [1, 2, 3, 4, 5]]  # arrivals during a batch run together next
+
+
+def test_batches_respect_the_budget_and_max_batch():
+    fp = serve.footprint_bytes(7, 10)
+    fake = FakeBatchGPU(delay=0.05)
+    server = serve.Server(lanes=1, budget_bytes=3 * fp, batch_runner=fake, max_batch=8)
+    futures = [server.submit(*cloud(), depth=7, tag=k) for k in range(7)]
+    assert [f.result(timeout=10)[0] for f in futures] == list(range(7))
+    server.close()
+    assert max(len(b) for b in fake.batches) <= 3
+    assert sum(fake.batches, []) == list(range(7))  # FIFO
+
+
+def test_deadline_passes_while_queued():
+    fake = FakeBatchGPU(delay=0.4)
+    server = serve.Server(lanes=1, budget_bytes=1 << 40, batch_runner=fake, max_batch=1)
+    busy = server.submit(*cloud(), depth=6, tag="busy")
+    time.sleep(0.05)
+    late = server.submit(*cloud(), deadline=0.1, depth=6, tag="late")
+    ok = server.submit(*cloud(), depth=6, tag="ok")
+    with pytest.raises(serve._sync.DeadlineExceeded):
+        late.result(timeout=10)
+    assert busy.result(timeout=10)[0] == "busy" and ok.result(timeout=10)[0] == "ok"
+    server.close()
+    assert ["late"] not in fake.batches  # never started
+
+
+def test_deadline_during_a_device_wait():
+    """A device wait that never completes (a fake event) gives up at the
+    request's deadline; the lane then serves the next request."""
+    from mojo_poissonrecon_b200 import _sync
+
+    def runner(points, normals, **kw):
+        if kw["tag"] == "stuck":
+            _sync.poll(lambda: False, _sync.current_deadline(), "fake device work")
+        return kw["tag"]
+
+    server = serve.Server(lanes=1, budget_bytes=1 << 40, runner=runner, max_batch=1)
+    t0 = time.monotonic()
+    stuck = server.submit(*cloud(), deadline=0.2, depth=6, tag="stuck")
+    nxt = server.submit(*cloud(), depth=6, tag="next")
+    with pytest.raises(_sync.DeadlineExceeded):
+        stuck.result(timeout=10)
+    assert time.monotonic() - t0 < 5
+    assert nxt.result(timeout=10)[0] == "next"
+    server.close()
+
+
+def test_poll_gives_up_at_the_deadline_with_a_fake_clock():
+    from mojo_poissonrecon_b200 import _sync
+
+    now = [0.0]
+    sleeps = []
+
+    def sleep(dt):
+        sleeps.append(dt)
+        now[0] += dt
+
+    with pytest.raises(_sync.DeadlineExceeded):
+        _sync.poll(lambda: False, 0.01, "x", clock=lambda: now[0], sleep=sleep)
+    assert now[0] >= 0.01 and max(sleeps) <= 1e-3
+    calls = iter([False, False, True])
+    _sync.poll(lambda: next(calls), 1.0, "y", clock=lambda: 0.0, sleep=lambda dt: None)
+    assert _sync.current_deadline() is None
+    with _sync.deadline(5.0):
+        assert _sync.current_deadline() == 5.0
+    assert _sync.current_deadline() is None
+
+
+def test_cancelled_request_never_runs():
+    fake = FakeBatchGPU(delay=0.3)
+    server = serve.Server(lanes=1, budget_bytes=1 << 40, batch_runner=fake, max_batch=1)
+    busy = server.submit(*cloud(), depth=6, tag="busy")
+    time.sleep(0.05)
+    gone = server.submit(*cloud(), depth=6, tag="gone")
+    assert gone.cancel()
+    after = server.submit(*cloud(), depth=6, tag="after")
+    assert busy.result(timeout=10)[0] == "busy" and after.result(timeout=10)[0] == "after"
+    server.close()
+    assert ["gone"] not in fake.batches
+
+
+def test_allocator_refusal_retries_one_at_a_time():
+    fake = FakeBatchGPU(delay=0.01, oom_batches=1)
+    server = serve.Server(lanes=1, budget_bytes=1 << 40, batch_runner=fake, max_batch=8)
+    gate = server.submit(*cloud(), depth=6, tag="gate", sleep=0.2)
+    time.sleep(0.05)
+    futures = [server.submit(*cloud(), depth=6, tag=k) for k in range(3)]
+    assert gate.result(timeout=10)[0] == "gate"
+    assert [f.result(timeout=10)[0] for f in futures] == [0, 1, 2]
+    server.close()
+    assert [0, 1, 2] in fake.batches and [0] in fake.batches and [2] in fake.batches
+
+
+def test_allocator_refusal_of_a_single_request_is_reported():
+    def runner(points, normals, **kw):
+        if kw["tag"] == "huge":
+            raise MemoryError("simulated device allocation refusal")
+        return kw["tag"]
+
+    server = serve.Server(lanes=1, budget_bytes=1 << 40, runner=runner, max_batch=4)
+    huge = server.submit(*cloud(), depth=6, tag="huge")
+    fine = server.submit(*cloud(), depth=6, tag="fine")
+    with pytest.raises(MemoryError):
+        huge.result(timeout=10)
+    assert fine.result(timeout=10)[0] == "fine"
+    server.close()
+
+
+def test_one_bad_request_fails_alone_inside_a_batch():
+    fake = FakeBatchGPU(delay=0.01, fail_tag="bad")
+    server = serve.Server(lanes=1, budget_bytes=1 << 40, batch_runner=fake, max_batch=8)
+    gate = server.submit(*cloud(), depth=6, tag="gate", sleep=0.2)
+    time.sleep(0.05)
+    futures = {t: server.submit(*cloud(), depth=6, tag=t) for t in ("a", "bad", "b")}
+    gate.result(timeout=10)
+    assert futures["a"].result(timeout=10)[0] == "a" and futures["b"].result(timeout=10)[0] == "b"
+    with pytest.raises(ValueError):
+        futures["bad"].result(timeout=10)
+    server.close()
+
+
+def test_footprint_model_counts_the_solver_levels():
+    # level 0 of side 257: six padded FP32 arrays; the model is dominated by the
+    # grids and the hierarchy at depth >= 8
+    n = 257
+    h = serve.hierarchy_bytes(n)
+    assert h > 6 * 4 * n ** 3
+    assert h < 12 * 4 * n ** 3
+    assert serve.footprint_bytes(8, 0) > 4 * 8 * n ** 3 + h
+
+
+@pytest.mark.gpu
+def test_footprint_model_bounds_the_measured_peak():
+    """The admission model against torch's peak allocation of one batched
+    reconstruction per depth (within -10 % .. +40 %)."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from mojo_poissonrecon_b200 import batch, solver32, workloads
+
+    rng = np.random.default_rng(3)
+    for depth, count in ((6, 20_000), (7, 50_000), (8, 200_000)):
+        p, n = workloads.torus(count, noise=0.0, confidence=None, rng=rng)
+        solver32.clear_engines()
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        base = torch.cuda.memory_allocated()
+        torch.cuda.reset_peak_memory_stats()
+        batch.reconstruct_many([(p, n, depth)], tol=1e-8)
+        torch.cuda.synchronize()
+        peak = torch.cuda.max_memory_allocated() - base
+        model = serve.footprint_bytes(depth, count)
+        assert 0.9 * peak <= model <= 1.4 * peak, (depth, peak, model)
 
 
 @pytest.mark.gpu
@@ -114,7 +311,10 @@ def test_same_result_alone_and_in_the_mix():
             p, n = workloads.torus(size, noise=0.0, confidence=None, rng=rng)
         clouds.append((p, n, depth))
     alone = [mpr.reconstruct(p, n, depth=d, precision="fp32_refined", tol=1e-8) for p, n, d in clouds]
-    mixed = serve.reconstruct_batch(clouds, lanes=3)
+    mixed = serve.reconstruct_batch(clouds, lanes=3)  # batches of whatever is queued
+    single = serve.reconstruct_batch(clouds, lanes=3, max_batch=1)  # one reconstruction per lane
+    for a, b in zip(alone, single):
+        assert np.array_equal(a.vertices, b.vertices) and np.array_equal(a.faces, b.faces)
     for a, b in zip(alone, mixed):
         assert np.array_equal(a.vertices, b.vertices)
         assert np.array_equal(a.faces, b.faces)
