@@ -139,7 +139,10 @@ class Hierarchy32:
     which is solved exactly with its inverse."""
 
     def __init__(self, n: int, device: torch.device, z_chunk: int = 0, coarse_sweeps: int | None = None,
-                 galerkin_ws: torch.Tensor | None = None):
+                 galerkin_ws: torch.Tensor | None = None, transient_coef: bool = False):
+        """transient_coef: packed levels keep their 14 coefficient planes only
+        during `setup` (allocated there, freed once packed), which saves their
+        memory between solves at the cost of a fill per set-up."""
         self.status = torch.zeros(1, dtype=torch.int32, device=device)
         self.lib = nat.lib()
         self.device = device
@@ -148,9 +151,12 @@ class Hierarchy32:
         self.sizes = level_sizes(n)
         self.levels = [Level32(m, device, self.lib, i == 0) for i, m in enumerate(self.sizes)]
         self.first_coarse = next(i for i, m in enumerate(self.sizes) if m <= COARSE_N)
+        self.transient_coef = bool(transient_coef)
         for lv in self.levels[:self.first_coarse]:
             if not lv.seven:
                 lv.pack(device, self.lib)
+                if self.transient_coef:
+                    lv.coef = None
         self.inverse = torch.zeros(27 * 27, dtype=torch.float32, device=device)  # of the 3^3 level
         # scratch of the separable Galerkin products (27-point fine levels), at most GALERKIN_SCRATCH bytes;
         # hierarchies set up one after another on one stream may share one (galerkin_ws)
@@ -190,18 +196,27 @@ class Hierarchy32:
         nat.check(L.pb_level_setup_f32(screen.data_ptr(), top.n, self.pw, top.D.data_ptr(), top.invD.data_ptr(),
                                        top.weights.data_ptr(), s), "level setup")
         if not top.seven:
+            if top.coef is None:
+                top.coef = torch.zeros(14, top.count, dtype=torch.float32, device=self.device)
             nat.check(L.pb_level27_from7_f32(top.D.data_ptr(), top.n, top.coef.data_ptr(), s), "level27 from 7")
             nat.check(L.pb_level27_finish_f32(top.coef.data_ptr(), top.n, top.invD.data_ptr(),
                                               top.weights.data_ptr(), s), "level27 finish")
+        def planes(lv):  # zero-filled: the kernels write interior nodes only
+            if lv.coef is None:
+                lv.coef = torch.zeros(14, lv.count, dtype=torch.float32, device=self.device)
+            return lv.coef
+
         for fine, lv in zip(self.levels[:-1], self.levels[1:]):
             src, seven = (fine.D, 1) if fine.seven else (fine.coef, 0)
-            nat.check(L.pb_galerkin_f32(src.data_ptr(), fine.n, seven, fine.weights.data_ptr(), lv.coef.data_ptr(),
-                                        self.galerkin_ws.data_ptr(), self.galerkin_ws.numel() * 4, s), "galerkin")
+            nat.check(L.pb_galerkin_f32(src.data_ptr(), fine.n, seven, fine.weights.data_ptr(),
+                                        planes(lv).data_ptr(), self.galerkin_ws.data_ptr(),
+                                        self.galerkin_ws.numel() * 4, s), "galerkin")
             nat.check(L.pb_level27_finish_f32(lv.coef.data_ptr(), lv.n, lv.invD.data_ptr(), lv.weights.data_ptr(), s),
                       "level27 finish")
-        for lv in self.levels:
-            if lv.packed is not None:
-                nat.check(L.pb_pack27_f32(lv.coef.data_ptr(), lv.n, *lv.packed_ptrs(), s), "pack27")
+            if fine.packed is not None:  # its planes are read for the last time by the product above
+                nat.check(L.pb_pack27_f32(fine.coef.data_ptr(), fine.n, *fine.packed_ptrs(), s), "pack27")
+                if self.transient_coef:
+                    fine.coef = None
         nat.check(L.pb_coarse_inverse_f32(self.levels[-1].coef.data_ptr(), 3, self.inverse.data_ptr(), s),
                   "coarse inverse")
         nat.check(L.pb_coarse27_image_f32(*self._image_args, s), "coarse image")
@@ -287,17 +302,28 @@ def apply_tuning(lib, n: int, device: torch.device) -> None:
     _TUNED.add(key)
 
 
+LEAN_MIN_N = 513  # engines of this side or larger run lean (RefinedEngine)
+
+
 class RefinedEngine:
     """FCG(1) state for one grid side and point weight, reused across solves.
+
+    Lean engines (side >= LEAN_MIN_N, where a grid is 1 GB and more) keep
+    between solves only the hierarchy's operators: they solve on the caller's
+    rhs and screen in place instead of copies, hand the final iterate out
+    instead of a clone, release the FCG vectors after each solve, keep the
+    packed levels' coefficient planes only during set-up, and re-capture the
+    iteration graph per solve (its pointers change), with an eager prologue.
 
     Not thread-safe: one engine serves one stream at a time (the batch and
     serving paths create one engine per concurrent slot)."""
 
-    def __init__(self, n: int, point_weight: float, device: torch.device):
+    def __init__(self, n: int, point_weight: float, device: torch.device, lean: bool | None = None):
         self.n = n
         self.pw = float(point_weight)
         self.device = device
         self.lib = nat.lib()
+        self.lean = n >= LEAN_MIN_N if lean is None else bool(lean)
         apply_tuning(self.lib, n, device)  # before any launch shape is captured
         # Graph capture needs a stream other than the legacy default stream;
         # the engine's buffers are allocated on it and it runs every solve.
@@ -306,12 +332,13 @@ class RefinedEngine:
             self._allocate(n, device)
 
     def _allocate(self, n: int, device: torch.device) -> None:
-        self.h = Hierarchy32(n, device)
-        f64 = lambda: torch.empty((n, n, n), dtype=torch.float64, device=device)
-        self.screen, self.b = f64(), f64()
-        self.xs = (f64(), f64())  # iterate, alternating by iteration parity
-        f32 = lambda: torch.empty((n, n, n), dtype=torch.float32, device=device)
-        self.ps = (f32(), f32())  # search direction (stored in FP32), alternating by iteration parity
+        self.h = Hierarchy32(n, device, transient_coef=self.lean)
+        if self.lean:
+            self.screen = self.b = None  # bound per solve
+            self.xs = self.ps = None  # allocated per solve
+        else:
+            self.screen, self.b = self._f64(), self._f64()
+            self._vectors()
         self.scal = torch.zeros(8, dtype=torch.float64, device=device)
         self.ctrl = torch.zeros(2, dtype=torch.float64, device=device)
         self.flags = torch.zeros(4, dtype=torch.int32, device=device)
@@ -326,8 +353,23 @@ class RefinedEngine:
         self.graph = ctypes.c_void_p()
         self.exec = ctypes.c_void_p()
         self.setup_graph = None
+        self._warm = False
         self.prologue_launches = 0
         self.body_launches = 0
+
+    def _f64(self) -> torch.Tensor:
+        return torch.empty((self.n,) * 3, dtype=torch.float64, device=self.device)
+
+    def _vectors(self) -> None:
+        n, device = self.n, self.device
+        self.xs = (self._f64(), self._f64())  # iterate, alternating by iteration parity
+        f32 = lambda: torch.empty((n, n, n), dtype=torch.float32, device=device)
+        self.ps = (f32(), f32())  # search direction (stored in FP32), alternating by iteration parity
+
+    def _drop_graph(self) -> None:
+        if self.exec.value or self.graph.value:
+            self.lib.pb_graph_destroy(self.exec, self.graph)
+        self.exec, self.graph = ctypes.c_void_p(), ctypes.c_void_p()
 
     def __del__(self):
         try:
@@ -337,8 +379,9 @@ class RefinedEngine:
             pass
 
     def nbytes(self) -> int:
-        return sum(t.numel() * t.element_size() for t in (self.screen, self.b) + self.xs + self.ps) + \
-            self.h.nbytes()
+        owned = [t for t in (self.screen, self.b) if t is not None and not self.lean]
+        owned += list(self.xs or ()) + list(self.ps or ())
+        return sum(t.numel() * t.element_size() for t in owned) + self.h.nbytes()
 
     def _iteration(self, handle: int) -> None:
         L, s = self.lib, nat.stream_handle()
@@ -390,10 +433,16 @@ class RefinedEngine:
         work (rhs, screen) and before its later work (the returned field)."""
         caller = torch.cuda.current_stream(self.device)
         self.stream.wait_stream(caller)
+        if self.lean:
+            rhs.record_stream(self.stream)
+            screen.record_stream(self.stream)
         with torch.cuda.stream(self.stream):
             x, stats = self._solve(rhs, screen, tol, max_cycles)
-            x = x.clone()
+            if not self.lean:
+                x = x.clone()
         caller.wait_stream(self.stream)
+        if self.lean:
+            x.record_stream(caller)  # allocated on the engine's stream, used on the caller's from here
         return x, stats
 
     def _prologue(self) -> None:
@@ -408,8 +457,9 @@ class RefinedEngine:
         """The prologue as one graph launch: its ~45 launches touch the same
         pointers on every solve, so they are captured once per engine (after one
         eager run that sets kernel attributes and loads the modules) and
-        replayed, which takes their host launch cost off small solves."""
-        if not SETUP_GRAPH or EAGER_LOOP:
+        replayed, which takes their host launch cost off small solves.  Lean
+        engines run it eagerly (their pointers change per solve)."""
+        if not SETUP_GRAPH or EAGER_LOOP or self.lean:
             self._prologue()
             return
         if self.setup_graph is None:
@@ -429,8 +479,24 @@ class RefinedEngine:
     def _solve(self, rhs: torch.Tensor, screen: torch.Tensor, tol: float, max_cycles: int):
         L, s = self.lib, nat.stream_handle()
         stats = SolveStats()
-        self.screen.copy_(screen)
-        self.b.copy_(rhs)
+        if self.lean:
+            self.screen, self.b = screen, rhs
+            self._vectors()
+            self._drop_graph()
+        else:
+            self.screen.copy_(screen)
+            self.b.copy_(rhs)
+        try:
+            x, stats = self._iterate(stats, tol, max_cycles)
+        finally:
+            if self.lean:  # nothing of this solve stays bound to the engine
+                self.screen = self.b = None
+                self.xs = self.ps = None
+                self._drop_graph()
+        return x, stats
+
+    def _iterate(self, stats: SolveStats, tol: float, max_cycles: int):
+        L, s = self.lib, nat.stream_handle()
         self._run_prologue()
         _sync.wait("solver prologue")
         both = torch.cat([self.norm2, self.bnorm]).cpu()
@@ -451,10 +517,12 @@ class RefinedEngine:
                         break
             else:
                 if not self.exec.value:
-                    # one eager iteration first sets kernel attributes outside the
-                    # capture; its effect is discarded by restarting below
-                    self._iteration(0)
-                    self._start()
+                    if not self._warm:
+                        # one eager iteration first sets kernel attributes outside the
+                        # capture; its effect is discarded by restarting below
+                        self._iteration(0)
+                        self._start()
+                        self._warm = True
                     self._capture()
                 nat.check(L.pb_graph_launch(self.exec, s), "graph launch")
             _sync.wait("solver iterations")
