@@ -426,15 +426,24 @@ int pb_batch_loop_condition(unsigned long long handle, const double *scal, const
  *   PROLONG_PLANES         fine planes per block of pb_prolong_fac_f32
  *   FCG_DIRECTION_PLANES   planes per block of pb_fcg_direction_f64 (default 24, at least 8)
  *   FCG_UPDATE_PLANES      planes per block of pb_fcg_update_f64 (default 24, at least 8)
- * The same values apply to the grouped launches described after they are set.
- * value 0 clears an entry.  Results do not depend on these values. */
+ *   FCG_DIRECTION_VARIANT  register budget of pb_fcg_direction_f64: 0 = 4 resident
+ *                          blocks per SM, 1 = 6, 2 = 8
+ *   FCG_UPDATE_VARIANT     pb_fcg_update_f64: 0 = 5 resident blocks per SM,
+ *                          1 = 6 resident blocks per SM, 2 = 8, 3 = the next planes
+ *                          prefetched into shared memory by cp.async
+ * The plane counts also apply to the grouped launches described after they are
+ * set.  value 0 clears an entry.  Results do not depend on these values, except
+ * the FCG passes' planes per block: they shape the inner products' partial-sum
+ * trees, so another value changes results by rounding. */
 enum {
     PB_TUNE_SWEEP_Z_CHUNK = 0,
     PB_TUNE_RESTRICT_PLANES = 1,
     PB_TUNE_PROLONG_PLANES = 2,
     PB_TUNE_FCG_DIRECTION_PLANES = 3,
     PB_TUNE_FCG_UPDATE_PLANES = 4,
-    PB_TUNE_PARAMS = 5
+    PB_TUNE_FCG_DIRECTION_VARIANT = 5,
+    PB_TUNE_FCG_UPDATE_VARIANT = 6,
+    PB_TUNE_PARAMS = 7
 };
 int pb_tune_set(int64_t param, int64_t n, int64_t value);
 int64_t pb_tune_get(int64_t param, int64_t n);

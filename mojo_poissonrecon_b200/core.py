@@ -221,8 +221,11 @@ def _splat_assemble(ctx: _Context, points: torch.Tensor, normals: torch.Tensor, 
     L = ctx.lib
     n = (1 << depth) + 1
     count = points.shape[0]
-    grids = {k: torch.zeros((n, n, n), dtype=torch.float64, device=ctx.device)
+    grids = {k: torch.empty((n, n, n), dtype=torch.float64, device=ctx.device)
              for k in ("density", "vx", "vy", "vz", "screen", "rhs")}
+    # the splat accumulates into zeroed grids (core.py:229-236); assembly writes every rhs node
+    for k in ("density", "vx", "vy", "vz", "screen") if count else grids:
+        ctx.check(L.pb_fill_f64(grids[k].data_ptr(), n ** 3, 0.0, ctx.stream), "zero grid")
     accepted = torch.zeros(1, dtype=torch.int64, device=ctx.device)
     if count:
         ptr, size = ctx.ws.get(L.pb_splat_workspace_size(count, n))

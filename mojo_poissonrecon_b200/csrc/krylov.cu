@@ -128,7 +128,10 @@ __device__ __forceinline__ void direction_sums_body(const float* __restrict__ z,
         for (int k = 0; k < 4; ++k) part[4 * block + k] = v[k];
 }
 
-__global__ void __launch_bounds__(kThreads, 4) direction_sums_kernel(const float* __restrict__ z, Pad g,
+// MINB: resident blocks per SM the compiler must allow (register budget); the
+// autotuner picks among the compiled variants (PB_TUNE_FCG_DIRECTION_VARIANT).
+template <int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) direction_sums_kernel(const float* __restrict__ z, Pad g,
                                                                      const float* __restrict__ p0,
                                                                      const float* __restrict__ p1,
                                                                      const float* __restrict__ r32,
@@ -292,7 +295,158 @@ __device__ __forceinline__ void update_residual_body(const float* __restrict__ z
     if (lin_tid() == 0) part[block] = v[0];
 }
 
-__global__ void __launch_bounds__(kUThreads) update_residual_kernel(
+// ---- pass 2 with the next planes prefetched by cp.async -------------------------
+// The same arithmetic as update_residual_body, in the same order.  Each
+// thread copies the values it will read of plane k + 2 (its x, z, p, b and
+// screen, and its halo node's x, z, p) into its own shared-memory slots with
+// cp.async while it works on plane k, so two planes of loads are in flight per
+// thread without holding registers; a thread only reads its own slots, so
+// cp.async.wait_group suffices (the tile of new iterates keeps its barrier).
+constexpr int kRing = 3;
+
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ void update_residual_prefetch_body(
+    const float* __restrict__ z, Pad g, float* p0, float* p1, double* x0, double* x1, const double* __restrict__ b,
+    const double* __restrict__ screen, double pw, const double* __restrict__ scal, const int* __restrict__ flags,
+    float* __restrict__ r32, double* __restrict__ part, int tz, int tile_x, int tile_y, int tile_z, int64_t block) {
+    __shared__ double tiles[2][kUY + 2][kUX + 2];
+    __shared__ double shared[1][32];
+    __shared__ double rd[kRing][4][kUThreads];  // own x, b, screen; halo x
+    __shared__ float rf[kRing][4][kUThreads];   // own z, p; halo z, p
+    const int n = g.n;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kUX + tx;
+    const int bx = tile_x * kUX, by = tile_y * kUY;
+    const int x = bx + tx, y = by + ty;
+    const int z0 = tile_z * tz, z1 = min(n, z0 + tz);
+    const double h = (double)(n - 1), h2 = h * h;
+    const int odd = flags[1] & 1;
+    const bool first = flags[0] != 0;
+    const float* __restrict__ pp = odd ? p1 : p0;
+    float* __restrict__ pn = odd ? p0 : p1;
+    const double* __restrict__ xc = odd ? x1 : x0;
+    double* __restrict__ xn = odd ? x0 : x1;
+    const double beta = first ? 0.0 : scal[1], alpha = scal[2];
+    const int64_t nn = (int64_t)n * n;
+    auto dir_at = [&](int64_t ii, int64_t cc) -> double {
+        double val = (double)z[cc];
+        if (!first) val -= beta * (double)pp[ii];
+        return val;
+    };
+    auto dir_of = [&](float zv, float pv) -> double {  // dir_at from prefetched values
+        double val = (double)zv;
+        if (!first) val -= beta * (double)pv;
+        return val;
+    };
+    const Halo hl(tid, bx, by);
+    const bool halo_in = hl.inside(n);
+    const bool inside = x < n && y < n;
+    const int64_t i0 = inside ? (int64_t)z0 * nn + (int64_t)y * n + x : 0;
+    const int64_t c0 = inside ? g.at(x, y, z0) : 0;
+    const int64_t hi0 = halo_in ? (int64_t)z0 * nn + (int64_t)hl.hy * n + hl.hx : 0;
+    const int64_t hc0 = halo_in ? g.at(hl.hx, hl.hy, z0) : 0;
+    auto issue = [&](int p) {  // plane p's values into slot p % kRing, one commit group
+        const int sl = p % kRing;
+        const int64_t dz = p - z0;
+        if (inside && p < n && p <= z1) {  // own x, z, p of planes z0 .. z1 (z1: the last plane's upper neighbour)
+            const int64_t ip = i0 + dz * nn, cq = c0 + dz * g.plane;
+            cp_async8(&rd[sl][0][tid], xc + ip);
+            cp_async4(&rf[sl][0][tid], z + cq);
+            if (!first) cp_async4(&rf[sl][1][tid], pp + ip);
+            if (p < z1) {
+                cp_async8(&rd[sl][1][tid], b + ip);
+                cp_async8(&rd[sl][2][tid], screen + ip);
+            }
+        }
+        if (halo_in && p < z1) {
+            const int64_t hp = hi0 + dz * nn, hq = hc0 + dz * g.plane;
+            cp_async8(&rd[sl][3][tid], xc + hp);
+            cp_async4(&rf[sl][2][tid], z + hq);
+            if (!first) cp_async4(&rf[sl][3][tid], pp + hp);
+        }
+        cp_commit();
+    };
+    issue(z0);
+    issue(z0 + 1);
+    cp_wait<1>();
+    double dm = 0.0, xm = 0.0, xb = 0.0;
+    if (inside) {
+        const int sl = z0 % kRing;
+        dm = dir_of(rf[sl][0][tid], rf[sl][1][tid]);
+        xm = rd[sl][0][tid] + alpha * dm;
+        xb = z0 > 0 ? xc[i0 - nn] + alpha * dir_at(i0 - nn, c0 - g.plane) : 0.0;
+    }
+    int64_t i = i0, c = c0;
+    const int degxy = (x > 0) + (x + 1 < n) + (y > 0) + (y + 1 < n);
+    double v[1] = {0.0};
+    for (int k = z0; k < z1; ++k) {
+        issue(k + 2);  // into the slot of plane k - 1, read for the last time before the previous barrier
+        cp_wait<1>();  // planes up to k + 1 have landed
+        const int sk = k % kRing, sn = (k + 1) % kRing;
+        const double hv = halo_in ? rd[sk][3][tid] + alpha * dir_of(rf[sk][2][tid], rf[sk][3][tid]) : 0.0;
+        const bool up = k + 1 < n;
+        double da = 0.0, xa = 0.0, bi = 0.0, sc = 0.0;
+        if (inside) {
+            if (up) {
+                da = dir_of(rf[sn][0][tid], rf[sn][1][tid]);
+                xa = rd[sn][0][tid] + alpha * da;
+            }
+            bi = rd[sk][1][tid];
+            sc = rd[sk][2][tid];
+        }
+        double(*tile)[kUX + 2] = tiles[k & 1];
+        tile[ty + 1][tx + 1] = inside ? xm : 0.0;
+        if (hl.has) tile[hl.sy][hl.sx] = hv;
+        __syncthreads();
+        if (inside) {
+            double s = 0.0;
+            s += tile[ty + 1][tx];
+            s += tile[ty + 1][tx + 2];
+            s += tile[ty][tx + 1];
+            s += tile[ty + 2][tx + 1];
+            s += xb;
+            s += xa;
+            const int deg = degxy + (k > 0) + up;
+            pn[i] = (float)dm;
+            xn[i] = xm;
+            const double r = bi - (((double)deg * h2 + pw * sc * h2) * xm - s * h2);
+            r32[c] = (float)r;
+            v[0] += r * r;
+            i += nn;
+            c += g.plane;
+        }
+        xb = xm;
+        xm = xa;
+        dm = da;
+    }
+    cp_wait<0>();
+    block_sums<1>(v, shared);
+    if (lin_tid() == 0) part[block] = v[0];
+}
+
+__global__ void __launch_bounds__(kUThreads) update_residual_prefetch_kernel(
+    const float* __restrict__ z, Pad g, float* p0, float* p1, double* x0, double* x1, const double* __restrict__ b,
+    const double* __restrict__ screen, double pw, const double* __restrict__ scal, const int* __restrict__ flags,
+    float* __restrict__ r32, double* __restrict__ part, int tz) {
+    update_residual_prefetch_body(z, g, p0, p1, x0, x1, b, screen, pw, scal, flags, r32, part, tz, blockIdx.x,
+                                  blockIdx.y, blockIdx.z, block_index());
+}
+
+// MINB as above (PB_TUNE_FCG_UPDATE_VARIANT; the default 5 matches a 48-register budget).
+template <int MINB>
+__global__ void __launch_bounds__(kUThreads, MINB) update_residual_kernel(
     const float* __restrict__ z, Pad g, float* p0, float* p1, double* x0, double* x1, const double* __restrict__ b,
     const double* __restrict__ screen, double pw, const double* __restrict__ scal, const int* __restrict__ flags,
     float* __restrict__ r32, double* __restrict__ part, int tz) {
@@ -382,7 +536,7 @@ __global__ void direction_finish_grouped_kernel(const batch::GridDesc* __restric
 
 // ptr[0] z, ptr[1] p0, ptr[2] p1, ptr[3] x0, ptr[4] x1, ptr[5] b, ptr[6] screen, ptr[7] r32, ptr[8] the
 // cloud's scalars, ptr[9] partials.
-__global__ void __launch_bounds__(kUThreads) update_residual_grouped_kernel(const batch::GridDesc* __restrict__ descs,
+__global__ void __launch_bounds__(kUThreads, 5) update_residual_grouped_kernel(const batch::GridDesc* __restrict__ descs,
                                                                             int count, const int* __restrict__ flags) {
     int bx, by, bz;
     const batch::GridDesc& d = batch::locate(descs, count, blockIdx.x, bx, by, bz);
@@ -535,8 +689,13 @@ extern "C" int pb_fcg_direction_f64(const float* z, const float* p0, const float
     cudaStream_t s = (cudaStream_t)stream;
     const int tz = direction_planes((int)n);
     const dim3 grid = flat_grid_of((int)n, tz);
-    direction_sums_kernel<<<grid, kThreads, 0, s>>>(z, pad_of((int)n), p0, p1, r32, screen, point_weight,
-                                                          flags, part, tz);
+    auto dir = direction_sums_kernel<4>;
+    switch (tuned(PB_TUNE_FCG_DIRECTION_VARIANT, n, 0)) {
+        case 1: dir = direction_sums_kernel<6>; break;
+        case 2: dir = direction_sums_kernel<8>; break;
+        default: break;
+    }
+    dir<<<grid, kThreads, 0, s>>>(z, pad_of((int)n), p0, p1, r32, screen, point_weight, flags, part, tz);
     PB_CHECK_LAUNCH("fcg direction_sums_kernel");
     direction_finish_kernel<<<1, 1024, 0, s>>>(part, (int)count(grid), flags, scal);
     PB_CHECK_LAUNCH("fcg direction_finish_kernel");
@@ -558,8 +717,15 @@ extern "C" int pb_fcg_update_f64(const float* z, float* p0, float* p1, double* x
     cudaStream_t s = (cudaStream_t)stream;
     const int tz = update_planes((int)n);
     const dim3 grid = tile_grid_of((int)n, tz);
-    update_residual_kernel<<<grid, dim3(kUX, kUY), 0, s>>>(z, pad_of((int)n), p0, p1, x0, x1, b, screen,
-                                                           point_weight, scal, flags, r32, part, tz);
+    auto upd = update_residual_kernel<5>;
+    switch (tuned(PB_TUNE_FCG_UPDATE_VARIANT, n, 0)) {
+        case 1: upd = update_residual_kernel<6>; break;
+        case 2: upd = update_residual_kernel<8>; break;
+        case 3: upd = update_residual_prefetch_kernel; break;
+        default: break;
+    }
+    upd<<<grid, dim3(kUX, kUY), 0, s>>>(z, pad_of((int)n), p0, p1, x0, x1, b, screen, point_weight, scal, flags,
+                                        r32, part, tz);
     PB_CHECK_LAUNCH("fcg update_residual_kernel");
     sum_kernel<<<1, 1024, 0, s>>>(part, (int)count(grid), scal + 4);
     PB_CHECK_LAUNCH("fcg sum_kernel");

@@ -12,10 +12,12 @@ its launchers consult; this module fills it by measurement:
   (MPR_B200_TUNE_CACHE, default ~/.cache/mojo_poissonrecon_b200/tune.json),
   so a process applies the stored choice without measuring again.
 
-Parameters (PB_TUNE_*): the TMA sweep's planes per block (z chunk), the
-level-0 residual-restriction's coarse planes per block, the prolongation's
-fine planes per block, and the planes per block of the two FCG passes.  The
-values change launch shapes only, never results.
+Parameters searched (PB_TUNE_*): the TMA sweep's planes per block (z chunk),
+the level-0 residual-restriction's coarse planes per block, the
+prolongation's fine planes per block, and which compiled variant each FCG
+pass runs (register budgets; cp.async prefetching for pass 2).  These change
+launch shapes only, never results: every node's arithmetic and every
+reduction's order stay the same.
 """
 
 from __future__ import annotations
@@ -25,9 +27,16 @@ import os
 import statistics
 import threading
 
-SWEEP_Z_CHUNK, RESTRICT_PLANES, PROLONG_PLANES, FCG_DIRECTION_PLANES, FCG_UPDATE_PLANES = range(5)
+(SWEEP_Z_CHUNK, RESTRICT_PLANES, PROLONG_PLANES, FCG_DIRECTION_PLANES, FCG_UPDATE_PLANES, FCG_DIRECTION_VARIANT,
+ FCG_UPDATE_VARIANT) = range(7)
 NAMES = {SWEEP_Z_CHUNK: "sweep_z_chunk", RESTRICT_PLANES: "restrict_planes", PROLONG_PLANES: "prolong_planes",
-         FCG_DIRECTION_PLANES: "fcg_direction_planes", FCG_UPDATE_PLANES: "fcg_update_planes"}
+         FCG_DIRECTION_PLANES: "fcg_direction_planes", FCG_UPDATE_PLANES: "fcg_update_planes",
+         FCG_DIRECTION_VARIANT: "fcg_direction_variant", FCG_UPDATE_VARIANT: "fcg_update_variant"}
+# Searched by autotune(): the parameters that never change results.  The FCG
+# passes' planes per block also set the shape of their partial-sum trees, so a
+# different value changes the inner products (and the iterates) by rounding;
+# they stay at the built-in 24 unless set explicitly.
+SEARCHED = (SWEEP_Z_CHUNK, RESTRICT_PLANES, PROLONG_PLANES, FCG_DIRECTION_VARIANT, FCG_UPDATE_VARIANT)
 _LOCK = threading.Lock()
 
 
@@ -52,6 +61,10 @@ def candidates(param: int, n: int) -> list[int]:
         return [0] + [v for v in (1, 2, 4, 8, 16, 32) if v <= n]
     if param in (FCG_DIRECTION_PLANES, FCG_UPDATE_PLANES):
         return [0] + [v for v in (8, 12, 16, 24, 32, 48, 64) if v <= max(n, 8)]
+    if param == FCG_DIRECTION_VARIANT:
+        return [0, 1, 2]
+    if param == FCG_UPDATE_VARIANT:
+        return [0, 1, 2, 3]
     raise ValueError(f"unknown tuning parameter {param}")
 
 
@@ -120,7 +133,7 @@ def autotune(n: int, device=None, repeats: int = 10, params=None, path: str | No
 
     lib = nat.lib()
     dev = nat.require_cuda() if device is None else device
-    params = list(NAMES) if params is None else list(params)
+    params = list(SEARCHED) if params is None else list(params)
     gen = torch.Generator(device=dev).manual_seed(1234)
     h = Hierarchy32(n, dev)
     l0, l1 = h.levels[0], h.levels[1]
@@ -151,7 +164,7 @@ def autotune(n: int, device=None, repeats: int = 10, params=None, path: str | No
         if param == PROLONG_PLANES:
             return lambda: nat.check(lib.pb_prolong_fac_f32(l1.ea.data_ptr(), l0.eb.data_ptr(),
                                                             l0.weights.data_ptr(), n, s), "prolong")
-        if param == FCG_DIRECTION_PLANES:
+        if param in (FCG_DIRECTION_PLANES, FCG_DIRECTION_VARIANT):
             return lambda: nat.check(lib.pb_fcg_direction_f64(l0.ea.data_ptr(), p0.data_ptr(), p1.data_ptr(),
                                                               l0.rhs.data_ptr(), screen.data_ptr(), n, 4.0,
                                                               scal.data_ptr(), flags.data_ptr(), ws_ptr, ws_size, s),

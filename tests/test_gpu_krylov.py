@@ -189,3 +189,56 @@ def test_fcg_update_matches_restatement(L, n, first, it):
         "r32"
     assert float(scal[4].item()) == pytest.approx(float(np.sum(r_want ** 2)), rel=1e-9)
     assert np.array_equal(scal.cpu().numpy()[:4], [1.0, beta, alpha, 0.0]), "scalars untouched"
+
+
+@pytest.mark.parametrize("n", (33, 65))
+def test_fcg_launch_variants_are_bit_identical(L, n):
+    """Every launch shape the autotuner may choose (register budgets, the
+    cp.async-prefetching pass 2, planes per block) gives the same bits."""
+    from mojo_poissonrecon_b200 import tune
+
+    pw = 4.0
+    screen, b, x, z, r, p = fcg_state(L, n, 99 + n)
+    dz, dr = to_padded(L, z.astype(np.float32)), to_padded(L, r.astype(np.float32))
+    ds, db = dev(screen), dev(b)
+    ws = torch.empty(int(L.pb_fcg_workspace_size(n)), dtype=torch.uint8, device="cuda")
+
+    def run():
+        dp = [dev(a, torch.float32) for a in p]
+        xs = [dev(x), torch.zeros((n, n, n), dtype=torch.float64, device="cuda")]
+        scal = torch.zeros(8, dtype=torch.float64, device="cuda")
+        scal[0] = 7.5
+        flags = torch.tensor([0, 0, 1, 0], dtype=torch.int32, device="cuda")
+        r32 = torch.zeros(geometry(L, n)[1], dtype=torch.float32, device="cuda")
+        rin = dr.clone()
+        s = stream()
+        assert L.pb_fcg_direction_f64(dz.data_ptr(), dp[0].data_ptr(), dp[1].data_ptr(), rin.data_ptr(),
+                                      ds.data_ptr(), n, pw, scal.data_ptr(), flags.data_ptr(), ws.data_ptr(),
+                                      ws.numel(), s) == 0
+        assert L.pb_fcg_update_f64(dz.data_ptr(), dp[0].data_ptr(), dp[1].data_ptr(), xs[0].data_ptr(),
+                                   xs[1].data_ptr(), db.data_ptr(), ds.data_ptr(), r32.data_ptr(), n, pw,
+                                   scal.data_ptr(), flags.data_ptr(), ws.data_ptr(), ws.numel(), s) == 0
+        return [t.cpu() for t in (scal, xs[1], dp[1], r32)]
+
+    L.pb_tune_clear()
+    try:
+        want = run()
+        for param, value in [(tune.FCG_UPDATE_VARIANT, v) for v in (1, 2, 3)] + \
+                            [(tune.FCG_DIRECTION_VARIANT, v) for v in (1, 2)]:
+            assert param in tune.SEARCHED
+            assert L.pb_tune_set(param, n, value) == 0
+            got = run()
+            for a, b_ in zip(got, want):
+                assert torch.equal(a, b_), (param, value)
+            L.pb_tune_clear()
+        # planes per block reshape the partial-sum trees: equal to rounding, not searched
+        for param, value in ((tune.FCG_UPDATE_PLANES, 8), (tune.FCG_DIRECTION_PLANES, 12)):
+            assert param not in tune.SEARCHED
+            assert L.pb_tune_set(param, n, value) == 0
+            got = run()
+            for a, b_ in zip(got, want):
+                assert torch.allclose(a.double(), b_.double(), rtol=1e-9, atol=1e-9 * float(b_.abs().max())), \
+                    (param, value)
+            L.pb_tune_clear()
+    finally:
+        L.pb_tune_clear()
