@@ -67,7 +67,7 @@ def parse_args():
                          "deep: depth 10")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the autotuner (built-in launch shapes); by default it runs before the warm-up")
-    ap.add_argument("--lanes", type=int, default=4)
+    ap.add_argument("--lanes", type=int, default=2)
     ap.add_argument("--duration", type=float, default=10.0, help="serving: seconds of arrivals")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
     return ap.parse_args()
@@ -548,16 +548,16 @@ def run_batch(args) -> dict:
             times.append(e0.elapsed_time(e1) / 1e3)
     per = statistics.median(times)
     lanes = {}
-    if args.lanes > 0:
-        warm_lanes(args.lanes, sorted({d for _, _, d in clouds}), clouds[0][:2])
+    if args.lanes > 0:  # the same clouds, one core.reconstruct per lane at a time (4 lanes)
+        warm_lanes(4, sorted({d for _, _, d in clouds}), clouds[0][:2])
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        with serve.Server(lanes=args.lanes) as server:
+        with serve.Server(lanes=4, max_batch=1) as server:
             futures = [server.submit(p, n, depth=d) for p, n, d in clouds]
             out = [f.result() for f in futures]
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
-        lanes = {"lanes": args.lanes, "recons_per_s": round(len(clouds) / wall, 2), "wall_s": round(wall, 3),
+        lanes = {"lanes": 4, "recons_per_s": round(len(clouds) / wall, 2), "wall_s": round(wall, 3),
                  "service_p99_ms": round(float(np.percentile([t.service_ms for _, t in out], 99)), 3)}
     return {"metric": METRIC, "workload": "batch: 256 uneven clouds (1k-200k points, depths 5-8, ellipsoids/tori)",
             "value": round(len(clouds) / per, 2), "unit": "recons/s", "n_gpus": 1, "precision": "fp32_refined",
@@ -611,19 +611,18 @@ def run_serving(args) -> dict:
     (median 50k, sigma 1, clipped to [1k, 2M]) and depths in {6,7,8,9}.  The
     clouds of the first 48 requests are generated before the clock starts and
     request k reuses cloud k mod 48 (with its own depth), so point generation
-    does not stall the arrivals."""
+    does not stall the arrivals.  The server batches whatever is queued (same
+    depth per batch) on `--lanes` lanes; latency = arrival to result."""
     import torch
 
-    from mojo_poissonrecon_b200 import serve, workloads
+    from mojo_poissonrecon_b200 import batch, serve, workloads
 
     stream = workloads.serving_stream(rate=args.rate, duration=args.duration, seed=4)
     pool = [workloads.request_cloud(size, shape, seed) for _, size, _, shape, seed in stream[:48]]
-    warm_lanes(args.lanes, (6, 7, 8, 9), pool[0])
-    with serve.Server(lanes=args.lanes) as server:  # and one request per depth through a server
-        for d in (6, 7, 8, 9):
-            server.submit(*pool[0], depth=d).result()
+    batch.reconstruct_many([(pool[0][0], pool[0][1], d) for d in (6, 7, 8, 9)], tol=TOL)  # modules, attributes
     torch.cuda.synchronize()
-    with serve.Server(lanes=args.lanes) as server:
+    lanes = max(1, args.lanes)
+    with serve.Server(lanes=lanes) as server:
         t0 = time.perf_counter()
         futures = []
         for k, (arrival, _, depth, _, _) in enumerate(stream):
@@ -634,17 +633,20 @@ def run_serving(args) -> dict:
             futures.append((depth, server.submit(p, n, depth=depth)))
         done = [(d, f.result()) for d, f in futures]
         wall = time.perf_counter() - t0
+        batches = server.batches
     lat = [t.latency_ms for _, (_, t) in done]
     by_depth = {}
     for d in (6, 7, 8, 9):
-        ls = [t.service_ms for dd, (_, t) in done if dd == d]
+        ls = [t for dd, (_, t) in done if dd == d]
         if ls:
-            by_depth[d] = {"count": len(ls), "service_p50_ms": round(statistics.median(ls), 2)}
+            by_depth[d] = {"count": len(ls), "latency_p50_ms": round(statistics.median(t.latency_ms for t in ls), 1),
+                           "service_p50_ms": round(statistics.median(t.service_ms for t in ls), 2)}
     return {"metric": METRIC, "workload": f"serving: Poisson arrivals {args.rate}/s for {args.duration} s, "
                                           "log-normal sizes (median 50k), depths 6-9",
             "value": round(len(done) / wall, 2), "unit": "recons/s", "n_gpus": 1, "requests": len(done),
             "p50_ms": round(statistics.median(lat), 2), "p99_ms": round(float(np.percentile(lat, 99)), 2),
-            "offered_rate": args.rate, "wall_s": round(wall, 2), "lanes": args.lanes, "service_by_depth": by_depth,
+            "offered_rate": args.rate, "wall_s": round(wall, 2), "lanes": lanes, "batches": batches,
+            "mean_batch": round(len(done) / max(batches, 1), 2), "by_depth": by_depth,
             "precision": "fp32_refined", "tol": TOL, "data": "synthetic (workloads.serving_stream, seed 4)"}
 
 

@@ -1,10 +1,11 @@
 """Continuous batching of reconstructions on one GPU.
 
 A `Server` keeps `lanes` workers.  Requests wait in a FIFO queue; a free lane
-takes the queue's head and, behind it, further queued requests (up to
-`max_batch`) while their estimated device footprints fit next to the requests
-already in flight, and runs them as one batch: `batch.reconstruct_many`, whose
-solver does one grouped launch per solver step for all of the batch's clouds.
+takes the queue's head and, from the requests queued behind it, those of the
+same depth and parameters (up to `max_batch`) while their estimated device
+footprints fit next to the requests already in flight, and runs them as one
+batch: `batch.reconstruct_many`, whose solver does one grouped launch per
+solver step for all of the batch's clouds.
 A request that arrives while batches are on the GPU joins the next batch a
 lane takes, so the GPU never waits for a batch boundary while work is queued,
 and with two or more lanes one batch's host work (preparation, result copies)
@@ -131,7 +132,7 @@ class Server:
 
     def __init__(self, lanes: int = 2, memory_fraction: float = 0.6, device: int | None = None,
                  budget_bytes: int | None = None, runner=None, batch_runner=None, max_batch: int = 64,
-                 drain_limit_s: float = 600.0, **defaults):
+                 drain_limit_s: float = 600.0, group_depths: bool = True, lookahead: int = 256, **defaults):
         """runner: optional callable(points, normals, **kwargs) -> result that
         replaces one GPU reconstruction; batch_runner: optional callable(list of
         (points, normals, kwargs)) -> list of results (or exceptions) that
@@ -139,7 +140,9 @@ class Server:
         failure logic runs without a device, as the tests do.  max_batch = 1
         runs one reconstruction per lane at a time (core.reconstruct).
         drain_limit_s bounds how long a lane waits for the device work of a
-        request that overran its deadline before it gives the lane up."""
+        request that overran its deadline before it gives the lane up.
+        group_depths: a batch takes requests of its head's depth only;
+        lookahead: how many queued requests behind the head a lane scans."""
         if lanes < 1:
             raise ValueError("lanes must be positive")
         if max_batch < 1:
@@ -148,6 +151,8 @@ class Server:
         self._batch_runner = batch_runner
         self.max_batch = int(max_batch)
         self.drain_limit_s = float(drain_limit_s)
+        self.group_depths = bool(group_depths)
+        self.lookahead = int(lookahead)
         self._fake = runner is not None or batch_runner is not None
         if not self._fake:
             self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
@@ -231,29 +236,38 @@ class Server:
 
     def _take(self) -> list | None:
         """The next batch: the queue's head (alone if nothing is in flight and it
-        needs the whole budget) and the queued requests behind it, in order,
-        while they fit next to what is in flight and suit the same batch."""
+        needs the whole budget) and, from the next `lookahead` queued requests,
+        those that suit the same batch (same parameters and, with
+        group_depths, the same depth, so small requests do not wait on deep
+        ones) while they fit next to what is in flight.  Requests passed over
+        keep their places."""
         with self._cv:
             while True:
                 self._expire_queued()
                 if self._queue:
                     head = self._queue[0]
                     if self._inflight == 0 or self._inflight_bytes + head.footprint <= self.budget:
-                        taken = [self._queue.popleft()]
-                        used = self._inflight_bytes + head.footprint
-                        while (self._queue and len(taken) < self.max_batch
-                               and used + self._queue[0].footprint <= self.budget
-                               and self._compatible(head, self._queue[0])):
-                            nxt = self._queue.popleft()
-                            if not nxt.future.set_running_or_notify_cancel():
-                                continue
-                            used += nxt.footprint
-                            taken.append(nxt)
-                        if not head.future.set_running_or_notify_cancel():
-                            taken.pop(0)
-                            used -= head.footprint
-                            if not taken:
-                                continue
+                        self._queue.popleft()
+                        taken = [head] if head.future.set_running_or_notify_cancel() else []
+                        used = self._inflight_bytes + (head.footprint if taken else 0)
+                        if taken:
+                            rest = collections.deque()
+                            scanned = 0
+                            while self._queue and len(taken) < self.max_batch and scanned < self.lookahead:
+                                nxt = self._queue.popleft()
+                                scanned += 1
+                                if (self._compatible(head, nxt) and used + nxt.footprint <= self.budget
+                                        and (not self.group_depths or
+                                             nxt.kwargs.get("depth") == head.kwargs.get("depth"))):
+                                    if nxt.future.set_running_or_notify_cancel():
+                                        used += nxt.footprint
+                                        taken.append(nxt)
+                                    continue
+                                rest.append(nxt)
+                            rest.extend(self._queue)
+                            self._queue = rest
+                        if not taken:
+                            continue
                         self._inflight += len(taken)
                         self._inflight_bytes = used
                         return taken

@@ -128,7 +128,7 @@ def cloud():
 
 def test_queued_requests_form_the_next_batch():
     fake = FakeBatchGPU(delay=0.3)
-    server = serve.Server(lanes=1, budget_bytes=1 << 40, batch_runner=fake, max_batch=8)
+    server = serve.Server(lanes=1, budget_bytes=1 << 40, batch_runner=fake, max_batch=8, group_depths=False)
     first = server.submit(*cloud(), depth=6, tag=0)
     time.sleep(0.1)  # the first batch (one request) is on the "device"
     rest = [server.submit(*cloud(), depth=6 + (k % 2), tag=k) for k in range(1, 6)]
@@ -136,6 +136,19 @@ def test_queued_requests_form_the_next_batch():
     assert [f.result(timeout=10)[0] for f in rest] == [1, 2, 3, 4, 5]
     server.close()
     assert fake.batches == [[0], [1, 2, 3, 4, 5]]  # arrivals during a batch run together next
+
+
+def test_batches_group_one_depth_and_keep_the_others_in_order():
+    fake = FakeBatchGPU(delay=0.2)
+    server = serve.Server(lanes=1, budget_bytes=1 << 40, batch_runner=fake, max_batch=8)
+    gate = server.submit(*cloud(), depth=5, tag="gate")
+    time.sleep(0.05)
+    order = [(6, "a"), (9, "b"), (6, "c"), (7, "d"), (9, "e"), (6, "f")]
+    futures = [server.submit(*cloud(), depth=d, tag=t) for d, t in order]
+    gate.result(timeout=10)
+    assert [f.result(timeout=10)[0] for f in futures] == [t for _, t in order]
+    server.close()
+    assert fake.batches == [["gate"], ["a", "c", "f"], ["b", "e"], ["d"]]
 
 
 def test_batches_respect_the_budget_and_max_batch():
