@@ -248,8 +248,11 @@ __device__ __forceinline__ void sweep_body(const CUtensorMap* map_e, const CUten
     }
 }
 
-template <bool ZERO_IN, int SLOTS>
-__global__ void __launch_bounds__(kThreads, PB_SWEEP_MIN_BLOCKS)
+// SLOTS planes in the shared ring (at least 3: planes t-1, t, t+1), MINB
+// resident blocks per SM the register budget must allow; the autotuner picks
+// among the compiled pairs (PB_TUNE_SWEEP_VARIANT).
+template <bool ZERO_IN, int SLOTS, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
     sweep_kernel(const __grid_constant__ CUtensorMap map_e, const __grid_constant__ CUtensorMap map_rhs,
                  const __grid_constant__ CUtensorMap map_invD, Params p) {
     sweep_body<ZERO_IN, SLOTS>(&map_e, &map_rhs, &map_invD, p, blockIdx.x, blockIdx.y, blockIdx.z);
@@ -419,13 +422,18 @@ extern "C" int pb_sweep_tma_f32(const float* e_in, float* e_out, const float* rh
     prm.ntx = (N - 1) / kTX > 0 ? (N - 1) / kTX : 1;
     prm.nty = (N - 1) / kTY > 0 ? (N - 1) / kTY : 1;
     const int tiles = prm.ntx * prm.nty;
+    // ring slots and resident blocks per SM: (5, 2) built in, (4, 3) and (3, 3) as variants
+    const int64_t variant = tuned(PB_TUNE_SWEEP_VARIANT, n, 0);
+    const int ring = variant == 1 ? 4 : variant == 2 ? 3 : kSlots;
+    const int per_sm = variant == 0 ? PB_SWEEP_MIN_BLOCKS : 3;
     if (z_chunk <= 0) z_chunk = tuned(PB_TUNE_SWEEP_Z_CHUNK, n, 0);
     if (z_chunk <= 0) {
         // c chunks per tile: minimise waves x (planes per chunk + the 4 planes a
-        // chunk loads beyond its range), waves = ceil(tiles c / (2 blocks x 148
-        // SMs)).  At 257^3 this picks c = 9 (two waves, 66 us a sweep) over the
-        // one-wave c = 4 (70 us, 40 of 296 slots idle); measured on B200.
-        const int64_t slots = 2 * kSMs;
+        // chunk loads beyond its range), waves = ceil(tiles c / (resident blocks x
+        // 148 SMs)).  At 257^3 with 2 blocks per SM this picks c = 9 (two waves,
+        // 66 us a sweep) over the one-wave c = 4 (70 us, 40 of 296 slots idle);
+        // measured on B200.
+        const int64_t slots = (int64_t)per_sm * kSMs;
         int64_t best = -1;
         int chosen = 1;
         for (int c = 1; c <= N; ++c) {
@@ -448,16 +456,22 @@ extern "C" int pb_sweep_tma_f32(const float* e_in, float* e_out, const float* rh
     PB_TRY(make_map(&mi, invD, N, prm.P, kBoxY));
     PB_TRY(make_map(&me, mode == 1 ? rhs : e_in, N, prm.P, kBoxY));
     const dim3 grid(prm.ntx, prm.nty, (N + prm.z_chunk - 1) / prm.z_chunk);
-    const size_t smem = sizeof(Geo2<kTY, kSlots>::Smem) + 128;
     cudaStream_t s = (cudaStream_t)stream;
-    auto launch = [&](auto kernel) -> int {
+    auto launch = [&](auto kernel, size_t smem) -> int {
         PB_CHECK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                       "sweep_tma smem");
         kernel<<<grid, kThreads, smem, s>>>(me, mr, mi, prm);
         PB_CHECK_LAUNCH("sweep_tma kernel");
         return PB_OK;
     };
-    return mode == 1 ? launch(sweep_kernel<true, kSlots>) : launch(sweep_kernel<false, kSlots>);
+    const size_t s5 = sizeof(Geo2<kTY, kSlots>::Smem) + 128, s4 = sizeof(Geo2<kTY, 4>::Smem) + 128,
+                 s3 = sizeof(Geo2<kTY, 3>::Smem) + 128;
+    if (ring == 4)
+        return mode == 1 ? launch(sweep_kernel<true, 4, 3>, s4) : launch(sweep_kernel<false, 4, 3>, s4);
+    if (ring == 3)
+        return mode == 1 ? launch(sweep_kernel<true, 3, 3>, s3) : launch(sweep_kernel<false, 3, 3>, s3);
+    return mode == 1 ? launch(sweep_kernel<true, kSlots, PB_SWEEP_MIN_BLOCKS>, s5)
+                     : launch(sweep_kernel<false, kSlots, PB_SWEEP_MIN_BLOCKS>, s5);
 }
 
 // fine += s * trilinear(coarse) (coarse side (n+1)/2), padded layouts, s the

@@ -15,7 +15,8 @@ its launchers consult; this module fills it by measurement:
 Parameters searched (PB_TUNE_*): the TMA sweep's planes per block (z chunk),
 the level-0 residual-restriction's coarse planes per block, the
 prolongation's fine planes per block, and which compiled variant each FCG
-pass runs (register budgets; cp.async prefetching for pass 2).  These change
+pass runs (register budgets; cp.async prefetching for pass 2) and the sweep
+(shared-ring depth with its resident blocks per SM).  These change
 launch shapes only, never results: every node's arithmetic and every
 reduction's order stay the same.
 """
@@ -28,15 +29,17 @@ import statistics
 import threading
 
 (SWEEP_Z_CHUNK, RESTRICT_PLANES, PROLONG_PLANES, FCG_DIRECTION_PLANES, FCG_UPDATE_PLANES, FCG_DIRECTION_VARIANT,
- FCG_UPDATE_VARIANT) = range(7)
+ FCG_UPDATE_VARIANT, SWEEP_VARIANT) = range(8)
 NAMES = {SWEEP_Z_CHUNK: "sweep_z_chunk", RESTRICT_PLANES: "restrict_planes", PROLONG_PLANES: "prolong_planes",
          FCG_DIRECTION_PLANES: "fcg_direction_planes", FCG_UPDATE_PLANES: "fcg_update_planes",
-         FCG_DIRECTION_VARIANT: "fcg_direction_variant", FCG_UPDATE_VARIANT: "fcg_update_variant"}
+         FCG_DIRECTION_VARIANT: "fcg_direction_variant", FCG_UPDATE_VARIANT: "fcg_update_variant",
+         SWEEP_VARIANT: "sweep_variant"}
 # Searched by autotune(): the parameters that never change results.  The FCG
 # passes' planes per block also set the shape of their partial-sum trees, so a
 # different value changes the inner products (and the iterates) by rounding;
 # they stay at the built-in 24 unless set explicitly.
-SEARCHED = (SWEEP_Z_CHUNK, RESTRICT_PLANES, PROLONG_PLANES, FCG_DIRECTION_VARIANT, FCG_UPDATE_VARIANT)
+# The sweep's variant comes first: the z chunk is then searched for the variant chosen.
+SEARCHED = (SWEEP_VARIANT, SWEEP_Z_CHUNK, RESTRICT_PLANES, PROLONG_PLANES, FCG_DIRECTION_VARIANT, FCG_UPDATE_VARIANT)
 _LOCK = threading.Lock()
 
 
@@ -65,6 +68,8 @@ def candidates(param: int, n: int) -> list[int]:
         return [0, 1, 2]
     if param == FCG_UPDATE_VARIANT:
         return [0, 1, 2, 3]
+    if param == SWEEP_VARIANT:
+        return [0, 1, 2]
     raise ValueError(f"unknown tuning parameter {param}")
 
 
@@ -154,7 +159,7 @@ def autotune(n: int, device=None, repeats: int = 10, params=None, path: str | No
     s = stream.cuda_stream
 
     def launch(param):
-        if param == SWEEP_Z_CHUNK:
+        if param in (SWEEP_Z_CHUNK, SWEEP_VARIANT):
             return lambda: nat.check(lib.pb_sweep_tma_f32(l0.ea.data_ptr(), l0.eb.data_ptr(), l0.rhs.data_ptr(),
                                                           l0.invD.data_ptr(), n, 0, 0, status.data_ptr(), s), "sweep")
         if param == RESTRICT_PLANES:

@@ -178,3 +178,35 @@ def test_engine_graphs_replay_new_inputs():
     solver32.clear_engines()
     fresh, _ = solver32.solve_refined(*systems[1], 4.0, ws)
     assert torch.equal(replayed, fresh)
+
+
+@pytest.mark.parametrize("n", [65, 257])
+def test_sweep_variants_bit_identical(L, n):
+    """The sweep's autotuned variants (shared-ring depth, resident blocks per SM)
+    and z chunks compute the same bits as the built-in launch shape."""
+    from mojo_poissonrecon_b200 import tune
+
+    screen, rhs, x, D, invD, W = setup(L, n, 31 * n)
+    e_in = to_padded(L, x.astype(np.float32))
+    r32 = to_padded(L, rhs.astype(np.float32))
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+
+    def sweep(mode):
+        out = torch.zeros_like(e_in)
+        assert L.pb_sweep_tma_f32(e_in.data_ptr(), out.data_ptr(), r32.data_ptr(), invD.data_ptr(), n, mode, 0,
+                                  status.data_ptr(), s) == 0
+        return out
+
+    L.pb_tune_clear()
+    try:
+        want = [sweep(0), sweep(1)]
+        for variant in (1, 2):
+            for z_chunk in (0, 17):
+                L.pb_tune_set(tune.SWEEP_VARIANT, n, variant)
+                L.pb_tune_set(tune.SWEEP_Z_CHUNK, n, z_chunk)
+                got = [sweep(0), sweep(1)]
+                assert torch.equal(got[0], want[0]) and torch.equal(got[1], want[1]), (variant, z_chunk)
+        assert int(status.item()) == 0
+    finally:
+        L.pb_tune_clear()
