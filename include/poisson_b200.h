@@ -428,6 +428,8 @@ int pb_batch_loop_condition(unsigned long long handle, const double *scal, const
  *   FCG_UPDATE_PLANES      planes per block of pb_fcg_update_f64 (default 24, at least 8)
  *   FCG_DIRECTION_VARIANT  register budget of pb_fcg_direction_f64: 0 = 4 resident
  *                          blocks per SM, 1 = 6, 2 = 8
+ *   RESTRICT_VARIANT       pb_residual_restrict_f32: 1 = both fine planes of a coarse
+ *                          plane in one loop over their items
  *   SWEEP_VARIANT          pb_sweep_tma_f32: 0 = a 5-plane shared ring with 2 resident
  *                          blocks per SM, 1 = 4 planes with 3 blocks, 2 = 3 planes with 3
  *   FCG_UPDATE_VARIANT     pb_fcg_update_f64: 0 = 5 resident blocks per SM,
@@ -446,7 +448,8 @@ enum {
     PB_TUNE_FCG_DIRECTION_VARIANT = 5,
     PB_TUNE_FCG_UPDATE_VARIANT = 6,
     PB_TUNE_SWEEP_VARIANT = 7,
-    PB_TUNE_PARAMS = 8
+    PB_TUNE_RESTRICT_VARIANT = 8,
+    PB_TUNE_PARAMS = 9
 };
 int pb_tune_set(int64_t param, int64_t n, int64_t value);
 int64_t pb_tune_get(int64_t param, int64_t n);

@@ -29,17 +29,18 @@ import statistics
 import threading
 
 (SWEEP_Z_CHUNK, RESTRICT_PLANES, PROLONG_PLANES, FCG_DIRECTION_PLANES, FCG_UPDATE_PLANES, FCG_DIRECTION_VARIANT,
- FCG_UPDATE_VARIANT, SWEEP_VARIANT) = range(8)
+ FCG_UPDATE_VARIANT, SWEEP_VARIANT, RESTRICT_VARIANT) = range(9)
 NAMES = {SWEEP_Z_CHUNK: "sweep_z_chunk", RESTRICT_PLANES: "restrict_planes", PROLONG_PLANES: "prolong_planes",
          FCG_DIRECTION_PLANES: "fcg_direction_planes", FCG_UPDATE_PLANES: "fcg_update_planes",
          FCG_DIRECTION_VARIANT: "fcg_direction_variant", FCG_UPDATE_VARIANT: "fcg_update_variant",
-         SWEEP_VARIANT: "sweep_variant"}
+         SWEEP_VARIANT: "sweep_variant", RESTRICT_VARIANT: "restrict_variant"}
 # Searched by autotune(): the parameters that never change results.  The FCG
 # passes' planes per block also set the shape of their partial-sum trees, so a
 # different value changes the inner products (and the iterates) by rounding;
 # they stay at the built-in 24 unless set explicitly.
 # The sweep's variant comes first: the z chunk is then searched for the variant chosen.
-SEARCHED = (SWEEP_VARIANT, SWEEP_Z_CHUNK, RESTRICT_PLANES, PROLONG_PLANES, FCG_DIRECTION_VARIANT, FCG_UPDATE_VARIANT)
+SEARCHED = (SWEEP_VARIANT, SWEEP_Z_CHUNK, RESTRICT_VARIANT, RESTRICT_PLANES, PROLONG_PLANES, FCG_DIRECTION_VARIANT,
+            FCG_UPDATE_VARIANT)
 _LOCK = threading.Lock()
 
 
@@ -70,6 +71,8 @@ def candidates(param: int, n: int) -> list[int]:
         return [0, 1, 2, 3]
     if param == SWEEP_VARIANT:
         return [0, 1, 2]
+    if param == RESTRICT_VARIANT:
+        return [0, 1]
     raise ValueError(f"unknown tuning parameter {param}")
 
 
@@ -162,7 +165,7 @@ def autotune(n: int, device=None, repeats: int = 10, params=None, path: str | No
         if param in (SWEEP_Z_CHUNK, SWEEP_VARIANT):
             return lambda: nat.check(lib.pb_sweep_tma_f32(l0.ea.data_ptr(), l0.eb.data_ptr(), l0.rhs.data_ptr(),
                                                           l0.invD.data_ptr(), n, 0, 0, status.data_ptr(), s), "sweep")
-        if param == RESTRICT_PLANES:
+        if param in (RESTRICT_PLANES, RESTRICT_VARIANT):
             return lambda: nat.check(lib.pb_residual_restrict_f32(l0.ea.data_ptr(), l0.rhs.data_ptr(),
                                                                   l0.D.data_ptr(), l0.weights.data_ptr(),
                                                                   l1.rhs.data_ptr(), n, s), "restrict")

@@ -210,3 +210,32 @@ def test_sweep_variants_bit_identical(L, n):
         assert int(status.item()) == 0
     finally:
         L.pb_tune_clear()
+
+
+@pytest.mark.parametrize("n", [65, 257])
+def test_residual_restrict_variants_bit_identical(L, n):
+    """The paired variant and other coarse planes per block compute the same bits."""
+    from mojo_poissonrecon_b200 import tune
+
+    screen, rhs, x, D, invD, W = setup(L, n, 17 * n)
+    e = to_padded(L, x.astype(np.float32))
+    r32 = to_padded(L, rhs.astype(np.float32))
+    cn = (n + 1) // 2
+    s = torch.cuda.current_stream().cuda_stream
+
+    def run():
+        out = torch.zeros(geometry(L, cn)[1], dtype=torch.float32, device="cuda")
+        assert L.pb_residual_restrict_f32(e.data_ptr(), r32.data_ptr(), D.data_ptr(), W.data_ptr(), out.data_ptr(),
+                                          n, s) == 0
+        return out
+
+    L.pb_tune_clear()
+    try:
+        want = run()
+        for variant in (0, 1):
+            for planes in (0, 1, 3, 8):
+                L.pb_tune_set(tune.RESTRICT_VARIANT, n, variant)
+                L.pb_tune_set(tune.RESTRICT_PLANES, n, planes)
+                assert torch.equal(run(), want), (variant, planes)
+    finally:
+        L.pb_tune_clear()
