@@ -651,21 +651,26 @@ def run_serving(args) -> dict:
 
 
 def run_deep(args) -> dict:
-    """20,000,000 points on a union of 64 spheres, depth 10 (1025^3)."""
+    """20,000,000 points on a union of 64 spheres, depth 10 (1025^3): each
+    precision's reconstruction timed with CUDA events and its peak device
+    memory, then the refined field (rel-res 1e-8) against the FP64 field solved
+    to 1e-10 on the same grids."""
     import torch
 
     import mojo_poissonrecon_b200 as mpr
-    from mojo_poissonrecon_b200 import solver32, workloads
+    from mojo_poissonrecon_b200 import core, solver32, workloads
 
     pts, nrm = workloads.sphere_union(20_000_000, spheres=64, seed=2)
     dp, dn = torch.from_numpy(pts).cuda(), torch.from_numpy(nrm).cuda()
     out = {}
     for prec in ("fp32_refined", "fp64"):
-        solver32.clear_engines()  # the refined engine (~100 GB at 1025^3) must not outlive its run
+        solver32.clear_engines()  # no engine of the other precision stays resident
         torch.cuda.empty_cache()
         torch.cuda.reset_peak_memory_stats()
         mpr.reconstruct(dp[:200_000], dn[:200_000], depth=10, precision=prec, tol=TOL, device_out=True)
         torch.cuda.synchronize()
+        base = torch.cuda.memory_allocated()
+        torch.cuda.reset_peak_memory_stats()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         mesh = mpr.reconstruct(dp, dn, depth=10, precision=prec, tol=TOL, device_out=True)
@@ -673,11 +678,26 @@ def run_deep(args) -> dict:
         torch.cuda.synchronize()
         out[prec] = {"ms": round(e0.elapsed_time(e1), 1), "vertices": int(mesh.vertices.shape[0]),
                      "faces": int(mesh.faces.shape[0]), "residual_norm": mesh.residual_norm,
-                     "peak_memory_gib": round(torch.cuda.max_memory_allocated() / 2**30, 1)}
+                     "peak_memory_gib": round((torch.cuda.max_memory_allocated() - base) / 2**30, 1),
+                     "resident_before_gib": round(base / 2**30, 1)}
+        del mesh
+    solver32.clear_engines()
+    torch.cuda.empty_cache()
+    ctx = core._Context()
+    up, un, _, _ = core._prepare(ctx, dp, dn, 1.1)
+    kw = dict(depth=10, point_weight=4.0, confidence=False, cycles=4, samples_per_node=1.5, max_cycles=400,
+              octree=False)
+    f32, _, _, st32, _ = core._solve_device(ctx, up, un, precision="fp32_refined", tol=TOL, **kw)
+    solver32.clear_engines()
+    f64, _, _, st64, _ = core._solve_device(ctx, up, un, precision="fp64", tol=1e-10, **kw)
+    scale = float(f64.abs().max())
+    accuracy = {"refined_cycles": st32.cycles, "refined_rel_residual": st32.relative_residual,
+                "fp64_cycles_to_1e-10": st64.cycles, "fp64_rel_residual": st64.relative_residual,
+                "field_max_rel_err_refined_vs_fp64_1e-10": float((f32 - f64).abs().max()) / scale}
     return {"metric": METRIC, "workload": "deep: 20M points on 64 spheres, depth 10 (1025^3), solve to 1e-8, "
                                           "dual contour", "value": round(1e3 / out["fp32_refined"]["ms"], 4),
             "unit": "recons/s", "n_gpus": 1, "fp32_refined": out["fp32_refined"], "fp64": out["fp64"],
-            "data": "synthetic (workloads.sphere_union, seed 2)"}
+            "accuracy": accuracy, "data": "synthetic (workloads.sphere_union, seed 2)"}
 
 
 def main():
