@@ -298,16 +298,17 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
             algorithmic = 16.0 * n**3  # read e, rhs, 1/D and write e, FP32, per launch
             gbs = algorithmic / (avg_ms / 1e3) / 1e9
             kernel_table.insert(0, {
-                "kernel": "tma::sweep_kernel<0, 5> (fused red-black sweep, level 0)", "us": round(avg_ms * 1e3, 1),
+                "kernel": "tma::sweep_kernel (fused red-black sweep, level 0; ring/occupancy variant "
+                          f"{int(_native.lib().pb_tune_get(7, n))})", "us": round(avg_ms * 1e3, 1),
                 "algorithmic_bytes": int(algorithmic), "achieved_gbs": round(gbs, 1),
                 "frac_of_measured_hbm": round(gbs / hbm_peak()[0], 3),
                 "traffic": read_profile_traffic(SWEEP_PROFILE),
                 "timing": "CUDA events around each finest-level sweep of 5 eager V-cycles"})
         # the dominant kernel of the launch list (profiles/launches_refined_d8.md)
-        top = next(k for k in kernel_table if k["kernel"].startswith("fcg::update_residual_kernel"))
+        top = next(k for k in kernel_table if k["kernel"].startswith("fcg::update_residual"))
         peak, peak_src = hbm_peak()
         achieved = top["algorithmic_bytes"] / (top["us"] * 1e-6) / 1e9
-        roofline = {"kernel": "pb::fcg::update_residual_kernel (FCG pass 2, FP64 residual, 257^3)",
+        roofline = {"kernel": f"pb::{top['kernel']} (FCG pass 2, FP64 residual, {n}^3)",
                     "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                     "frac": round(achieved / peak, 4), "peak_source": peak_src,
                     "avg_launch_ms": round(top["us"] / 1e3, 4), "launches_timed": 20,
@@ -387,17 +388,23 @@ def kernel_rooflines(eng, n: int, L) -> list:
         out.append({"kernel": name, "us": round(us, 1), "algorithmic_bytes": int(nbytes),
                     "achieved_gbs": round(gbs, 1), "frac_of_measured_hbm": round(gbs / peak, 3)})
 
-    timed("residual_restrict32_kernel (level 0)", lambda s: L.pb_residual_restrict_f32(
+    var = {name: int(L.pb_tune_get(code, n)) for name, code in
+           (("sweep", 7), ("restrict", 8), ("direction", 5), ("update", 6))}  # PB_TUNE_*_VARIANT
+    rr_name = "residual_restrict32_paired_kernel" if var["restrict"] == 1 else "residual_restrict32_kernel"
+    dir_name = f"fcg::direction_sums_kernel<{(4, 6, 8)[var['direction']]}>"
+    upd_name = ("fcg::update_residual_prefetch_kernel" if var["update"] == 3
+                else f"fcg::update_residual_kernel<{(5, 6, 8)[var['update']]}>")
+    timed(f"{rr_name} (level 0)", lambda s: L.pb_residual_restrict_f32(
         l0.ea.data_ptr(), l0.rhs.data_ptr(), l0.D.data_ptr(), l0.weights.data_ptr(), l1.rhs.data_ptr(), n, s),
         16 * N + 4 * N1)
     timed("prolong_add32_kernel (level 0)", lambda s: L.pb_prolong_fac_f32(
         l1.ea.data_ptr(), l0.eb.data_ptr(), l0.weights.data_ptr(), n, s), 12 * N + 4 * N1)
     timed("relax27p_kernel x2 (one sweep, level 1, packed FP16)", lambda s: L.pb_relax27p_f32(
         l1.ea.data_ptr(), l1.eb.data_ptr(), l1.rhs.data_ptr(), *l1.packed_ptrs(), l1.n, s), 68 * N1)
-    timed("fcg::direction_sums_kernel", lambda s: L.pb_fcg_direction_f64(
+    timed(dir_name, lambda s: L.pb_fcg_direction_f64(
         l0.ea.data_ptr(), p0, p1, l0.rhs.data_ptr(), eng.screen.data_ptr(), n, eng.pw, eng.scal.data_ptr(),
         eng.flags.data_ptr(), eng.ws_ptr, eng.ws_size, s), 20 * N)
-    timed("fcg::update_residual_kernel", lambda s: L.pb_fcg_update_f64(
+    timed(upd_name, lambda s: L.pb_fcg_update_f64(
         l0.ea.data_ptr(), p0, p1, x0, x1, eng.b.data_ptr(), eng.screen.data_ptr(), l0.rhs.data_ptr(), n, eng.pw,
         eng.scal.data_ptr(), eng.flags.data_ptr(), eng.ws_ptr, eng.ws_size, s), 48 * N)
     return out
