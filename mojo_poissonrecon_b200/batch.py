@@ -264,7 +264,8 @@ class BatchSolver:
         self.body_launches = L.pb_launch_count() - before
 
     # -- solve -----------------------------------------------------------------------
-    def solve(self, rhs: list, screen: list, point_weights, tol: float = 1e-8, max_cycles: int = 200):
+    def solve(self, rhs: list, screen: list, point_weights, tol: float = 1e-8, max_cycles: int = 200,
+              phases=None):
         """Solve A_k x_k = b_k for every cloud to ||b_k - A_k x_k|| <= tol ||b_k||.
 
         rhs, screen: per cloud dense FP64 (n, n, n) CUDA tensors (read in place;
@@ -284,11 +285,12 @@ class BatchSolver:
         for t in list(rhs) + list(screen):
             t.record_stream(self.stream)
         with torch.cuda.stream(self.stream):
-            xs, stats = self._solve(rhs, screen, pws, tol, max_cycles)
+            xs, stats = self._solve(rhs, screen, pws, tol, max_cycles, phases)
         caller.wait_stream(self.stream)
         return [x.clone() for x in xs], stats  # on the caller's stream
 
-    def _solve(self, rhs, screen, pws, tol, max_cycles):
+    def _solve(self, rhs, screen, pws, tol, max_cycles, phases=None):
+        mark = phases.mark if phases is not None else (lambda name: None)
         L, s = self.lib, nat.stream_handle()
         K = len(self.clouds)
         # prologue per cloud: levels' set-up, x0 = 0.5 and its residual, ||b||
@@ -309,8 +311,10 @@ class BatchSolver:
         self.flags[:, 0] = 1
         self.flags[:, 2] = ((self.norm2 > target2) & (max_cycles > 0)).to(torch.int32)
         self.scal.zero_()
+        mark("solver prologue")
         self.launches = self._plan(rhs, screen, pws)
         self._capture()
+        mark("solver plan and capture")
         nat.check(L.pb_graph_launch(self.exec, s), "batch graph launch")
         _sync.wait("batched solver iterations")
         host = torch.cat([self.flags[:, 1].to(torch.float64), self.scal[:, 4], self.norm2, self.bnorm,
@@ -342,16 +346,38 @@ def _footprint(depth: int, points: int) -> int:
     return footprint_bytes(depth, points)
 
 
+class _Phases:
+    """Host wall time per phase of reconstruct_many (profile=dict), each phase
+    closed by a device synchronisation; a no-op without a dict."""
+
+    def __init__(self, sink: dict | None):
+        import time
+
+        self.sink, self.clock = sink, time.perf_counter
+        self.t = self.clock() if sink is not None else 0.0
+
+    def mark(self, name: str) -> None:
+        if self.sink is None:
+            return
+        torch.cuda.synchronize()
+        now = self.clock()
+        self.sink[name] = self.sink.get(name, 0.0) + (now - self.t)
+        self.t = now
+
+
 def reconstruct_many(clouds, *, depth: int = 6, point_weight: float = 4.0, confidence: bool = False,
                      scale: float = 1.1, samples_per_node: float = 1.5, tol: float = 1e-8, max_cycles: int = 200,
-                     budget_bytes: int | None = None, device_out: bool = False) -> list:
+                     budget_bytes: int | None = None, device_out: bool = False, profile: dict | None = None) -> list:
     """Reconstruct many clouds with batched solves (module docstring).
 
     clouds: (points, normals) or (points, normals, depth) tuples (NumPy or
     torch).  Precision is "fp32_refined" to relative residual `tol`.  Clouds
     run in waves whose estimated device footprint fits `budget_bytes`
     (default: 60 % of the device's free memory).  Returns core.Mesh objects in
-    input order, bit-identical to core.reconstruct of each cloud alone."""
+    input order, bit-identical to core.reconstruct of each cloud alone.
+    profile: a dict that receives the host seconds of each phase (with a
+    device synchronisation after each, so only for measurements)."""
+    phases = _Phases(profile)
     dev = nat.require_cuda()
     items = []
     for k, cloud in enumerate(clouds):
@@ -372,21 +398,25 @@ def reconstruct_many(clouds, *, depth: int = 6, point_weight: float = 4.0, confi
         out[k] = core.reconstruct(p, nrm, depth=d, point_weight=point_weight, confidence=confidence, scale=scale,
                                   samples_per_node=samples_per_node, precision="fp32_refined", tol=tol,
                                   max_cycles=max_cycles, device_out=device_out)
+    phases.mark("validate and small clouds")
     big = sorted((it for it in items if it[3] >= MIN_DEPTH), key=lambda it: -it[3])
     wave, used = [], 0
     for it in big:
         need = _footprint(it[3], len(it[1]))
         if wave and used + need > budget_bytes:
-            _run_wave(wave, out, dev, point_weight, confidence, scale, samples_per_node, tol, max_cycles, device_out)
+            _run_wave(wave, out, dev, point_weight, confidence, scale, samples_per_node, tol, max_cycles, device_out,
+                      phases)
             wave, used = [], 0
         wave.append(it)
         used += need
     if wave:
-        _run_wave(wave, out, dev, point_weight, confidence, scale, samples_per_node, tol, max_cycles, device_out)
+        _run_wave(wave, out, dev, point_weight, confidence, scale, samples_per_node, tol, max_cycles, device_out,
+                  phases)
     return out
 
 
-def _run_wave(wave, out, dev, point_weight, confidence, scale, samples_per_node, tol, max_cycles, device_out):
+def _run_wave(wave, out, dev, point_weight, confidence, scale, samples_per_node, tol, max_cycles, device_out,
+              phases: _Phases):
     L = nat.lib()
     ctx = core._Context()
     s = ctx.stream
@@ -401,6 +431,7 @@ def _run_wave(wave, out, dev, point_weight, confidence, scale, samples_per_node,
             src = arr if isinstance(arr, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(arr))
             staging[slot, a:b].copy_(src.to(torch.float64))
     both = staging.to(dev, non_blocking=True)
+    phases.mark("stage and upload")
     # preparation of every cloud, then one read of all kept counts
     kept = torch.zeros(len(wave), dtype=torch.int64, device=dev)
     maps = torch.empty((len(wave), 4), dtype=torch.float64, device=dev)
@@ -420,6 +451,7 @@ def _run_wave(wave, out, dev, point_weight, confidence, scale, samples_per_node,
     _sync.wait("prepare points")
     kept_h = kept.cpu().numpy()
     del both
+    phases.mark("prepare")
     solve_idx, grids, accepted_all = [], [], []
     for j, (_, _, _, d) in enumerate(wave):
         k = int(kept_h[j])
@@ -433,15 +465,19 @@ def _run_wave(wave, out, dev, point_weight, confidence, scale, samples_per_node,
         grids.append(g)
         accepted_all.append(acc)
         solve_idx.append(j)
+    ctx.ws = nat.Workspace(dev)  # the splats' scratch is not needed past this point
+    phases.mark("splat and assemble")
     fields = {}
     stats = {}
     if solve_idx:
         solver = BatchSolver([(1 << wave[j][3]) + 1 for j in solve_idx], dev)
+        phases.mark("solver allocation")
         f, st = solver.solve([grids[j]["rhs"] for j in solve_idx], [grids[j]["screen"] for j in solve_idx],
-                             point_weight, tol=tol, max_cycles=max_cycles)
+                             point_weight, tol=tol, max_cycles=max_cycles, phases=phases)
         for j, fj, sj in zip(solve_idx, f, st):
             fields[j], stats[j] = fj, sj
         del solver
+    phases.mark("solve")
     # iso-values and extraction counts for every cloud, then one read of all counts
     pending = []
     counts = torch.zeros((len(wave), 2), dtype=torch.int64, device=dev)
@@ -459,6 +495,7 @@ def _run_wave(wave, out, dev, point_weight, confidence, scale, samples_per_node,
     acc_check = torch.stack([a for a in accepted_all if a is not None]) if solve_idx else None
     _sync.wait("extract count")
     host_counts = counts.cpu().numpy()
+    phases.mark("iso and extraction counts")
     if acc_check is not None:
         acc_h = acc_check.cpu().numpy().ravel()
         for j, a in zip(solve_idx, acc_h):
@@ -478,6 +515,7 @@ def _run_wave(wave, out, dev, point_weight, confidence, scale, samples_per_node,
                                             ptr, size, s), "extract emit")
             ctx.check(L.pb_map_vertices_f64(vertices.data_ptr(), nv, maps[j].data_ptr(), s), "map vertices")
         results[j] = (vertices, faces, vdens, iso)
+    phases.mark("extraction emit")
     # meshes to the host together (pinned buffers, one synchronisation)
     flat = []
     for j in sorted(results):
@@ -490,6 +528,7 @@ def _run_wave(wave, out, dev, point_weight, confidence, scale, samples_per_node,
     for j in range(len(wave)):
         if j not in results:
             out[wave[j][0]] = _empty_mesh(dev, device_out)
+    phases.mark("results to host")
 
 
 def _empty_mesh(dev, device_out: bool):

@@ -84,6 +84,9 @@ __device__ __forceinline__ int64_t block_index() {
 // registers; the ghosts of the padded z are zero, so the 6-neighbour sum needs
 // no tests.  Compiled for 4 resident blocks per SM (64 registers), which keeps
 // more loads in flight than the occupancy-first default.
+// TZC > 0: the planes per block as a compile-time constant (the built-in kTZ),
+// which lets the compiler unroll the z march; 0: the runtime tz.
+template <int TZC>
 __device__ __forceinline__ void direction_sums_body(const float* __restrict__ z, Pad g, const float* __restrict__ p0,
                                                     const float* __restrict__ p1, const float* __restrict__ r32,
                                                     const double* __restrict__ screen, double pw,
@@ -93,7 +96,8 @@ __device__ __forceinline__ void direction_sums_body(const float* __restrict__ z,
     const int n = g.n;
     const unsigned t = bx * kThreads + threadIdx.x;  // flattened over the plane's (x, y): full warps
     const int y = t < (unsigned)(n * n) ? (int)(t / (unsigned)n) : n, x = (int)(t - (unsigned)y * n);
-    const int z0 = by * tz, z1 = min(n, z0 + tz);
+    const int tzv = TZC > 0 ? TZC : tz;
+    const int z0 = by * tzv, z1 = min(n, z0 + tzv);
     const double h = (double)(n - 1), h2 = h * h;
     const bool first = flags[0] != 0;
     const float* __restrict__ pp = (flags[1] & 1) ? p1 : p0;
@@ -130,7 +134,7 @@ __device__ __forceinline__ void direction_sums_body(const float* __restrict__ z,
 
 // MINB: resident blocks per SM the compiler must allow (register budget); the
 // autotuner picks among the compiled variants (PB_TUNE_FCG_DIRECTION_VARIANT).
-template <int MINB>
+template <int MINB, int TZC>
 __global__ void __launch_bounds__(kThreads, MINB) direction_sums_kernel(const float* __restrict__ z, Pad g,
                                                                      const float* __restrict__ p0,
                                                                      const float* __restrict__ p1,
@@ -138,7 +142,7 @@ __global__ void __launch_bounds__(kThreads, MINB) direction_sums_kernel(const fl
                                                                      const double* __restrict__ screen, double pw,
                                                                      const int* __restrict__ flags,
                                                                      double* __restrict__ part, int tz) {
-    direction_sums_body(z, g, p0, p1, r32, screen, pw, flags, part, tz, blockIdx.x, blockIdx.y, block_index());
+    direction_sums_body<TZC>(z, g, p0, p1, r32, screen, pw, flags, part, tz, blockIdx.x, blockIdx.y, block_index());
 }
 
 // Sums pass 1's partials (fixed order) and forms the step's scalars:
@@ -205,6 +209,7 @@ struct Halo {
 // registers (about 7 global loads per node instead of 23 with every neighbour
 // formed from memory).  Nodes outside the domain hold 0 and
 // the neighbour sum adds x-, x+, y-, y+, z-, z+ in that order.
+template <int TZC>
 __device__ __forceinline__ void update_residual_body(const float* __restrict__ z, Pad g, float* p0, float* p1,
                                                      double* x0, double* x1, const double* __restrict__ b,
                                                      const double* __restrict__ screen, double pw,
@@ -217,7 +222,8 @@ __device__ __forceinline__ void update_residual_body(const float* __restrict__ z
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kUX + tx;
     const int bx = tile_x * kUX, by = tile_y * kUY;
     const int x = bx + tx, y = by + ty;
-    const int z0 = tile_z * tz, z1 = min(n, z0 + tz);
+    const int tzv = TZC > 0 ? TZC : tz;
+    const int z0 = tile_z * tzv, z1 = min(n, z0 + tzv);
     const double h = (double)(n - 1), h2 = h * h;
     const int odd = flags[1] & 1;
     const bool first = flags[0] != 0;
@@ -318,6 +324,7 @@ __device__ __forceinline__ void cp_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+template <int TZC>
 __device__ __forceinline__ void update_residual_prefetch_body(
     const float* __restrict__ z, Pad g, float* p0, float* p1, double* x0, double* x1, const double* __restrict__ b,
     const double* __restrict__ screen, double pw, const double* __restrict__ scal, const int* __restrict__ flags,
@@ -330,7 +337,8 @@ __device__ __forceinline__ void update_residual_prefetch_body(
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kUX + tx;
     const int bx = tile_x * kUX, by = tile_y * kUY;
     const int x = bx + tx, y = by + ty;
-    const int z0 = tile_z * tz, z1 = min(n, z0 + tz);
+    const int tzv = TZC > 0 ? TZC : tz;
+    const int z0 = tile_z * tzv, z1 = min(n, z0 + tzv);
     const double h = (double)(n - 1), h2 = h * h;
     const int odd = flags[1] & 1;
     const bool first = flags[0] != 0;
@@ -436,21 +444,22 @@ __device__ __forceinline__ void update_residual_prefetch_body(
     if (lin_tid() == 0) part[block] = v[0];
 }
 
+template <int TZC>
 __global__ void __launch_bounds__(kUThreads) update_residual_prefetch_kernel(
     const float* __restrict__ z, Pad g, float* p0, float* p1, double* x0, double* x1, const double* __restrict__ b,
     const double* __restrict__ screen, double pw, const double* __restrict__ scal, const int* __restrict__ flags,
     float* __restrict__ r32, double* __restrict__ part, int tz) {
-    update_residual_prefetch_body(z, g, p0, p1, x0, x1, b, screen, pw, scal, flags, r32, part, tz, blockIdx.x,
+    update_residual_prefetch_body<TZC>(z, g, p0, p1, x0, x1, b, screen, pw, scal, flags, r32, part, tz, blockIdx.x,
                                   blockIdx.y, blockIdx.z, block_index());
 }
 
 // MINB as above (PB_TUNE_FCG_UPDATE_VARIANT; the default 5 matches a 48-register budget).
-template <int MINB>
+template <int MINB, int TZC>
 __global__ void __launch_bounds__(kUThreads, MINB) update_residual_kernel(
     const float* __restrict__ z, Pad g, float* p0, float* p1, double* x0, double* x1, const double* __restrict__ b,
     const double* __restrict__ screen, double pw, const double* __restrict__ scal, const int* __restrict__ flags,
     float* __restrict__ r32, double* __restrict__ part, int tz) {
-    update_residual_body(z, g, p0, p1, x0, x1, b, screen, pw, scal, flags, r32, part, tz, blockIdx.x, blockIdx.y,
+    update_residual_body<TZC>(z, g, p0, p1, x0, x1, b, screen, pw, scal, flags, r32, part, tz, blockIdx.x, blockIdx.y,
                          blockIdx.z, block_index());
 }
 
@@ -518,7 +527,7 @@ __global__ void __launch_bounds__(kThreads, 4) direction_sums_grouped_kernel(con
     int bx, by, bz;
     const batch::GridDesc& d = batch::locate(descs, count, blockIdx.x, bx, by, bz);
     if (!batch::cloud_active(flags, d.cloud)) return;
-    direction_sums_body((const float*)d.ptr[0], pad_of((int)d.n), (const float*)d.ptr[1], (const float*)d.ptr[2],
+    direction_sums_body<kTZ>((const float*)d.ptr[0], pad_of((int)d.n), (const float*)d.ptr[1], (const float*)d.ptr[2],
                         (const float*)d.ptr[3], (const double*)d.ptr[4], aux_double(d.aux[0]),
                         flags + d.cloud * batch::kFlagStride, (double*)d.ptr[5], (int)d.aux[1], bx, by,
                         bx + d.gx * (int64_t)by);
@@ -536,12 +545,12 @@ __global__ void direction_finish_grouped_kernel(const batch::GridDesc* __restric
 
 // ptr[0] z, ptr[1] p0, ptr[2] p1, ptr[3] x0, ptr[4] x1, ptr[5] b, ptr[6] screen, ptr[7] r32, ptr[8] the
 // cloud's scalars, ptr[9] partials.
-__global__ void __launch_bounds__(kUThreads, 5) update_residual_grouped_kernel(const batch::GridDesc* __restrict__ descs,
+__global__ void __launch_bounds__(kUThreads, 4) update_residual_grouped_kernel(const batch::GridDesc* __restrict__ descs,
                                                                             int count, const int* __restrict__ flags) {
     int bx, by, bz;
     const batch::GridDesc& d = batch::locate(descs, count, blockIdx.x, bx, by, bz);
     if (!batch::cloud_active(flags, d.cloud)) return;
-    update_residual_body((const float*)d.ptr[0], pad_of((int)d.n), (float*)d.ptr[1], (float*)d.ptr[2],
+    update_residual_prefetch_body<kTZ>((const float*)d.ptr[0], pad_of((int)d.n), (float*)d.ptr[1], (float*)d.ptr[2],
                          (double*)d.ptr[3], (double*)d.ptr[4], (const double*)d.ptr[5], (const double*)d.ptr[6],
                          aux_double(d.aux[0]), (const double*)d.ptr[8], flags + d.cloud * batch::kFlagStride,
                          (float*)d.ptr[7], (double*)d.ptr[9], (int)d.aux[1], bx, by, bz,
@@ -592,7 +601,7 @@ int describe_fcg_direction(GridDesc& d) {
     for (int k = 0; k < 6; ++k)
         if (!d.ptr[k]) return fail(PB_ERR_INVALID, "batch fcg direction: bad args");
     if (n < 2 || n > 4097 || d.ptr[1] == d.ptr[2]) return fail(PB_ERR_INVALID, "batch fcg direction: bad args");
-    const int tz = fcg::direction_planes(n);
+    const int tz = fcg::kTZ;  // grouped launches keep the built-in planes per block
     const dim3 g = fcg::flat_grid_of(n, tz);
     d.gx = g.x;
     d.gy = g.y;
@@ -607,7 +616,7 @@ int describe_fcg_update(GridDesc& d) {
         if (!d.ptr[k]) return fail(PB_ERR_INVALID, "batch fcg update: bad args");
     if (n < 2 || n > 4097 || d.ptr[1] == d.ptr[2] || d.ptr[3] == d.ptr[4])
         return fail(PB_ERR_INVALID, "batch fcg update: bad args");
-    const int tz = fcg::update_planes(n);
+    const int tz = fcg::kTZ;
     const dim3 g = fcg::tile_grid_of(n, tz);
     d.gx = g.x;
     d.gy = g.y;
@@ -624,8 +633,8 @@ int describe_fcg_reduce(GridDesc& d) {
 
 // Partial-sum doubles one cloud of side n needs (both FCG passes).
 int64_t fcg_partials(int n) { return (int64_t)fcg::blocks_of(n) * 4; }
-int64_t fcg_direction_blocks(int n) { return fcg::count(fcg::flat_grid_of(n, fcg::direction_planes(n))); }
-int64_t fcg_update_blocks(int n) { return fcg::count(fcg::tile_grid_of(n, fcg::update_planes(n))); }
+int64_t fcg_direction_blocks(int n) { return fcg::count(fcg::flat_grid_of(n, fcg::kTZ)); }
+int64_t fcg_update_blocks(int n) { return fcg::count(fcg::tile_grid_of(n, fcg::kTZ)); }
 
 int launch_fcg(int kind, const GridDesc* descs, int count, int64_t blocks, const int* flags, cudaStream_t s) {
     switch (kind) {
@@ -689,10 +698,11 @@ extern "C" int pb_fcg_direction_f64(const float* z, const float* p0, const float
     cudaStream_t s = (cudaStream_t)stream;
     const int tz = direction_planes((int)n);
     const dim3 grid = flat_grid_of((int)n, tz);
-    auto dir = direction_sums_kernel<4>;
+    const bool fixed = tz == kTZ;
+    auto dir = fixed ? direction_sums_kernel<4, kTZ> : direction_sums_kernel<4, 0>;
     switch (tuned(PB_TUNE_FCG_DIRECTION_VARIANT, n, 0)) {
-        case 1: dir = direction_sums_kernel<6>; break;
-        case 2: dir = direction_sums_kernel<8>; break;
+        case 1: dir = fixed ? direction_sums_kernel<6, kTZ> : direction_sums_kernel<6, 0>; break;
+        case 2: dir = fixed ? direction_sums_kernel<8, kTZ> : direction_sums_kernel<8, 0>; break;
         default: break;
     }
     dir<<<grid, kThreads, 0, s>>>(z, pad_of((int)n), p0, p1, r32, screen, point_weight, flags, part, tz);
@@ -717,11 +727,12 @@ extern "C" int pb_fcg_update_f64(const float* z, float* p0, float* p1, double* x
     cudaStream_t s = (cudaStream_t)stream;
     const int tz = update_planes((int)n);
     const dim3 grid = tile_grid_of((int)n, tz);
-    auto upd = update_residual_kernel<5>;
+    const bool fixed = tz == kTZ;
+    auto upd = fixed ? update_residual_kernel<5, kTZ> : update_residual_kernel<5, 0>;
     switch (tuned(PB_TUNE_FCG_UPDATE_VARIANT, n, 0)) {
-        case 1: upd = update_residual_kernel<6>; break;
-        case 2: upd = update_residual_kernel<8>; break;
-        case 3: upd = update_residual_prefetch_kernel; break;
+        case 1: upd = fixed ? update_residual_kernel<6, kTZ> : update_residual_kernel<6, 0>; break;
+        case 2: upd = fixed ? update_residual_kernel<8, kTZ> : update_residual_kernel<8, 0>; break;
+        case 3: upd = fixed ? update_residual_prefetch_kernel<kTZ> : update_residual_prefetch_kernel<0>; break;
         default: break;
     }
     upd<<<grid, dim3(kUX, kUY), 0, s>>>(z, pad_of((int)n), p0, p1, x0, x1, b, screen, point_weight, scal, flags,

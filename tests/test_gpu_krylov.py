@@ -8,8 +8,9 @@ r = b - A x_new, ||r||^2), on small odd sides, first and later steps, both
 buffer parities.  A is the reference's operator (capi.mojo:282-306, 413-553):
 (A x)_i = (deg_i + pw s_i) h^2 x_i - h^2 sum of in-grid neighbours, h = n - 1.
 
-Tolerances: element-wise values (x_new, p_new) within 4 ulp of the restatement
-(the update may fuse a multiply-add); residuals within 1e-12 of the largest
+Tolerances: x_new within 4 eps of the magnitudes it is formed from
+(|x| + |alpha| (|z| + |beta p|): the update may fuse multiply-adds), p_new within
+one FP32 ulp; residuals within 1e-12 of the largest
 term of A x (the neighbour sum cancels); inner products and their quotients
 within 1e-11 relative (a parallel tree sum against NumPy's pairwise sum)."""
 
@@ -176,8 +177,10 @@ def test_fcg_update_matches_restatement(L, n, first, it):
     direction = z - beta * p[odd] if not first else z.copy()
     x_want = x + alpha * direction
     x_got = xs[1 - odd].cpu().numpy()
-    ulp = np.spacing(np.maximum(np.abs(x_want), np.abs(x)))
-    assert np.all(np.abs(x_got - x_want) <= 4 * ulp), "x_new"
+    # the kernel may fuse z - beta p and x + alpha d into multiply-adds: each rounding is
+    # relative to the magnitudes before cancellation, |x| + |alpha| (|z| + |beta p|)
+    scale = np.abs(x) + abs(alpha) * (np.abs(z) + abs(beta) * np.abs(p[odd]))
+    assert np.all(np.abs(x_got - x_want) <= 4 * np.finfo(np.float64).eps * scale), "x_new"
     assert np.array_equal(xs[odd].cpu().numpy(), x), "x_old untouched"
     p_got = dp[1 - odd].cpu().numpy().astype(np.float64)
     assert np.all(np.abs(p_got - f32(direction)) <= np.spacing(np.abs(direction).astype(np.float32))), "p_new"

@@ -65,9 +65,10 @@ def test_tune_table_rejects_bad_entries(args):
     assert lib.pb_tune_set(*args) == 1
 
 
-def test_tuned_plane_counts_change_grouped_launch_shapes_only():
-    """The FCG pass-2 grid follows the tuned planes per block (blocks = tiles x
-    ceil(n / planes)); the partial-sum capacity covers the shallowest choice."""
+def test_grouped_fcg_launches_keep_the_built_in_planes():
+    """Grouped (batched) FCG launches use 24 planes per block whatever the
+    table says, so a batch's inner products have the single path's default
+    partial-sum trees; the partial-sum capacity covers the shallowest choice."""
     from mojo_poissonrecon_b200 import _native
 
     lib = _native.lib()
@@ -75,9 +76,7 @@ def test_tuned_plane_counts_change_grouped_launch_shapes_only():
     try:
         assert lib.pb_batch_fcg_blocks(257, 1) == 9 * 33 * 11  # 24 planes
         lib.pb_tune_set(tune.FCG_UPDATE_PLANES, 257, 8)
-        assert lib.pb_batch_fcg_blocks(257, 1) == 9 * 33 * 33
-        lib.pb_tune_set(tune.FCG_UPDATE_PLANES, 257, 2)  # below the minimum: clamped to 8
-        assert lib.pb_batch_fcg_blocks(257, 1) == 9 * 33 * 33
-        assert lib.pb_batch_fcg_partials(257) >= lib.pb_batch_fcg_blocks(257, 1)
+        assert lib.pb_batch_fcg_blocks(257, 1) == 9 * 33 * 11
+        assert lib.pb_batch_fcg_partials(257) >= 9 * 33 * 33  # the 8-plane single-path grid fits too
     finally:
         lib.pb_tune_clear()
