@@ -161,7 +161,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     if not args.no_tune:  # before any engine captures its launch shapes
         from mojo_poissonrecon_b200 import tune
 
-        found = tune.autotune((1 << args.depth) + 1, device=dev, write=False)
+        found = tune.autotune((1 << args.depth) + 1, device=dev, write=True)  # cached for later processes
         tuning = {k: {"chosen": v["best"], "default_us": round(v["default_s"] * 1e6, 1),
                       "tuned_us": round(v["best_s"] * 1e6, 1)} for k, v in found.items()}
 
