@@ -46,6 +46,7 @@ DEPTH = 8
 TOL = 1e-8
 SWEEP_PROFILE = os.path.join(ROOT, "profiles", "sweep_tma_f32_257.md")
 UPDATE_PROFILE = os.path.join(ROOT, "profiles", "fcg_update_residual_257.md")
+RESTRICT_PROFILE = os.path.join(ROOT, "profiles", "residual_restrict32_257.md")
 
 
 def parse_args():
@@ -395,6 +396,7 @@ def kernel_rooflines(eng, n: int, L) -> list:
     dir_name = f"fcg::direction_sums_kernel<{(4, 6, 8)[var['direction']]}>"
     upd_name = ("fcg::update_residual_prefetch_kernel" if var["update"] == 3
                 else f"fcg::update_residual_kernel<{(5, 6, 8)[var['update']]}>")
+    rr_at = len(out)
     timed(f"{rr_name} (level 0)", lambda s: L.pb_residual_restrict_f32(
         l0.ea.data_ptr(), l0.rhs.data_ptr(), l0.D.data_ptr(), l0.weights.data_ptr(), l1.rhs.data_ptr(), n, s),
         16 * N + 4 * N1)
@@ -405,6 +407,8 @@ def kernel_rooflines(eng, n: int, L) -> list:
     timed(dir_name, lambda s: L.pb_fcg_direction_f64(
         l0.ea.data_ptr(), p0, p1, l0.rhs.data_ptr(), eng.screen.data_ptr(), n, eng.pw, eng.scal.data_ptr(),
         eng.flags.data_ptr(), eng.ws_ptr, eng.ws_size, s), 20 * N)
+    if n == 257:
+        out[rr_at]["traffic"] = read_profile_traffic(RESTRICT_PROFILE)
     timed(upd_name, lambda s: L.pb_fcg_update_f64(
         l0.ea.data_ptr(), p0, p1, x0, x1, eng.b.data_ptr(), eng.screen.data_ptr(), l0.rhs.data_ptr(), n, eng.pw,
         eng.scal.data_ptr(), eng.flags.data_ptr(), eng.ws_ptr, eng.ws_size, s), 48 * N)
