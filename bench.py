@@ -164,7 +164,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
 
         found = tune.autotune((1 << args.depth) + 1, device=dev, write=True)  # cached for later processes
         tuning = {k: {"chosen": v["best"], "default_us": round(v["default_s"] * 1e6, 1),
-                      "tuned_us": round(v["best_s"] * 1e6, 1)} for k, v in found.items()}
+                      "tuned_us": round(v["best_s"] * 1e6, 1)} for k, v in found.items()}  # name@side: a level
 
     def barrier():
         if dist is not None:

@@ -466,6 +466,76 @@ __global__ void __launch_bounds__(256) relax27p_kernel(const float* __restrict__
     relax27p_body<COLOUR, ZERO>(prev, next, rhs, h, inv, g, pk, blockIdx.x, blockIdx.y);
 }
 
+// The same colour pass with the neighbour planes staged in shared memory.  A
+// block owns 32 compact columns (64 x) by 8 rows of the colour's nodes and
+// marches `tz` planes; each plane of `prev` (and, for the colour-1 pass, the
+// colour-0 values of `next`) over the tile and its one-node halo is loaded
+// once, coalesced, into a ring of four planes, so a node reads its 26
+// neighbours from shared memory instead of 26 gathers.  Out-of-grid halo
+// entries read zero, as the ghosts do.  Same values, same summation order:
+// results are bit-identical to relax27p_kernel.
+constexpr int kTPi = 32, kTPy = 8, kTPRing = 4;
+constexpr int kTPW = 2 * kTPi + 4, kTPH = kTPy + 2;  // staged x from 2 i0 - 2, y from y0 - 1
+
+template <int COLOUR, bool ZERO>
+__global__ void __launch_bounds__(kTPi* kTPy) relax27p_tiled_kernel(const float* __restrict__ prev, float* next,
+                                                                    const float* __restrict__ rhs,
+                                                                    const __half* __restrict__ h,
+                                                                    const float* __restrict__ inv, Geom g, Packed pk,
+                                                                    int tz) {
+    constexpr bool kPrev = !ZERO, kNext = COLOUR == 1;
+    __shared__ float sp[kPrev ? kTPRing : 1][kTPH][kTPW];
+    __shared__ float sn[kNext ? kTPRing : 1][kTPH][kTPW];
+    const int n = g.n;
+    const int i0 = blockIdx.x * kTPi, y0 = blockIdx.y * kTPy;
+    const int z0 = blockIdx.z * tz, z1 = min(n, z0 + tz);
+    const int tid = threadIdx.x, ti = tid % kTPi, ty = tid / kTPi;
+    const int xs0 = 2 * i0 - 2, ys0 = y0 - 1;
+    auto stage = [&](int z) {  // plane z (>= -1) into ring slot (z + 1) % kTPRing
+        const int slot = (z + 1) % kTPRing;
+        for (int k = tid; k < kTPH * kTPW; k += kTPi * kTPy) {
+            const int ry = k / kTPW, rx = k - ry * kTPW;
+            const int x = xs0 + rx, y = ys0 + ry;
+            const bool ok = x >= -1 && x <= n && y >= -1 && y <= n && z <= n;
+            const int64_t o = ok ? g.at(x, y, z) : 0;
+            if (kPrev) sp[kPrev ? slot : 0][ry][rx] = ok ? prev[o] : 0.0f;
+            if (kNext) sn[kNext ? slot : 0][ry][rx] = ok && ((x + y + z) & 1) != COLOUR ? next[o] : 0.0f;
+        }
+    };
+    if (kPrev || kNext) {
+        stage(z0 - 1);
+        stage(z0);
+    }
+    const int i = i0 + ti, y = y0 + ty;
+    for (int z = z0; z < z1; ++z) {
+        if (kPrev || kNext) {
+            if (z + 1 <= n) stage(z + 1);  // into the slot of plane z - 3, last read before the previous barrier
+            __syncthreads();
+        }
+        if (i >= pk.Pc || y >= n) continue;
+        const int x = 2 * i + ((y + z + COLOUR) & 1);
+        if (x >= n) continue;
+        const int64_t p = g.at(x, y, z), q = pk.at(i, y, z);
+        float cf[26];
+        load_couplings(h, q, cf);
+        float s = 0.0f;
+#pragma unroll
+        for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+            for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+                for (int dx = -1; dx <= 1; ++dx) {
+                    if (!(dx || dy || dz)) continue;
+                    const bool other = ((dx + dy + dz) & 1) != 0;
+                    if (ZERO && !(COLOUR == 1 && other)) continue;
+                    const int sl = (z + dz + 1) % kTPRing, ry = ty + 1 + dy, rx = x + dx - xs0;
+                    const float v = (COLOUR == 1 && other) ? sn[kNext ? sl : 0][ry][rx] : sp[kPrev ? sl : 0][ry][rx];
+                    s += cf[packed_index(dx, dy, dz)] * v;
+                }
+        next[p] = inv[q] * rhs[p] + s;
+    }
+}
+
 // res = s (rhs - A e) on a packed level, one thread per node.
 __device__ __forceinline__ void residual27p_body(const float* __restrict__ e, const float* __restrict__ rhs,
                                                  const __half* __restrict__ h0, const __half* __restrict__ h1,
@@ -1001,6 +1071,24 @@ extern "C" int pb_relax27p_f32(const float* e_prev, float* e_next, const float* 
     const dim3 block(256);
     const dim3 grid((pk.Pc * (int)n + 255) / 256, (int)n);
     const __half *a = (const __half*)h0, *b = (const __half*)h1;
+    if (tuned(PB_TUNE_RELAX27_VARIANT, n, 0) == 1) {  // shared-memory staged neighbours
+        const int tiles = ((pk.Pc + kTPi - 1) / kTPi) * (((int)n + kTPy - 1) / kTPy);
+        const int64_t want = 2LL * 8 * kSMs;  // about two waves of 8 resident blocks per SM
+        int tz = (int)(((int64_t)n * tiles + want - 1) / want);
+        tz = tz < 2 ? 2 : (tz > 16 ? 16 : tz);
+        const dim3 tg((pk.Pc + kTPi - 1) / kTPi, ((int)n + kTPy - 1) / kTPy, ((int)n + tz - 1) / tz);
+        if (e_prev) {
+            relax27p_tiled_kernel<0, false><<<tg, kTPi * kTPy, 0, s>>>(e_prev, e_next, rhs, a, inv0, g, pk, tz);
+            PB_CHECK_LAUNCH("relax27p_tiled_kernel");
+            relax27p_tiled_kernel<1, false><<<tg, kTPi * kTPy, 0, s>>>(e_prev, e_next, rhs, b, inv1, g, pk, tz);
+        } else {
+            relax27p_kernel<0, true><<<grid, block, 0, s>>>(nullptr, e_next, rhs, a, inv0, g, pk);  // no neighbours
+            PB_CHECK_LAUNCH("relax27p_kernel");
+            relax27p_tiled_kernel<1, true><<<tg, kTPi * kTPy, 0, s>>>(nullptr, e_next, rhs, b, inv1, g, pk, tz);
+        }
+        PB_CHECK_LAUNCH("relax27p_tiled_kernel");
+        return PB_OK;
+    }
     if (e_prev) {
         relax27p_kernel<0, false><<<grid, block, 0, s>>>(e_prev, e_next, rhs, a, inv0, g, pk);
         PB_CHECK_LAUNCH("relax27p_kernel");

@@ -298,7 +298,9 @@ def apply_tuning(lib, n: int, device: torch.device) -> None:
         return
     from . import tune
 
-    tune.apply(lib, tune.gpu_name(device), n)
+    gpu = tune.gpu_name(device)
+    for side in level_sizes(n):  # per-level parameters are cached under each level's side
+        tune.apply(lib, gpu, side)
     _TUNED.add(key)
 
 

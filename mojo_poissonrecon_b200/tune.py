@@ -29,18 +29,21 @@ import statistics
 import threading
 
 (SWEEP_Z_CHUNK, RESTRICT_PLANES, PROLONG_PLANES, FCG_DIRECTION_PLANES, FCG_UPDATE_PLANES, FCG_DIRECTION_VARIANT,
- FCG_UPDATE_VARIANT, SWEEP_VARIANT, RESTRICT_VARIANT) = range(9)
+ FCG_UPDATE_VARIANT, SWEEP_VARIANT, RESTRICT_VARIANT, RELAX27_VARIANT) = range(10)
 NAMES = {SWEEP_Z_CHUNK: "sweep_z_chunk", RESTRICT_PLANES: "restrict_planes", PROLONG_PLANES: "prolong_planes",
          FCG_DIRECTION_PLANES: "fcg_direction_planes", FCG_UPDATE_PLANES: "fcg_update_planes",
          FCG_DIRECTION_VARIANT: "fcg_direction_variant", FCG_UPDATE_VARIANT: "fcg_update_variant",
-         SWEEP_VARIANT: "sweep_variant", RESTRICT_VARIANT: "restrict_variant"}
+         SWEEP_VARIANT: "sweep_variant", RESTRICT_VARIANT: "restrict_variant",
+         RELAX27_VARIANT: "relax27_variant"}
 # Searched by autotune(): the parameters that never change results.  The FCG
 # passes' planes per block also set the shape of their partial-sum trees, so a
 # different value changes the inner products (and the iterates) by rounding;
 # they stay at the built-in 24 unless set explicitly.
 # The sweep's variant comes first: the z chunk is then searched for the variant chosen.
 SEARCHED = (SWEEP_VARIANT, SWEEP_Z_CHUNK, RESTRICT_VARIANT, RESTRICT_PLANES, PROLONG_PLANES, FCG_DIRECTION_VARIANT,
-            FCG_UPDATE_VARIANT)
+            FCG_UPDATE_VARIANT, RELAX27_VARIANT)
+# Searched per packed level side of the hierarchy (not per the top side).
+PER_LEVEL = (RELAX27_VARIANT,)
 _LOCK = threading.Lock()
 
 
@@ -71,7 +74,7 @@ def candidates(param: int, n: int) -> list[int]:
         return [0, 1, 2, 3]
     if param == SWEEP_VARIANT:
         return [0, 1, 2]
-    if param == RESTRICT_VARIANT:
+    if param in (RESTRICT_VARIANT, RELAX27_VARIANT):
         return [0, 1]
     raise ValueError(f"unknown tuning parameter {param}")
 
@@ -182,13 +185,26 @@ def autotune(n: int, device=None, repeats: int = 10, params=None, path: str | No
                                                        l0.rhs.data_ptr(), n, 4.0, scal.data_ptr(), flags.data_ptr(),
                                                        ws_ptr, ws_size, s), "fcg update")
 
+    def level_launch(lv):  # one packed sweep on level lv, from its own work arrays
+        return lambda: nat.check(lib.pb_relax27p_f32(lv.ea.data_ptr(), lv.eb.data_ptr(), lv.rhs.data_ptr(),
+                                                     *lv.packed_ptrs(), lv.n, s), "relax27p")
+
+    jobs = []  # (param, side, launch, result name)
+    for param in params:
+        if param in PER_LEVEL:
+            for lv in h.levels:
+                if lv.packed is not None:
+                    for t in (lv.ea, lv.rhs):
+                        t.uniform_(0.0, 1.0, generator=gen)
+                    jobs.append((param, lv.n, level_launch(lv), f"{NAMES[param]}@{lv.n}"))
+        else:
+            jobs.append((param, n, launch(param), NAMES[param]))
     result = {}
     with _LOCK:
-        for param in params:
-            fn = launch(param)
+        for param, side, fn, name in jobs:
 
-            def time_one(value, fn=fn, param=param):
-                nat.check(lib.pb_tune_set(param, n, value), "tune set")
+            def time_one(value, fn=fn, param=param, side=side):
+                nat.check(lib.pb_tune_set(param, side, value), "tune set")
                 a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 a.record(stream)
                 fn()
@@ -197,16 +213,19 @@ def autotune(n: int, device=None, repeats: int = 10, params=None, path: str | No
                 e.synchronize()
                 return a.elapsed_time(e) / 2e3
 
-            best, timings = search(param, n, time_one, repeats=repeats)
-            nat.check(lib.pb_tune_set(param, n, best), "tune set")
-            result[NAMES[param]] = {"best": best, "default_s": timings[0], "best_s": timings[best],
-                                    "timings": {str(k): v for k, v in sorted(timings.items())}}
+            best, timings = search(param, side, time_one, repeats=repeats)
+            nat.check(lib.pb_tune_set(param, side, best), "tune set")
+            result[name] = {"best": best, "default_s": timings[0], "best_s": timings[best], "side": side,
+                            "timings": {str(k): v for k, v in sorted(timings.items())}}
         if status.item():
             raise RuntimeError("autotune: a bounded TMA wait gave up during the measurement")
         if write:
             entries = load_cache(path)
-            entries[cache_key(gpu_name(dev), n)] = {k: {"best": v["best"], "best_s": v["best_s"],
-                                                        "default_s": v["default_s"]} for k, v in result.items()}
+            gpu = gpu_name(dev)
+            for name, v in result.items():
+                key = cache_key(gpu, v["side"])
+                entries.setdefault(key, {})[name.split("@")[0]] = {"best": v["best"], "best_s": v["best_s"],
+                                                                   "default_s": v["default_s"]}
             store_cache(entries, path)
     return result
 

@@ -212,3 +212,40 @@ def test_full_cycle(L, n):
     h.check_status()
     want = mg.v_cycle(ops, ws, sizes, 0, rhs, coarse_sweeps=h.coarse_sweeps)
     assert np.abs(got - want).max() <= 1e-4 * np.abs(want).max()
+
+
+@pytest.mark.parametrize("n", [17, 65, 129])
+def test_relax27p_tiled_variant_bit_identical(n):
+    """The shared-memory staged packed sweep (tuner variant) gives the same bits
+    as the gather kernel, from zero and from a previous iterate."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from mojo_poissonrecon_b200 import _native, solver32, tune
+
+    L = _native.lib()
+    dev = torch.device("cuda")
+    h = solver32.Hierarchy32(2 * n - 1, dev)
+    rng = torch.Generator(device=dev).manual_seed(n)
+    screen = torch.rand((2 * n - 1,) * 3, dtype=torch.float64, device=dev, generator=rng) * 3
+    h.setup(screen, 4.0)
+    lv = h.levels[1]
+    assert lv.n == n and lv.packed is not None
+    lv.rhs.copy_(torch.randn(lv.rhs.shape, device=dev, generator=rng) * (lv.invD != 0))
+    lv.ea.copy_(torch.randn(lv.ea.shape, device=dev, generator=rng) * (lv.invD != 0))
+    s = torch.cuda.current_stream().cuda_stream
+
+    def sweep(zero):
+        out = torch.zeros_like(lv.ea)
+        assert L.pb_relax27p_f32(None if zero else lv.ea.data_ptr(), out.data_ptr(), lv.rhs.data_ptr(),
+                                 *lv.packed_ptrs(), n, s) == 0
+        return out
+
+    L.pb_tune_clear()
+    try:
+        want = [sweep(False), sweep(True)]
+        L.pb_tune_set(tune.RELAX27_VARIANT, n, 1)
+        got = [sweep(False), sweep(True)]
+        assert torch.equal(got[0], want[0]) and torch.equal(got[1], want[1])
+    finally:
+        L.pb_tune_clear()
