@@ -432,6 +432,8 @@ int pb_batch_loop_condition(unsigned long long handle, const double *scal, const
  *                          plane in one loop over their items
  *   RELAX27_VARIANT        pb_relax27p_f32 (per level side): 1 = the neighbour planes
  *                          staged in shared memory
+ *   RESIDUAL27_VARIANT     pb_residual_restrict27p_f32 (per level side): 1 = the
+ *                          residual with e's planes staged in shared memory
  *   SWEEP_VARIANT          pb_sweep_tma_f32: 0 = a 5-plane shared ring with 2 resident
  *                          blocks per SM, 1 = 4 planes with 3 blocks, 2 = 3 planes with 3
  *   FCG_UPDATE_VARIANT     pb_fcg_update_f64: 0 = 5 resident blocks per SM,
@@ -452,7 +454,8 @@ enum {
     PB_TUNE_SWEEP_VARIANT = 7,
     PB_TUNE_RESTRICT_VARIANT = 8,
     PB_TUNE_RELAX27_VARIANT = 9,
-    PB_TUNE_PARAMS = 10
+    PB_TUNE_RESIDUAL27_VARIANT = 10,
+    PB_TUNE_PARAMS = 11
 };
 int pb_tune_set(int64_t param, int64_t n, int64_t value);
 int64_t pb_tune_get(int64_t param, int64_t n);

@@ -574,6 +574,59 @@ __global__ void __launch_bounds__(256) residual27p_kernel(const float* __restric
     residual27p_body(e, rhs, h0, h1, i0, i1, fac, g, pk, res, blockIdx.x, blockIdx.y);
 }
 
+// The packed residual with e's planes staged in shared memory: a block owns a
+// 64 x 4 tile of nodes (both colours) and marches `tz` planes with a ring of
+// four planes of e over the tile and its halo; same values and order as
+// residual27p_kernel, so bit-identical results.
+constexpr int kTRx = 64, kTRy = 4;
+constexpr int kTRW = kTRx + 4, kTRH = kTRy + 2;  // staged x from x0 - 2, y from y0 - 1
+
+__global__ void __launch_bounds__(kTRx* kTRy) residual27p_tiled_kernel(
+    const float* __restrict__ e, const float* __restrict__ rhs, const __half* __restrict__ h0,
+    const __half* __restrict__ h1, const float* __restrict__ i0, const float* __restrict__ i1,
+    const float* __restrict__ fac, Geom g, Packed pk, float* __restrict__ res, int tz) {
+    __shared__ float se[kTPRing][kTRH][kTRW];
+    const int n = g.n;
+    const int x0 = blockIdx.x * kTRx, y0 = blockIdx.y * kTRy;
+    const int z0 = blockIdx.z * tz, z1 = min(n, z0 + tz);
+    const int tid = threadIdx.x, tx = tid % kTRx, ty = tid / kTRx;
+    const int xs0 = x0 - 2, ys0 = y0 - 1;
+    auto stage = [&](int z) {
+        const int slot = (z + 1) % kTPRing;
+        for (int k = tid; k < kTRH * kTRW; k += kTRx * kTRy) {
+            const int ry = k / kTRW, rx = k - ry * kTRW;
+            const int x = xs0 + rx, y = ys0 + ry;
+            const bool ok = x >= -1 && x <= n && y >= -1 && y <= n && z <= n;
+            se[slot][ry][rx] = ok ? e[g.at(x, y, z)] : 0.0f;
+        }
+    };
+    stage(z0 - 1);
+    stage(z0);
+    const int x = x0 + tx, y = y0 + ty;
+    for (int z = z0; z < z1; ++z) {
+        if (z + 1 <= n) stage(z + 1);
+        __syncthreads();
+        if (x >= n || y >= n) continue;
+        const int colour = (x + y + z) & 1;
+        const __half* __restrict__ h = colour ? h1 : h0;
+        const int64_t p = g.at(x, y, z), q = pk.at(x >> 1, y, z);
+        float cf[26];
+        load_couplings(h, q, cf);
+        float s = 0.0f;
+#pragma unroll
+        for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+            for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+                for (int dx = -1; dx <= 1; ++dx) {
+                    if (!(dx || dy || dz)) continue;
+                    s += cf[packed_index(dx, dy, dz)] * se[(z + dz + 1) % kTPRing][ty + 1 + dy][tx + 2 + dx];
+                }
+        const float inv = colour ? i1[q] : i0[q];
+        res[p] = fac[p] * (rhs[p] - (se[(z + 1) % kTPRing][ty + 1][tx + 2] - s) / inv);
+    }
+}
+
 // ---- exact solve on the 3^3 level -----------------------------------------------
 // The 27 x 27 operator of the coarsest level inverted once per set-up by one
 // warp: FP64 Gauss-Jordan without pivoting (the Galerkin operator is
@@ -1110,10 +1163,20 @@ extern "C" int pb_residual_restrict27p_f32(const float* e, const float* rhs, con
         return fail(PB_ERR_INVALID, "residual_restrict27p: bad args");
     cudaStream_t s = (cudaStream_t)stream;
     const int fn = (int)n, cn = (fn + 1) / 2;
-    residual27p_kernel<<<dim3((fn * fn + 255) / 256, fn), 256, 0, s>>>(e, rhs, (const __half*)h0, (const __half*)h1,
-                                                                     inv0, inv1, weights, geom(fn), packed_of(fn),
-                                                                     res);
-    PB_CHECK_LAUNCH("residual27p_kernel");
+    if (tuned(PB_TUNE_RESIDUAL27_VARIANT, n, 0) == 1) {  // shared-memory staged e planes
+        const int tiles = ((fn + kTRx - 1) / kTRx) * ((fn + kTRy - 1) / kTRy);
+        const int64_t want = 2LL * 8 * kSMs;
+        int tz = (int)(((int64_t)fn * tiles + want - 1) / want);
+        tz = tz < 2 ? 2 : (tz > 16 ? 16 : tz);
+        const dim3 tg((fn + kTRx - 1) / kTRx, (fn + kTRy - 1) / kTRy, (fn + tz - 1) / tz);
+        residual27p_tiled_kernel<<<tg, kTRx * kTRy, 0, s>>>(e, rhs, (const __half*)h0, (const __half*)h1, inv0, inv1,
+                                                           weights, geom(fn), packed_of(fn), res, tz);
+        PB_CHECK_LAUNCH("residual27p_tiled_kernel");
+    } else {
+        residual27p_kernel<<<dim3((fn * fn + 255) / 256, fn), 256, 0, s>>>(
+            e, rhs, (const __half*)h0, (const __half*)h1, inv0, inv1, weights, geom(fn), packed_of(fn), res);
+        PB_CHECK_LAUNCH("residual27p_kernel");
+    }
     restrict27_kernel<<<plane_grid(cn, 256), 256, 0, s>>>(res, geom(fn), coarse_rhs, geom(cn));
     PB_CHECK_LAUNCH("restrict27_kernel");
     return PB_OK;

@@ -29,21 +29,21 @@ import statistics
 import threading
 
 (SWEEP_Z_CHUNK, RESTRICT_PLANES, PROLONG_PLANES, FCG_DIRECTION_PLANES, FCG_UPDATE_PLANES, FCG_DIRECTION_VARIANT,
- FCG_UPDATE_VARIANT, SWEEP_VARIANT, RESTRICT_VARIANT, RELAX27_VARIANT) = range(10)
+ FCG_UPDATE_VARIANT, SWEEP_VARIANT, RESTRICT_VARIANT, RELAX27_VARIANT, RESIDUAL27_VARIANT) = range(11)
 NAMES = {SWEEP_Z_CHUNK: "sweep_z_chunk", RESTRICT_PLANES: "restrict_planes", PROLONG_PLANES: "prolong_planes",
          FCG_DIRECTION_PLANES: "fcg_direction_planes", FCG_UPDATE_PLANES: "fcg_update_planes",
          FCG_DIRECTION_VARIANT: "fcg_direction_variant", FCG_UPDATE_VARIANT: "fcg_update_variant",
          SWEEP_VARIANT: "sweep_variant", RESTRICT_VARIANT: "restrict_variant",
-         RELAX27_VARIANT: "relax27_variant"}
+         RELAX27_VARIANT: "relax27_variant", RESIDUAL27_VARIANT: "residual27_variant"}
 # Searched by autotune(): the parameters that never change results.  The FCG
 # passes' planes per block also set the shape of their partial-sum trees, so a
 # different value changes the inner products (and the iterates) by rounding;
 # they stay at the built-in 24 unless set explicitly.
 # The sweep's variant comes first: the z chunk is then searched for the variant chosen.
 SEARCHED = (SWEEP_VARIANT, SWEEP_Z_CHUNK, RESTRICT_VARIANT, RESTRICT_PLANES, PROLONG_PLANES, FCG_DIRECTION_VARIANT,
-            FCG_UPDATE_VARIANT, RELAX27_VARIANT)
+            FCG_UPDATE_VARIANT, RELAX27_VARIANT, RESIDUAL27_VARIANT)
 # Searched per packed level side of the hierarchy (not per the top side).
-PER_LEVEL = (RELAX27_VARIANT,)
+PER_LEVEL = (RELAX27_VARIANT, RESIDUAL27_VARIANT)
 _LOCK = threading.Lock()
 
 
@@ -74,7 +74,7 @@ def candidates(param: int, n: int) -> list[int]:
         return [0, 1, 2, 3]
     if param == SWEEP_VARIANT:
         return [0, 1, 2]
-    if param in (RESTRICT_VARIANT, RELAX27_VARIANT):
+    if param in (RESTRICT_VARIANT, RELAX27_VARIANT, RESIDUAL27_VARIANT):
         return [0, 1]
     raise ValueError(f"unknown tuning parameter {param}")
 
@@ -185,18 +185,23 @@ def autotune(n: int, device=None, repeats: int = 10, params=None, path: str | No
                                                        l0.rhs.data_ptr(), n, 4.0, scal.data_ptr(), flags.data_ptr(),
                                                        ws_ptr, ws_size, s), "fcg update")
 
-    def level_launch(lv):  # one packed sweep on level lv, from its own work arrays
-        return lambda: nat.check(lib.pb_relax27p_f32(lv.ea.data_ptr(), lv.eb.data_ptr(), lv.rhs.data_ptr(),
-                                                     *lv.packed_ptrs(), lv.n, s), "relax27p")
+    def level_launch(param, lv, nxt):  # one packed sweep or residual-restriction on level lv
+        if param == RELAX27_VARIANT:
+            return lambda: nat.check(lib.pb_relax27p_f32(lv.ea.data_ptr(), lv.eb.data_ptr(), lv.rhs.data_ptr(),
+                                                         *lv.packed_ptrs(), lv.n, s), "relax27p")
+        return lambda: nat.check(lib.pb_residual_restrict27p_f32(lv.ea.data_ptr(), lv.rhs.data_ptr(),
+                                                                 *lv.packed_ptrs(), lv.weights.data_ptr(), lv.n,
+                                                                 lv.res.data_ptr(), nxt.rhs.data_ptr(), s),
+                                 "residual_restrict27p")
 
     jobs = []  # (param, side, launch, result name)
     for param in params:
         if param in PER_LEVEL:
-            for lv in h.levels:
+            for lv, nxt in zip(h.levels[:-1], h.levels[1:]):
                 if lv.packed is not None:
                     for t in (lv.ea, lv.rhs):
                         t.uniform_(0.0, 1.0, generator=gen)
-                    jobs.append((param, lv.n, level_launch(lv), f"{NAMES[param]}@{lv.n}"))
+                    jobs.append((param, lv.n, level_launch(param, lv, nxt), f"{NAMES[param]}@{lv.n}"))
         else:
             jobs.append((param, n, launch(param), NAMES[param]))
     result = {}

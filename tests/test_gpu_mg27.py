@@ -215,9 +215,9 @@ def test_full_cycle(L, n):
 
 
 @pytest.mark.parametrize("n", [17, 65, 129])
-def test_relax27p_tiled_variant_bit_identical(n):
-    """The shared-memory staged packed sweep (tuner variant) gives the same bits
-    as the gather kernel, from zero and from a previous iterate."""
+def test_packed_level_tiled_variants_bit_identical(n):
+    """The shared-memory staged packed sweep and residual (tuner variants) give
+    the same bits as the gather kernels, from zero and from a previous iterate."""
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
@@ -241,11 +241,20 @@ def test_relax27p_tiled_variant_bit_identical(n):
                                  *lv.packed_ptrs(), n, s) == 0
         return out
 
+    def residual():
+        res = torch.zeros_like(lv.ea)
+        coarse = torch.zeros_like(h.levels[2].rhs)
+        assert L.pb_residual_restrict27p_f32(lv.ea.data_ptr(), lv.rhs.data_ptr(), *lv.packed_ptrs(),
+                                             lv.weights.data_ptr(), n, res.data_ptr(), coarse.data_ptr(), s) == 0
+        return res, coarse
+
     L.pb_tune_clear()
     try:
-        want = [sweep(False), sweep(True)]
+        want = [sweep(False), sweep(True), *residual()]
         L.pb_tune_set(tune.RELAX27_VARIANT, n, 1)
-        got = [sweep(False), sweep(True)]
-        assert torch.equal(got[0], want[0]) and torch.equal(got[1], want[1])
+        L.pb_tune_set(tune.RESIDUAL27_VARIANT, n, 1)
+        got = [sweep(False), sweep(True), *residual()]
+        for a, b in zip(got, want):
+            assert torch.equal(a, b)
     finally:
         L.pb_tune_clear()

@@ -57,7 +57,7 @@ def test_cache_round_trip_and_apply(tmp_path):
         lib.pb_tune_clear()
 
 
-@pytest.mark.parametrize("args", [(10, 257, 4), (-1, 257, 4), (0, 1, 4), (0, 257, -2), (0, 257, 5000)])
+@pytest.mark.parametrize("args", [(11, 257, 4), (-1, 257, 4), (0, 1, 4), (0, 257, -2), (0, 257, 5000)])
 def test_tune_table_rejects_bad_entries(args):
     from mojo_poissonrecon_b200 import _native
 
