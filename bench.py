@@ -34,7 +34,11 @@ import sys
 import tempfile
 import time
 
+import faulthandler
+
 import numpy as np
+
+faulthandler.enable()  # a crash in native code prints every thread's Python stack
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
@@ -647,7 +651,8 @@ def run_serving(args) -> dict:
     batch.reconstruct_many([(pool[0][0], pool[0][1], d) for d in (6, 7, 8, 9)], tol=TOL)  # modules, attributes
     torch.cuda.synchronize()
     lanes = max(1, args.lanes)
-    with serve.Server(lanes=lanes) as server:
+    sizes = lambda mesh: (int(mesh.vertices.shape[0]), int(mesh.faces.shape[0]))  # meshes are not kept
+    with serve.Server(lanes=lanes, on_result=sizes) as server:
         t0 = time.perf_counter()
         futures = []
         for k, (arrival, _, depth, _, _) in enumerate(stream):

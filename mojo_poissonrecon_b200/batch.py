@@ -33,8 +33,10 @@ cloud, and every kernel is deterministic.
 
 from __future__ import annotations
 
+import collections
 import ctypes
 import math
+import threading
 
 import numpy as np
 import torch
@@ -42,7 +44,8 @@ import torch
 from . import _native as nat
 from . import _sync, core
 from .solver import SolveStats, norm
-from .solver32 import MAX_ITER, TMA_MIN_N, Hierarchy32, apply_tuning, galerkin_scratch_bytes, level0_sweeps
+from .solver32 import (GRAPH_CAPTURE_LOCK, MAX_ITER, TMA_MIN_N, Hierarchy32, apply_tuning, galerkin_scratch_bytes,
+                       level0_sweeps)
 
 # descriptor kinds (include/poisson_b200.h)
 SWEEP, SWEEP_ZERO, PROLONG32, RESIDUAL_RESTRICT32 = 0, 1, 2, 3
@@ -89,15 +92,70 @@ class _Launch:
 
 
 class _Cloud:
-    """One cloud's solver state: its FP32 hierarchy and FP64/FP32 FCG vectors."""
+    """One cloud's solver state: its FP32 hierarchy and FP64/FP32 FCG vectors.
+    Every solve overwrites all of it (the hierarchy's ghosts stay zero), so a
+    cloud state of the same side can serve any later batch."""
 
     def __init__(self, n: int, device: torch.device, galerkin_ws: torch.Tensor):
         self.n = n
+        self.device = device
         self.h = Hierarchy32(n, device, galerkin_ws=galerkin_ws)
         f64 = lambda: torch.empty((n, n, n), dtype=torch.float64, device=device)
         f32 = lambda: torch.empty((n, n, n), dtype=torch.float32, device=device)
         self.xs = (f64(), f64())
         self.ps = (f32(), f32())
+        self.nbytes = self.h.nbytes() - self.h.galerkin_ws.numel() * 4 + 12 * n ** 3 * 2
+
+
+# Cloud states of finished batches, per (device, side), reused by later ones
+# (allocating a batch's hierarchies costs about 20 tensors per level per cloud);
+# at most POOL_FRACTION of the device's memory, least recently returned first out.
+POOL_FRACTION = 0.25
+_POOL: "collections.OrderedDict[int, _Cloud]" = collections.OrderedDict()
+_POOL_LOCK = threading.Lock()
+_STREAMS = threading.local()
+
+
+def _stream(device: torch.device) -> torch.cuda.Stream:
+    """This thread's stream for batched solves on `device`: one for the life of
+    the thread, so the caching allocator reuses the memory of earlier batches."""
+    table = getattr(_STREAMS, "by_device", None)
+    if table is None:
+        table = _STREAMS.by_device = {}
+    if device.index not in table:
+        table[device.index] = torch.cuda.Stream(device=device)
+    return table[device.index]
+
+
+def _take_cloud(n: int, device: torch.device, galerkin_ws: torch.Tensor) -> _Cloud:
+    with _POOL_LOCK:
+        for key, c in _POOL.items():
+            if c.n == n and c.device == device:
+                del _POOL[key]
+                c.h.galerkin_ws = galerkin_ws  # the batch's own scratch: batches on other lanes run concurrently
+                return c
+    return _Cloud(n, device, galerkin_ws)
+
+
+def _return_clouds(clouds) -> None:
+    if not clouds:
+        return
+    device = clouds[0].device
+    cap = POOL_FRACTION * torch.cuda.get_device_properties(device).total_memory
+    with _POOL_LOCK:
+        for c in clouds:
+            c.h.galerkin_ws = None  # not kept alive by the pool
+            _POOL[id(c)] = c
+        total = sum(c.nbytes for c in _POOL.values())
+        while _POOL and total > cap:
+            _, c = _POOL.popitem(last=False)
+            total -= c.nbytes
+
+
+def clear_pool() -> None:
+    """Drop every pooled cloud state (their memory returns to torch's cache)."""
+    with _POOL_LOCK:
+        _POOL.clear()
 
 
 class BatchSolver:
@@ -118,12 +176,12 @@ class BatchSolver:
                 raise ValueError(f"batched solves need sides 2^d + 1 >= {TMA_MIN_N} (got {n})")
         for n in set(self.sides):
             apply_tuning(self.lib, n, self.device)
-        self.stream = torch.cuda.Stream(device=self.device)
+        self.stream = _stream(self.device)
         K = len(self.sides)
         with torch.cuda.stream(self.stream):
             scratch = max(galerkin_scratch_bytes(n) for n in set(self.sides))
             self.galerkin_ws = torch.empty((scratch + 3) // 4, dtype=torch.float32, device=self.device)
-            self.clouds = [_Cloud(n, self.device, self.galerkin_ws) for n in self.sides]
+            self.clouds = [_take_cloud(n, self.device, self.galerkin_ws) for n in self.sides]
             self.flags = torch.zeros((K, 4), dtype=torch.int32, device=self.device)
             self.scal = torch.zeros((K, 8), dtype=torch.float64, device=self.device)
             self.ctrl = torch.zeros((K, 2), dtype=torch.float64, device=self.device)
@@ -143,6 +201,13 @@ class BatchSolver:
         self.exec = ctypes.c_void_p()
         self.body_launches = 0
         self.launches = []
+
+    def release(self) -> None:
+        """Hand the cloud states to the pool for later batches (after the solve's
+        results have been read: the caller's stream has waited for this one)."""
+        self.stream.synchronize()
+        clouds, self.clouds = self.clouds, []
+        _return_clouds(clouds)
 
     def __del__(self):
         try:
@@ -245,6 +310,10 @@ class BatchSolver:
                                                    self.history.data_ptr(), s), "batch loop condition")
 
     def _capture(self) -> None:
+        with GRAPH_CAPTURE_LOCK:
+            self._capture_locked()
+
+    def _capture_locked(self) -> None:
         L = self.lib
         s = nat.stream_handle()
         handle = ctypes.c_ulonglong()
@@ -476,6 +545,7 @@ def _run_wave(wave, out, dev, point_weight, confidence, scale, samples_per_node,
                              point_weight, tol=tol, max_cycles=max_cycles, phases=phases)
         for j, fj, sj in zip(solve_idx, f, st):
             fields[j], stats[j] = fj, sj
+        solver.release()
         del solver
     phases.mark("solve")
     # iso-values and extraction counts for every cloud, then one read of all counts

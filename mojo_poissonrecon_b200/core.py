@@ -147,7 +147,12 @@ def _host_all(tensors, device_out: bool) -> list:
             total += (nbytes + 63) // 64 * 64
         else:
             slots.append(-1)
-    buf = torch.empty(total, dtype=torch.uint8, pin_memory=True) if total else None
+    buf = None
+    if total:
+        try:
+            buf = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+        except RuntimeError:  # page-locked memory refused: pageable copies instead
+            slots = [-1] * len(slots)
     out = []
     for t, off in zip(tensors, slots):
         if off >= 0:

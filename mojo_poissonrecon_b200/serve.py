@@ -135,7 +135,8 @@ class Server:
 
     def __init__(self, lanes: int = 2, memory_fraction: float = 0.6, device: int | None = None,
                  budget_bytes: int | None = None, runner=None, batch_runner=None, max_batch: int = 64,
-                 drain_limit_s: float = 600.0, group_depths: bool = True, lookahead: int = 256, **defaults):
+                 drain_limit_s: float = 600.0, group_depths: bool = True, lookahead: int = 256, on_result=None,
+                 **defaults):
         """runner: optional callable(points, normals, **kwargs) -> result that
         replaces one GPU reconstruction; batch_runner: optional callable(list of
         (points, normals, kwargs)) -> list of results (or exceptions) that
@@ -145,7 +146,10 @@ class Server:
         drain_limit_s bounds how long a lane waits for the device work of a
         request that overran its deadline before it gives the lane up.
         group_depths: a batch takes requests of its head's depth only;
-        lookahead: how many queued requests behind the head a lane scans."""
+        lookahead: how many queued requests behind the head a lane scans.
+        on_result: optional callable(mesh) -> value that the future gets in the
+        mesh's place (a caller that writes meshes out or keeps only their sizes
+        need not hold every mesh until it reads its future)."""
         if lanes < 1:
             raise ValueError("lanes must be positive")
         if max_batch < 1:
@@ -156,6 +160,7 @@ class Server:
         self.drain_limit_s = float(drain_limit_s)
         self.group_depths = bool(group_depths)
         self.lookahead = int(lookahead)
+        self.on_result = on_result
         self._fake = runner is not None or batch_runner is not None
         if not self._fake:
             self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
@@ -293,6 +298,12 @@ class Server:
         elif req.deadline is not None and time.monotonic() > req.deadline:
             req.future.set_exception(_sync.DeadlineExceeded("the request finished after its deadline"))
         else:
+            if self.on_result is not None:
+                try:
+                    result = self.on_result(result)
+                except BaseException as error:
+                    req.future.set_exception(error)
+                    return
             req.future.set_result((result, req.timing))
 
     def _run_one(self, req: _Request):

@@ -72,6 +72,11 @@ EAGER_LOOP = False
 # once as a CUDA graph and replays it.
 SETUP_GRAPH = True
 
+# Graph captures (the iteration loops here and in batch.py, the prologue graph)
+# run one at a time in the process: serving lanes capture on their own
+# streams, and the capture APIs are kept out of each other's way.
+GRAPH_CAPTURE_LOCK = threading.RLock()
+
 # When set to a list, every finest-level sweep launched eagerly appends
 # (start, end, mode) CUDA events recorded on the launching stream around it.
 PROBE: list | None = None
@@ -402,6 +407,10 @@ class RefinedEngine:
 
     def _capture(self) -> None:
         """Capture one iteration as the body of a device-evaluated WHILE loop."""
+        with GRAPH_CAPTURE_LOCK:
+            self._capture_locked()
+
+    def _capture_locked(self) -> None:
         L = self.lib
         s = nat.stream_handle()
         handle = ctypes.c_ulonglong()
@@ -467,12 +476,13 @@ class RefinedEngine:
         if self.setup_graph is None:
             self._prologue()
             g = torch.cuda.CUDAGraph()
-            before = self.lib.pb_launch_count()
-            g.capture_begin(capture_error_mode="thread_local")  # other threads (serving lanes) stay free
-            try:
-                self._prologue()
-            finally:
-                g.capture_end()
+            with GRAPH_CAPTURE_LOCK:
+                before = self.lib.pb_launch_count()
+                g.capture_begin(capture_error_mode="thread_local")  # other threads (serving lanes) stay free
+                try:
+                    self._prologue()
+                finally:
+                    g.capture_end()
             self.prologue_launches = self.lib.pb_launch_count() - before
             self.setup_graph = g
         self.setup_graph.replay()
@@ -586,7 +596,11 @@ def engine_for(n: int, point_weight: float, device: torch.device, slot: int | No
 
 
 def clear_engines() -> None:
+    """Drop the cached engines and the batched solver's pooled cloud states."""
     _ENGINES.clear()
+    from . import batch
+
+    batch.clear_pool()
 
 
 def solve_refined(rhs: torch.Tensor, screen: torch.Tensor, point_weight: float, workspace: nat.Workspace, *,

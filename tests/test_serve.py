@@ -332,3 +332,11 @@ def test_same_result_alone_and_in_the_mix():
         assert np.array_equal(a.vertices, b.vertices)
         assert np.array_equal(a.faces, b.faces)
         assert a.iso_value == b.iso_value and a.residual_norm == b.residual_norm
+
+
+def test_on_result_replaces_the_result():
+    server = serve.Server(lanes=1, budget_bytes=1 << 40, runner=lambda p, n, **kw: kw["tag"] * 2, max_batch=1,
+                          on_result=lambda r: r + 1)
+    f = server.submit(*cloud(), depth=6, tag=5)
+    assert f.result(timeout=10)[0] == 11
+    server.close()
