@@ -113,3 +113,21 @@ def test_reconstruct_many_in_waves_matches_one_wave():
     many = batch.reconstruct_many(clouds, tol=1e-8, budget_bytes=1)  # every cloud its own wave
     for a, b in zip(one, many):
         assert np.array_equal(a.vertices, b.vertices) and np.array_equal(a.faces, b.faces)
+
+
+def test_batch_with_a_depth9_cloud_matches_single_reconstructions():
+    """A 513^3 cloud in a batch beside smaller ones: meshes identical to
+    core.reconstruct alone (whose depth-9 engine runs lean)."""
+    import mojo_poissonrecon_b200 as mpr
+    from mojo_poissonrecon_b200 import batch, workloads
+
+    rng = np.random.default_rng(29)
+    clouds = []
+    for depth, count in ((9, 120_000), (6, 20_000), (8, 60_000)):
+        p, n = workloads.torus(count, major=0.5, minor=0.2, noise=0.0, confidence=None, rng=rng)
+        clouds.append((p, n, depth))
+    meshes = batch.reconstruct_many(clouds, tol=1e-8)
+    for (p, n, d), mesh in zip(clouds, meshes):
+        want = mpr.reconstruct(p, n, depth=d, precision="fp32_refined", tol=1e-8)
+        assert np.array_equal(mesh.vertices, want.vertices) and np.array_equal(mesh.faces, want.faces), d
+        assert mesh.residual_norm == want.residual_norm
