@@ -309,7 +309,8 @@ def apply_tuning(lib, n: int, device: torch.device) -> None:
     _TUNED.add(key)
 
 
-LEAN_MIN_N = 513  # engines of this side or larger run lean (RefinedEngine)
+LEAN_MIN_N = 513  # engines of this side or larger run lean (RefinedEngine) and are not cached
+_WARM: set = set()  # (device, side) whose kernels have run once outside a capture
 
 
 class RefinedEngine:
@@ -360,7 +361,6 @@ class RefinedEngine:
         self.graph = ctypes.c_void_p()
         self.exec = ctypes.c_void_p()
         self.setup_graph = None
-        self._warm = False
         self.prologue_launches = 0
         self.body_launches = 0
 
@@ -529,12 +529,14 @@ class RefinedEngine:
                         break
             else:
                 if not self.exec.value:
-                    if not self._warm:
-                        # one eager iteration first sets kernel attributes outside the
-                        # capture; its effect is discarded by restarting below
+                    warm_key = (self.device.index, self.n)
+                    if warm_key not in _WARM:
+                        # one eager iteration first sets kernel attributes and loads the
+                        # kernels' modules outside any capture (once per process and
+                        # side); its effect is discarded by restarting below
                         self._iteration(0)
                         self._start()
-                        self._warm = True
+                        _WARM.add(warm_key)
                     self._capture()
                 nat.check(L.pb_graph_launch(self.exec, s), "graph launch")
             _sync.wait("solver iterations")
@@ -571,12 +573,17 @@ def _cached_bytes() -> int:
 
 
 def engine_for(n: int, point_weight: float, device: torch.device, slot: int | None = None) -> RefinedEngine:
-    """A cached engine for (device, n, point_weight, slot); least recently used
+    """An engine for (device, n, point_weight, slot), cached below LEAN_MIN_N; least recently used
     engines are dropped beyond ENGINE_CACHE_SIZE entries or ENGINE_CACHE_FRACTION
     of device memory (and all of them when an allocation runs out of memory).
     The caller owns the returned engine until its solve returns: one slot per
     concurrent thread."""
     slot = current_slot() if slot is None else slot
+    if n >= LEAN_MIN_N:
+        # a lean engine keeps only its hierarchy between solves (tens of GB at
+        # these sides); it is not cached: its memory returns to the allocator's
+        # cache after the solve and a new one costs an allocation and a fill
+        return RefinedEngine(n, point_weight, device)
     key = (device.index, n, float(point_weight), slot)
     with _ENGINE_LOCK:
         eng = _ENGINES.pop(key, None)
