@@ -72,7 +72,7 @@ def parse_args():
                          "deep: depth 10")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the autotuner (built-in launch shapes); by default it runs before the warm-up")
-    ap.add_argument("--lanes", type=int, default=2)
+    ap.add_argument("--lanes", type=int, default=1)
     ap.add_argument("--duration", type=float, default=10.0, help="serving: seconds of arrivals")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
     return ap.parse_args()
