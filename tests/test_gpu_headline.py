@@ -12,6 +12,8 @@ bit-identical to its serial build).
     REFINED_FIELD_TOL of the oracle's largest |field| (max norm), the iso-value
     within REFINED_ISO_TOL relative, and the mesh's face count within
     REFINED_FACES_TOL (relative) of the oracle's.
+* Depth 10 (1025^3), 4,000,000 samples on 64 spheres: the refined field and
+  mesh against the GPU FP64 solve to 1e-10 on the same grids.
 * Depth 9 (513^3), 2,000,000 samples on a union of 64 spheres (seed 2): FP64
   at 1 V-cycle bit-identical to the oracle; the FP32-refined solve against the
   GPU's FP64 solve (bit-identical to the oracle cycle for cycle) run to 1e-11.
@@ -147,3 +149,37 @@ def test_depth9_refined_against_tight_fp64(spheres9):
     err = float((got.field - want.field).abs().max() / want.field.abs().max())
     assert err <= REFINED_FIELD_TOL, err
     assert got.iso_value == pytest.approx(want.iso_value, rel=REFINED_ISO_TOL)
+
+
+def test_depth10_refined_against_tight_fp64():
+    """Depth 10 (1025^3, the deep configuration's grid) with 4,000,000 samples on
+    64 spheres: the FP32-refined field at rel-res 1e-8 against the FP64 solve to
+    1e-10 on the same grids (the FP64 path is bit-identical to the oracle cycle
+    for cycle at depths 8 and 9 above), and the refined reconstruction's mesh
+    counts against the FP64 one's."""
+    import mojo_poissonrecon_b200 as mpr
+    from mojo_poissonrecon_b200 import core, solver32, workloads
+
+    pts, nrm = workloads.sphere_union(4_000_000, spheres=64, seed=2)
+    dp, dn = torch.from_numpy(pts).cuda(), torch.from_numpy(nrm).cuda()
+    del pts, nrm
+    ctx = core._Context()
+    up, un, _, _ = core._prepare(ctx, dp, dn, 1.1)
+    kw = dict(depth=10, point_weight=4.0, confidence=False, cycles=4, samples_per_node=1.5, max_cycles=400,
+              octree=False)
+    f32, _, _, st32, _ = core._solve_device(ctx, up, un, precision="fp32_refined", tol=1e-8, **kw)
+    assert st32.relative_residual <= 1e-8
+    solver32.clear_engines()
+    f64, _, _, st64, _ = core._solve_device(ctx, up, un, precision="fp64", tol=1e-10, **kw)
+    assert st64.relative_residual <= 1e-10
+    err = float((f32 - f64).abs().max() / f64.abs().max())
+    assert err <= REFINED_FIELD_TOL, err
+    del f32, f64, up, un
+    torch.cuda.empty_cache()
+    a = mpr.reconstruct(dp, dn, depth=10, precision="fp32_refined", tol=1e-8, device_out=True)
+    na, fa = a.vertices.shape[0], a.faces.shape[0]
+    del a
+    b = mpr.reconstruct(dp, dn, depth=10, precision="fp64", tol=1e-10, max_cycles=400, device_out=True)
+    assert fa > 1_000_000
+    assert abs(fa - b.faces.shape[0]) <= REFINED_FACES_TOL * b.faces.shape[0]
+    assert abs(na - b.vertices.shape[0]) <= REFINED_FACES_TOL * b.vertices.shape[0]
