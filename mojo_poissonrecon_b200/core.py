@@ -275,6 +275,7 @@ def _solve_device(ctx: _Context, points: torch.Tensor, normals: torch.Tensor, *,
                   octree: bool, refine_method: str = "fcg"):
     tree = _octree_device(ctx, points, depth) if octree else None
     grids, accepted = _splat_assemble(ctx, points, normals, depth, point_weight, confidence, samples_per_node)
+    ctx.ws = nat.Workspace(ctx.device)  # the splat's scratch (GBs at 20M points) is not needed past here
     count = points.shape[0]
     if precision == "fp64":
         field, stats = solver.solve_fp64(grids["rhs"], grids["screen"], point_weight, ctx.ws, cycles=cycles,

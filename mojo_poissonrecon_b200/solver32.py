@@ -309,7 +309,7 @@ def apply_tuning(lib, n: int, device: torch.device) -> None:
     _TUNED.add(key)
 
 
-LEAN_MIN_N = 513  # engines of this side or larger run lean (RefinedEngine) and are not cached
+LEAN_MIN_N = 513  # engines of this side or larger run lean (RefinedEngine)
 _WARM: set = set()  # (device, side) whose kernels have run once outside a capture
 
 
@@ -573,17 +573,12 @@ def _cached_bytes() -> int:
 
 
 def engine_for(n: int, point_weight: float, device: torch.device, slot: int | None = None) -> RefinedEngine:
-    """An engine for (device, n, point_weight, slot), cached below LEAN_MIN_N; least recently used
+    """A cached engine for (device, n, point_weight, slot); least recently used
     engines are dropped beyond ENGINE_CACHE_SIZE entries or ENGINE_CACHE_FRACTION
     of device memory (and all of them when an allocation runs out of memory).
     The caller owns the returned engine until its solve returns: one slot per
     concurrent thread."""
     slot = current_slot() if slot is None else slot
-    if n >= LEAN_MIN_N:
-        # a lean engine keeps only its hierarchy between solves (tens of GB at
-        # these sides); it is not cached: its memory returns to the allocator's
-        # cache after the solve and a new one costs an allocation and a fill
-        return RefinedEngine(n, point_weight, device)
     key = (device.index, n, float(point_weight), slot)
     with _ENGINE_LOCK:
         eng = _ENGINES.pop(key, None)
