@@ -344,6 +344,22 @@ int pb_coarse27_image_f32(int64_t count, const int64_t *sizes, const float *cons
 int pb_coarse27_cycle_f32(int64_t count, const int64_t *sizes, const float *image, const float *rhs, float *e,
                           int64_t pre, int64_t post, int64_t inner, void *stream);
 
+/* A whole preconditioner hierarchy's set-up from one call: the launches of
+ * pb_level_setup_f32 (level 0 from the FP64 screen; for a 27-point level 0 also
+ * pb_level27_from7_f32 and pb_level27_finish_f32), then per level l >= 1
+ * pb_galerkin_f32 from level l-1, pb_level27_finish_f32, and pb_pack27_f32 of
+ * level l-1 when it is packed; pb_coarse_inverse_f32 of the last level and
+ * pb_coarse27_image_f32 of the levels from first_coarse on — in that order, so
+ * the results are those of the separate calls.  arrays: PB_LEVEL_ARRAYS device
+ * pointers per level, in the order D, invD, weights, coef, h0, h1, inv0, inv1
+ * (D on level 0 only; coef NULL for a 7-point level 0; the packed four NULL on
+ * levels that are not packed).  No counterpart in the reference, whose coarse
+ * levels are rediscretised per cycle (core.py:267-269). */
+enum { PB_LEVEL_ARRAYS = 8 };
+int pb_hierarchy_setup_f32(int64_t levels, const int64_t *sides, const void *const *arrays, int64_t first_coarse,
+                           const double *screen, double point_weight, void *galerkin_ws, size_t galerkin_bytes,
+                           float *inverse, float *image, size_t image_bytes, void *stream);
+
 /* ---- batches of clouds: one grouped launch per solver step ------------------
  * No counterpart in the reference, which solves one cloud at a time and level
  * by level (core.py:141-193, driven per cycle at :270-287).  A grouped launch

@@ -98,6 +98,7 @@ _SIGNATURES = {
     "pb_batch_describe": ([C, I, P, P, P, P, I, P, S, P], C),
     "pb_batch_launch": ([C, P, I, I, P, I, P], C),
     "pb_batch_loop_condition": ([ctypes.c_ulonglong, P, P, P, I, I, P, P], C),
+    "pb_hierarchy_setup_f32": ([I, P, P, I, P, F, P, S, P, P, S, P], C),
     "pb_tune_set": ([I, I, I], C),
     "pb_tune_get": ([I, I], I),
     "pb_tune_clear": ([], C),

@@ -1277,3 +1277,60 @@ int launch_coarse27(const GridDesc* descs, int count, int64_t blocks, int first_
 
 }  // namespace batch
 }  // namespace pb
+
+// ---- a whole hierarchy's set-up in one call ---------------------------------------
+// The sequence Hierarchy32.setup issues level by level, from one host call:
+// level 0 from the screen, each coarser level's Galerkin operator from the one
+// above, finish, and the packing of every packed level right after the product
+// that reads it for the last time; then the 3^3 inverse and the coarse image.
+// Same launches in the same order as the separate entry points.
+extern "C" int pb_hierarchy_setup_f32(int64_t levels, const int64_t* sides, const void* const* arrays,
+                                      int64_t first_coarse, const double* screen, double point_weight,
+                                      void* galerkin_ws, size_t galerkin_bytes, float* inverse, float* image,
+                                      size_t image_bytes, void* stream) {
+    constexpr int A = PB_LEVEL_ARRAYS;
+    if (levels < 2 || levels > 13 || !sides || !arrays || !screen || !inverse || !image || first_coarse < 1 ||
+        first_coarse >= levels)
+        return fail(PB_ERR_INVALID, "hierarchy setup: bad args");
+    for (int64_t l = 0; l < levels; ++l) {
+        if (!level_side_ok(sides[l]) || (l && sides[l] != (sides[l - 1] + 1) / 2))
+            return fail(PB_ERR_INVALID, "hierarchy setup: level sides must halve from a 2^k + 1 side down to 3");
+        if (!arrays[l * A + 1] || !arrays[l * A + 2] || (l && !arrays[l * A + 3]))
+            return fail(PB_ERR_INVALID, "hierarchy setup: level %lld misses invD, weights or coef", (long long)l);
+    }
+    if (sides[levels - 1] != 3) return fail(PB_ERR_INVALID, "hierarchy setup: the last level must have side 3");
+    auto D = [&](int64_t l) { return (float*)arrays[l * A + 0]; };
+    auto invD = [&](int64_t l) { return (float*)arrays[l * A + 1]; };
+    auto W = [&](int64_t l) { return (float*)arrays[l * A + 2]; };
+    auto coef = [&](int64_t l) { return (float*)arrays[l * A + 3]; };
+    auto packed = [&](int64_t l) { return arrays[l * A + 4] != nullptr; };
+    const bool seven = coef(0) == nullptr;
+    if (!D(0)) return fail(PB_ERR_INVALID, "hierarchy setup: level 0 needs D");
+    PB_TRY(pb_level_setup_f32(screen, sides[0], point_weight, D(0), invD(0), W(0), stream));
+    if (!seven) {
+        PB_TRY(pb_level27_from7_f32(D(0), sides[0], coef(0), stream));
+        PB_TRY(pb_level27_finish_f32(coef(0), sides[0], invD(0), W(0), stream));
+    }
+    for (int64_t l = 1; l < levels; ++l) {
+        const bool fine7 = l == 1 && seven;
+        PB_TRY(pb_galerkin_f32(fine7 ? D(0) : coef(l - 1), sides[l - 1], fine7 ? 1 : 0, W(l - 1), coef(l),
+                               galerkin_ws, galerkin_bytes, stream));
+        PB_TRY(pb_level27_finish_f32(coef(l), sides[l], invD(l), W(l), stream));
+        if (packed(l - 1))
+            PB_TRY(pb_pack27_f32(coef(l - 1), sides[l - 1], (void*)arrays[(l - 1) * A + 4],
+                                 (void*)arrays[(l - 1) * A + 5], (float*)arrays[(l - 1) * A + 6],
+                                 (float*)arrays[(l - 1) * A + 7], stream));
+    }
+    PB_TRY(pb_coarse_inverse_f32(coef(levels - 1), 3, inverse, stream));
+    const int64_t tail = levels - first_coarse;
+    const float* tc[kC27MaxLevels];
+    const float* ti[kC27MaxLevels];
+    const float* tw[kC27MaxLevels];
+    if (tail < 1 || tail > kC27MaxLevels) return fail(PB_ERR_INVALID, "hierarchy setup: 1 to 3 levels of side <= 9");
+    for (int64_t k = 0; k < tail; ++k) {
+        tc[k] = coef(first_coarse + k);
+        ti[k] = invD(first_coarse + k);
+        tw[k] = W(first_coarse + k);
+    }
+    return pb_coarse27_image_f32(tail, sides + first_coarse, tc, ti, tw, inverse, image, image_bytes, stream);
+}

@@ -194,37 +194,28 @@ class Hierarchy32:
 
     def setup(self, screen: torch.Tensor, point_weight: float) -> None:
         """Level 0 from the FP64 screen (D = (deg + pw*screen) h^-2, core.py:150-163),
-        then each coarser level's Galerkin operator from the one above it."""
-        L, s = self.lib, self.stream
+        then each coarser level's Galerkin operator from the one above it, the
+        packed forms, the 3^3 inverse and the coarse image: one library call
+        (pb_hierarchy_setup_f32)."""
         self.pw = float(point_weight)
-        top = self.levels[0]
-        nat.check(L.pb_level_setup_f32(screen.data_ptr(), top.n, self.pw, top.D.data_ptr(), top.invD.data_ptr(),
-                                       top.weights.data_ptr(), s), "level setup")
-        if not top.seven:
-            if top.coef is None:
-                top.coef = torch.zeros(14, top.count, dtype=torch.float32, device=self.device)
-            nat.check(L.pb_level27_from7_f32(top.D.data_ptr(), top.n, top.coef.data_ptr(), s), "level27 from 7")
-            nat.check(L.pb_level27_finish_f32(top.coef.data_ptr(), top.n, top.invD.data_ptr(),
-                                              top.weights.data_ptr(), s), "level27 finish")
-        def planes(lv):  # zero-filled: the kernels write interior nodes only
-            if lv.coef is None:
+        for i, lv in enumerate(self.levels):  # zero-filled: the kernels write interior nodes only
+            if lv.coef is None and not lv.seven:
                 lv.coef = torch.zeros(14, lv.count, dtype=torch.float32, device=self.device)
-            return lv.coef
-
-        for fine, lv in zip(self.levels[:-1], self.levels[1:]):
-            src, seven = (fine.D, 1) if fine.seven else (fine.coef, 0)
-            nat.check(L.pb_galerkin_f32(src.data_ptr(), fine.n, seven, fine.weights.data_ptr(),
-                                        planes(lv).data_ptr(), self.galerkin_ws.data_ptr(),
-                                        self.galerkin_ws.numel() * 4, s), "galerkin")
-            nat.check(L.pb_level27_finish_f32(lv.coef.data_ptr(), lv.n, lv.invD.data_ptr(), lv.weights.data_ptr(), s),
-                      "level27 finish")
-            if fine.packed is not None:  # its planes are read for the last time by the product above
-                nat.check(L.pb_pack27_f32(fine.coef.data_ptr(), fine.n, *fine.packed_ptrs(), s), "pack27")
-                if self.transient_coef:
-                    fine.coef = None
-        nat.check(L.pb_coarse_inverse_f32(self.levels[-1].coef.data_ptr(), 3, self.inverse.data_ptr(), s),
-                  "coarse inverse")
-        nat.check(L.pb_coarse27_image_f32(*self._image_args, s), "coarse image")
+        K, A = len(self.levels), 8
+        arrays = (ctypes.c_void_p * (K * A))()
+        for i, lv in enumerate(self.levels):
+            row = [lv.D, lv.invD, lv.weights, lv.coef] + list(lv.packed or (None,) * 4)
+            for k, t in enumerate(row):
+                arrays[i * A + k] = None if t is None else t.data_ptr()
+        sides = (ctypes.c_int64 * K)(*[lv.n for lv in self.levels])
+        nat.check(self.lib.pb_hierarchy_setup_f32(K, sides, arrays, self.first_coarse, screen.data_ptr(), self.pw,
+                                                  self.galerkin_ws.data_ptr(), self.galerkin_ws.numel() * 4,
+                                                  self.inverse.data_ptr(), self.image.data_ptr(),
+                                                  self.image.numel() * 4, self.stream), "hierarchy setup")
+        if self.transient_coef:
+            for lv in self.levels:
+                if lv.packed is not None:
+                    lv.coef = None  # freed once this stream's set-up has run (stream-ordered allocator)
 
     def _sweep(self, lv: Level32, src, dst, mode: int, coarse=None) -> None:
         """One red-black sweep dst <- S(src); mode 1 starts from zero, mode 2
