@@ -396,14 +396,18 @@ def kernel_rooflines(eng, n: int, L) -> list:
 
     var = {name: int(L.pb_tune_get(code, n)) for name, code in
            (("sweep", 7), ("restrict", 8), ("direction", 5), ("update", 6))}  # PB_TUNE_*_VARIANT
-    rr_name = "residual_restrict32_paired_kernel" if var["restrict"] == 1 else "residual_restrict32_kernel"
+    rr_name = {1: "residual_restrict32_paired_kernel", 2: "tma::residual_restrict_tma_kernel"}.get(
+        var["restrict"], "residual_restrict32_kernel")
     dir_name = f"fcg::direction_sums_kernel<{(4, 6, 8)[var['direction']]}>"
     upd_name = ("fcg::update_residual_prefetch_kernel" if var["update"] == 3
                 else f"fcg::update_residual_kernel<{(5, 6, 8)[var['update']]}>")
     rr_at = len(out)
-    timed(f"{rr_name} (level 0)", lambda s: L.pb_residual_restrict_f32(
-        l0.ea.data_ptr(), l0.rhs.data_ptr(), l0.D.data_ptr(), l0.weights.data_ptr(), l1.rhs.data_ptr(), n, s),
-        16 * N + 4 * N1)
+    rr_args = (l0.ea.data_ptr(), l0.rhs.data_ptr(), l0.D.data_ptr(), l0.weights.data_ptr(), l1.rhs.data_ptr(), n)
+    if var["restrict"] == 2:
+        timed(f"{rr_name} (level 0)", lambda s: L.pb_residual_restrict_tma_f32(*rr_args, h.status.data_ptr(), s),
+              16 * N + 4 * N1)
+    else:
+        timed(f"{rr_name} (level 0)", lambda s: L.pb_residual_restrict_f32(*rr_args, s), 16 * N + 4 * N1)
     timed("prolong_add32_kernel (level 0)", lambda s: L.pb_prolong_fac_f32(
         l1.ea.data_ptr(), l0.eb.data_ptr(), l0.weights.data_ptr(), n, s), 12 * N + 4 * N1)
     timed("relax27p_kernel x2 (one sweep, level 1, packed FP16)", lambda s: L.pb_relax27p_f32(
@@ -411,11 +415,12 @@ def kernel_rooflines(eng, n: int, L) -> list:
     timed(dir_name, lambda s: L.pb_fcg_direction_f64(
         l0.ea.data_ptr(), p0, p1, l0.rhs.data_ptr(), eng.screen.data_ptr(), n, eng.pw, eng.scal.data_ptr(),
         eng.flags.data_ptr(), eng.ws_ptr, eng.ws_size, s), 20 * N)
-    if n == 257:
+    if n == 257 and var["restrict"] != 2:  # the committed capture is of the per-thread-load kernels
         out[rr_at]["traffic"] = read_profile_traffic(RESTRICT_PROFILE)
     timed(upd_name, lambda s: L.pb_fcg_update_f64(
         l0.ea.data_ptr(), p0, p1, x0, x1, eng.b.data_ptr(), eng.screen.data_ptr(), l0.rhs.data_ptr(), n, eng.pw,
         eng.scal.data_ptr(), eng.flags.data_ptr(), eng.ws_ptr, eng.ws_size, s), 48 * N)
+    h.check_status()
     return out
 
 
@@ -682,9 +687,11 @@ def run_serving(args) -> dict:
 
 def run_deep(args) -> dict:
     """20,000,000 points on a union of 64 spheres, depth 10 (1025^3): each
-    precision's reconstruction timed with CUDA events and its peak device
-    memory, then the refined field (rel-res 1e-8) against the FP64 field solved
-    to 1e-10 on the same grids."""
+    precision's reconstruction timed with CUDA events (the refined one three
+    times, median; `device_allocations` counts the new device segments the
+    caching allocator took during each call) and its peak device memory, then
+    the refined field (rel-res 1e-8) against the FP64 field solved to 1e-10 on
+    the same grids."""
     import torch
 
     import mojo_poissonrecon_b200 as mpr
@@ -701,12 +708,19 @@ def run_deep(args) -> dict:
         torch.cuda.synchronize()
         base = torch.cuda.memory_allocated()
         torch.cuda.reset_peak_memory_stats()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        mesh = mpr.reconstruct(dp, dn, depth=10, precision=prec, tol=TOL, device_out=True)
-        e1.record()
-        torch.cuda.synchronize()
-        out[prec] = {"ms": round(e0.elapsed_time(e1), 1), "vertices": int(mesh.vertices.shape[0]),
+        times, segments = [], []
+        for _ in range(3 if prec == "fp32_refined" else 1):
+            mesh = None
+            seg0 = torch.cuda.memory_stats().get("segment.all.allocated", 0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            mesh = mpr.reconstruct(dp, dn, depth=10, precision=prec, tol=TOL, device_out=True)
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(round(e0.elapsed_time(e1), 1))
+            segments.append(torch.cuda.memory_stats().get("segment.all.allocated", 0) - seg0)
+        out[prec] = {"ms": statistics.median(times), "all_ms": times, "device_allocations": segments,
+                     "vertices": int(mesh.vertices.shape[0]),
                      "faces": int(mesh.faces.shape[0]), "residual_norm": mesh.residual_norm,
                      "peak_memory_gib": round((torch.cuda.max_memory_allocated() - base) / 2**30, 1),
                      "resident_before_gib": round(base / 2**30, 1)}

@@ -297,6 +297,13 @@ int pb_mesh_normals_emit_f64(const double *vertices, int64_t vertex_count, const
  * fine residual. */
 int pb_residual_restrict_f32(const float *e, const float *rhs, const float *D, const float *weights,
                              float *coarse_rhs, int64_t n, void *stream);
+/* The same result, bit for bit, with the fine planes of e, rhs, D and weights
+ * staged in shared memory by TMA (a four-plane ring two planes ahead, one
+ * mbarrier per plane); sides 2^k + 1 >= 33.  The FP32 cycle calls it in place
+ * of pb_residual_restrict_f32 where RESTRICT_VARIANT is 2.  A bounded wait
+ * that gives up sets *status (device int) to 1. */
+int pb_residual_restrict_tma_f32(const float *e, const float *rhs, const float *D, const float *weights,
+                                 float *coarse_rhs, int64_t n, int *status, void *stream);
 /* 14 planes of the Galerkin operator of the level below a level of side
  * fine_n with prolongation weights fine_weights: from level 0 (fine_is_7pt
  * != 0, `fine` = D; no workspace) or from 14 planes, one axis at a time over
@@ -445,7 +452,8 @@ int pb_batch_loop_condition(unsigned long long handle, const double *scal, const
  *   FCG_DIRECTION_VARIANT  register budget of pb_fcg_direction_f64: 0 = 4 resident
  *                          blocks per SM, 1 = 6, 2 = 8
  *   RESTRICT_VARIANT       pb_residual_restrict_f32: 1 = both fine planes of a coarse
- *                          plane in one loop over their items
+ *                          plane in one loop over their items; 2 = the FP32 cycle
+ *                          calls pb_residual_restrict_tma_f32 instead
  *   RELAX27_VARIANT        pb_relax27p_f32 (per level side): 1 = the neighbour planes
  *                          staged in shared memory
  *   RESIDUAL27_VARIANT     pb_residual_restrict27p_f32 (per level side): 1 = the

@@ -80,6 +80,7 @@ _SIGNATURES = {
     "pb_extract_count_f64": ([P, I, P, P, P, S, P], C),
     "pb_extract_emit_f64": ([P, P, I, P, P, P, P, P, S, P], C),
     "pb_residual_restrict_f32": ([P, P, P, P, P, I, P], C),
+    "pb_residual_restrict_tma_f32": ([P, P, P, P, P, I, P, P], C),
     "pb_galerkin_workspace_size": ([I, C], S),
     "pb_galerkin_f32": ([P, I, C, P, P, P, S, P], C),
     "pb_level27_from7_f32": ([P, I, P, P], C),

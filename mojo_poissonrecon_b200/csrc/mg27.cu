@@ -1289,7 +1289,7 @@ extern "C" int pb_hierarchy_setup_f32(int64_t levels, const int64_t* sides, cons
                                       void* galerkin_ws, size_t galerkin_bytes, float* inverse, float* image,
                                       size_t image_bytes, void* stream) {
     constexpr int A = PB_LEVEL_ARRAYS;
-    if (levels < 2 || levels > 13 || !sides || !arrays || !screen || !inverse || !image || first_coarse < 1 ||
+    if (levels < 2 || levels > 13 || !sides || !arrays || !screen || !inverse || !image || first_coarse < 0 ||
         first_coarse >= levels)
         return fail(PB_ERR_INVALID, "hierarchy setup: bad args");
     for (int64_t l = 0; l < levels; ++l) {
@@ -1306,6 +1306,8 @@ extern "C" int pb_hierarchy_setup_f32(int64_t levels, const int64_t* sides, cons
     auto packed = [&](int64_t l) { return arrays[l * A + 4] != nullptr; };
     const bool seven = coef(0) == nullptr;
     if (!D(0)) return fail(PB_ERR_INVALID, "hierarchy setup: level 0 needs D");
+    if (seven && first_coarse == 0)
+        return fail(PB_ERR_INVALID, "hierarchy setup: a 7-point level 0 cannot be part of the coarse cycle");
     PB_TRY(pb_level_setup_f32(screen, sides[0], point_weight, D(0), invD(0), W(0), stream));
     if (!seven) {
         PB_TRY(pb_level27_from7_f32(D(0), sides[0], coef(0), stream));

@@ -312,6 +312,162 @@ static int make_map(CUtensorMap* map, const float* base, int n, int P, int rows)
     return PB_OK;
 }
 
+// ---- level-0 residual with the scaled restriction, planes staged by TMA ----------
+// The arithmetic of residual_restrict32_kernel (stencil32.cu) on the same 64 x 4
+// coarse tile and z march, with its inputs brought in by cp.async.bulk.tensor
+// instead of per-thread float4 loads: per fine plane one box of e (144 x 11:
+// the 136 x 9 residual region and a one-node halo, x origin aligned to 16 B)
+// and one box each of rhs, D and s (136 x 9), into a ring of four planes, two
+// planes ahead of the plane being computed, each slot guarded by an mbarrier.
+// Every thread reads its float4 groups from shared memory; the residual ring
+// keeps planes 2zc-1 .. 2zc+1 for the restriction.  Per node and per coarse
+// node the same expressions in the same order: bit-identical results.  Waits
+// are bounded as in the sweep (status word, drain, stop).
+constexpr int kRCX = 64, kRCY = 4;
+constexpr int kRFX = 2 * kRCX + 8, kRFY = 2 * kRCY + 1;  // 136 x 9 residuals: fine x from 2 xc0 - 4, y from 2 yc0 - 1
+constexpr int kREX = kRFX + 8, kREY = kRFY + 2;          // 144 x 11 of e: fine x from 2 xc0 - 8, y from 2 yc0 - 2
+constexpr int kRSlots = 4, kRRes = 3, kRThreads = 256;
+constexpr int kREStride = (kREX * kREY + 31) / 32 * 32;  // 128-byte aligned boxes
+constexpr int kRFStride = (kRFX * kRFY + 31) / 32 * 32;
+constexpr uint32_t kREBytes = kREX * kREY * 4, kRFBytes = kRFX * kRFY * 4;
+
+struct RSmem {
+    float e[kRSlots][kREStride];
+    float rhs[kRSlots][kRFStride];
+    float d[kRSlots][kRFStride];
+    float w[kRSlots][kRFStride];
+    float res[kRRes][kRFY][kRFX];
+    unsigned long long bar[kRSlots];
+};
+
+__global__ void __launch_bounds__(kRThreads, 2)
+    residual_restrict_tma_kernel(const __grid_constant__ CUtensorMap map_e, const __grid_constant__ CUtensorMap map_b,
+                                 const __grid_constant__ CUtensorMap map_d, const __grid_constant__ CUtensorMap map_w,
+                                 int fn, int cn, int cz, float h2, float* __restrict__ coarse, int cP,
+                                 int* __restrict__ status) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const uint32_t raw = saddr(smem_raw);
+    RSmem& S = *reinterpret_cast<RSmem*>(smem_raw + (((raw + 127u) & ~127u) - raw));
+    const int xc0 = blockIdx.x * kRCX, yc0 = blockIdx.y * kRCY;
+    const int zc0 = blockIdx.z * cz, zc1 = min(cn, zc0 + cz);
+    const int fx0 = 2 * xc0 - 4, fy0 = 2 * yc0 - 1;
+    const int pe0 = 2 * zc0 - 2, pe1 = 2 * zc1;  // e planes read; rhs, D, s for pe0 + 1 .. pe1 - 1
+    const int tid = threadIdx.x;
+    auto slot_of = [&](int p) { return (p - pe0) % kRSlots; };
+    auto parity_of = [&](int p) { return (uint32_t)(((p - pe0) / kRSlots) & 1); };
+    auto issue = [&](int p) {
+        const int sl = slot_of(p);
+        const bool inner = p > pe0 && p < pe1;
+        bar_expect(&S.bar[sl], kREBytes + (inner ? 3 * kRFBytes : 0));
+        load_box(S.e[sl], &map_e, 2 * xc0 - 4, 2 * yc0 - 1, p + 1, &S.bar[sl]);
+        if (inner) {
+            load_box(S.rhs[sl], &map_b, 2 * xc0, 2 * yc0, p + 1, &S.bar[sl]);
+            load_box(S.d[sl], &map_d, 2 * xc0, 2 * yc0, p + 1, &S.bar[sl]);
+            load_box(S.w[sl], &map_w, 2 * xc0, 2 * yc0, p + 1, &S.bar[sl]);
+        }
+    };
+    if (tid == 0) {
+        for (int k = 0; k < kRSlots; ++k) bar_init(&S.bar[k]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    int issued = pe0;
+    if (tid == 0)
+        for (; issued <= pe1 && issued < pe0 + kRSlots; ++issued) issue(issued);
+    bool ok = bar_wait(&S.bar[slot_of(pe0)], parity_of(pe0));
+    ok = bar_wait(&S.bar[slot_of(pe0 + 1)], parity_of(pe0 + 1)) && ok;
+    ok = __syncthreads_and(ok);
+    for (int f = pe0 + 1; f < pe1 && ok; ++f) {
+        ok = __syncthreads_and(bar_wait(&S.bar[slot_of(f + 1)], parity_of(f + 1)));
+        if (!ok) break;
+        {  // s-weighted residual of fine plane f (residual_restrict32_body's expressions)
+            const float* ec = S.e[slot_of(f)];
+            const float* em = S.e[slot_of(f - 1)];
+            const float* ep = S.e[slot_of(f + 1)];
+            const float* bb = S.rhs[slot_of(f)];
+            const float* dd = S.d[slot_of(f)];
+            const float* ww = S.w[slot_of(f)];
+            float(*dst)[kRFX] = S.res[(f + kRRes) % kRRes];
+            constexpr int kGroups = kRFX / 4;
+            for (int i = tid; i < kRFY * kGroups; i += kRThreads) {
+                const int ly = i / kGroups, g = i - ly * kGroups;
+                const int x = fx0 + 4 * g, y = fy0 + ly;
+                float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (f >= 0 && f < fn && y >= 0 && y < fn && x >= 0 && x < fn) {
+                    const int q = (ly + 1) * kREX + 4 * g + 4, k = ly * kRFX + 4 * g;
+                    const float4 c = *reinterpret_cast<const float4*>(ec + q);
+                    const float4 ym = *reinterpret_cast<const float4*>(ec + q - kREX);
+                    const float4 yp = *reinterpret_cast<const float4*>(ec + q + kREX);
+                    const float4 zm = *reinterpret_cast<const float4*>(em + q);
+                    const float4 zp = *reinterpret_cast<const float4*>(ep + q);
+                    const float4 b = *reinterpret_cast<const float4*>(bb + k);
+                    const float4 d = *reinterpret_cast<const float4*>(dd + k);
+                    const float4 sw = *reinterpret_cast<const float4*>(ww + k);
+                    const float l = ec[q - 1], rr = ec[q + 4];
+                    const float s0 = l + c.y + ym.x + yp.x + zm.x + zp.x;
+                    const float s1 = c.x + c.z + ym.y + yp.y + zm.y + zp.y;
+                    const float s2 = c.y + c.w + ym.z + yp.z + zm.z + zp.z;
+                    const float s3 = c.z + rr + ym.w + yp.w + zm.w + zp.w;
+                    r.x = sw.x * (b.x - (d.x * c.x - s0 * h2));
+                    r.y = x + 1 < fn ? sw.y * (b.y - (d.y * c.y - s1 * h2)) : 0.f;
+                    r.z = x + 2 < fn ? sw.z * (b.z - (d.z * c.z - s2 * h2)) : 0.f;
+                    r.w = x + 3 < fn ? sw.w * (b.w - (d.w * c.w - s3 * h2)) : 0.f;
+                }
+                *reinterpret_cast<float4*>(&dst[ly][4 * g]) = r;
+            }
+        }
+        __syncthreads();  // plane f's residual complete; e of plane f - 1 read for the last time
+        if (f > pe0 + 1 && (f & 1)) {  // f = 2 zc + 1 with zc >= zc0: restrict coarse plane zc
+            const int zc = (f - 1) / 2;
+            const int cy = tid / kRCX, cx = tid - cy * kRCX;
+            const int xc = xc0 + cx, yc = yc0 + cy;
+            if (xc < cn && yc < cn) {
+                float sum = 0.0f;
+#pragma unroll
+                for (int oz = -1; oz <= 1; ++oz) {
+                    const int zz = 2 * zc + oz;
+#pragma unroll
+                    for (int oy = -1; oy <= 1; ++oy) {
+                        const float* row = S.res[(zz + kRRes) % kRRes][2 * cy + 1 + oy];
+#pragma unroll
+                        for (int ox = -1; ox <= 1; ++ox)
+                            sum += row[2 * cx + 4 + ox] * (float)((ox ? 1 : 2) * (oy ? 1 : 2) * (oz ? 1 : 2));
+                    }
+                }
+                coarse[((int64_t)(zc + 1) * (cn + 2) + (yc + 1)) * cP + (xc + 4)] = sum * (1.0f / 64.0f);
+            }
+            __syncthreads();  // before plane f + 1 overwrites the residual of plane 2 zc - 1
+        }
+        if (tid == 0 && issued <= pe1) {  // into the slot of plane f - 1, read for the last time above
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(issued++);
+        }
+    }
+    if (!ok) {
+        if (tid == 0) {
+            atomicExch(status, 1);
+            for (int p = max(pe0, issued - kRSlots); p < issued; ++p) (void)bar_wait(&S.bar[slot_of(p)], parity_of(p));
+        }
+        __syncthreads();
+    }
+}
+
+// A 3D map over a padded level with a box of `width` x `rows` x 1 floats.
+static int make_box_map(CUtensorMap* map, const float* base, int n, int P, int width, int rows) {
+    EncodeTiled enc = encoder();
+    if (!enc) return fail(PB_ERR_CUDA, "tma: cuTensorMapEncodeTiled is unavailable");
+    if (reinterpret_cast<uintptr_t>(base) & 15) return fail(PB_ERR_INVALID, "tma: arrays must be 16-byte aligned");
+    const cuuint64_t dims[3] = {(cuuint64_t)P, (cuuint64_t)(n + 2), (cuuint64_t)(n + 2)};
+    const cuuint64_t strides[2] = {(cuuint64_t)P * 4, (cuuint64_t)P * (n + 2) * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)width, (cuuint32_t)rows, 1};
+    const cuuint32_t estride[3] = {1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, estride,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(PB_ERR_CUDA, "tma: cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return PB_OK;
+}
+
 }  // namespace tma
 
 // ---- scaled prolongation add on the padded layout -------------------------------
@@ -561,3 +717,31 @@ int launch_prolong32(const GridDesc* descs, int count, int64_t blocks, const int
 
 }  // namespace batch
 }  // namespace pb
+
+// Level 0: coarse_rhs = P^T (s (rhs - A e)) / 8 with the fine planes staged by
+// TMA (same results as pb_residual_restrict_f32).  *status (device int) is set
+// to 1 if a bounded wait gave up.
+extern "C" int pb_residual_restrict_tma_f32(const float* e, const float* rhs, const float* D, const float* weights,
+                                            float* coarse_rhs, int64_t n, int* status, void* stream) {
+    using namespace pb::tma;
+    if (n < 33 || n > 4097 || ((n - 1) & (n - 2)) || !e || !rhs || !D || !weights || !coarse_rhs || !status)
+        return fail(PB_ERR_INVALID, "residual_restrict_tma: bad args (n must be 2^k + 1 >= 33)");
+    const int fn = (int)n, cn = (fn + 1) / 2;
+    const int P = pitch_for(fn);
+    CUtensorMap me, mb, md, mw;
+    PB_TRY(make_box_map(&me, e, fn, P, kREX, kREY));
+    PB_TRY(make_box_map(&mb, rhs, fn, P, kRFX, kRFY));
+    PB_TRY(make_box_map(&md, D, fn, P, kRFX, kRFY));
+    PB_TRY(make_box_map(&mw, weights, fn, P, kRFX, kRFY));
+    int cz = (int)tuned(PB_TUNE_RESTRICT_PLANES, n, 4);
+    if (cz < 1) cz = 1;
+    const dim3 grid((cn + kRCX - 1) / kRCX, (cn + kRCY - 1) / kRCY, (cn + cz - 1) / cz);
+    const size_t smem = sizeof(RSmem) + 128;
+    PB_CHECK_CUDA(cudaFuncSetAttribute(residual_restrict_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem),
+                  "residual_restrict_tma smem");
+    residual_restrict_tma_kernel<<<grid, kRThreads, smem, (cudaStream_t)stream>>>(
+        me, mb, md, mw, fn, cn, cz, (float)((fn - 1) * (fn - 1)), coarse_rhs, pitch_for(cn), status);
+    PB_CHECK_LAUNCH("residual_restrict_tma_kernel");
+    return PB_OK;
+}

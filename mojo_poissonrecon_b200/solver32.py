@@ -50,6 +50,7 @@ from .solver import SolveStats, level_sizes, norm
 COARSE_N = 9  # levels of this side or smaller: one single-block launch
 TMA_MIN_N = 33  # smallest side the TMA sweep takes (level 0 below it is a 27-point level)
 COARSE_SWEEPS = 1  # pre- and post-smoothing sweeps on every level below level 0
+RESTRICT_VARIANT = 8  # tuning parameter: 2 = level 0's residual-restriction staged by TMA
 
 
 def level0_sweeps(n: int) -> tuple[int, int]:
@@ -242,7 +243,7 @@ class Hierarchy32:
 
     def check_status(self) -> None:
         if int(self.status.item()):
-            raise RuntimeError("FP32 sweep: a bounded wait on a TMA barrier gave up (status word set)")
+            raise RuntimeError("FP32 cycle: a bounded wait on a TMA barrier gave up (status word set)")
 
     def v_cycle(self, level: int = 0, pre: int = 3, post: int = 3) -> torch.Tensor:
         """Correction for levels[level].rhs from a zero start; returns its tensor.
@@ -263,7 +264,11 @@ class Hierarchy32:
             self._sweep(lv, src, dst, 0)
             src, dst = dst, src
         nxt = self.levels[level + 1]
-        if lv.seven:
+        if lv.seven and L.pb_tune_get(RESTRICT_VARIANT, lv.n) == 2:
+            nat.check(L.pb_residual_restrict_tma_f32(src.data_ptr(), lv.rhs.data_ptr(), lv.D.data_ptr(),
+                                                     lv.weights.data_ptr(), nxt.rhs.data_ptr(), lv.n,
+                                                     self.status.data_ptr(), s), "residual_restrict_tma")
+        elif lv.seven:
             nat.check(L.pb_residual_restrict_f32(src.data_ptr(), lv.rhs.data_ptr(), lv.D.data_ptr(),
                                                  lv.weights.data_ptr(), nxt.rhs.data_ptr(), lv.n, s),
                       "residual_restrict32")

@@ -74,7 +74,9 @@ def candidates(param: int, n: int) -> list[int]:
         return [0, 1, 2, 3]
     if param == SWEEP_VARIANT:
         return [0, 1, 2]
-    if param in (RESTRICT_VARIANT, RELAX27_VARIANT, RESIDUAL27_VARIANT):
+    if param == RESTRICT_VARIANT:
+        return [0, 1, 2]
+    if param in (RELAX27_VARIANT, RESIDUAL27_VARIANT):
         return [0, 1]
     raise ValueError(f"unknown tuning parameter {param}")
 
@@ -169,9 +171,14 @@ def autotune(n: int, device=None, repeats: int = 10, params=None, path: str | No
             return lambda: nat.check(lib.pb_sweep_tma_f32(l0.ea.data_ptr(), l0.eb.data_ptr(), l0.rhs.data_ptr(),
                                                           l0.invD.data_ptr(), n, 0, 0, status.data_ptr(), s), "sweep")
         if param in (RESTRICT_PLANES, RESTRICT_VARIANT):
-            return lambda: nat.check(lib.pb_residual_restrict_f32(l0.ea.data_ptr(), l0.rhs.data_ptr(),
-                                                                  l0.D.data_ptr(), l0.weights.data_ptr(),
-                                                                  l1.rhs.data_ptr(), n, s), "restrict")
+            args = (l0.ea.data_ptr(), l0.rhs.data_ptr(), l0.D.data_ptr(), l0.weights.data_ptr(), l1.rhs.data_ptr(), n)
+
+            def restrict():  # as the FP32 cycle chooses (Hierarchy32.v_cycle)
+                if lib.pb_tune_get(RESTRICT_VARIANT, n) == 2:
+                    nat.check(lib.pb_residual_restrict_tma_f32(*args, status.data_ptr(), s), "restrict")
+                else:
+                    nat.check(lib.pb_residual_restrict_f32(*args, s), "restrict")
+            return restrict
         if param == PROLONG_PLANES:
             return lambda: nat.check(lib.pb_prolong_fac_f32(l1.ea.data_ptr(), l0.eb.data_ptr(),
                                                             l0.weights.data_ptr(), n, s), "prolong")

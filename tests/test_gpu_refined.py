@@ -239,3 +239,45 @@ def test_residual_restrict_variants_bit_identical(L, n):
                 assert torch.equal(run(), want), (variant, planes)
     finally:
         L.pb_tune_clear()
+
+
+@pytest.mark.parametrize("n", [33, 65, 129, 257])
+def test_residual_restrict_tma_bit_identical(L, n):
+    """The TMA-staged residual-restriction computes the plain kernel's bits at
+    every coarse-planes-per-block value, and no bounded wait gives up."""
+    from mojo_poissonrecon_b200 import tune
+
+    screen, rhs, x, D, invD, W = setup(L, n, 23 * n)
+    e = to_padded(L, x.astype(np.float32))
+    r32 = to_padded(L, rhs.astype(np.float32))
+    cn = (n + 1) // 2
+    s = torch.cuda.current_stream().cuda_stream
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    def out():
+        return torch.full((geometry(L, cn)[1],), float("nan"), dtype=torch.float32, device="cuda")
+
+    L.pb_tune_clear()
+    try:
+        want = torch.zeros(geometry(L, cn)[1], dtype=torch.float32, device="cuda")
+        assert L.pb_residual_restrict_f32(e.data_ptr(), r32.data_ptr(), D.data_ptr(), W.data_ptr(), want.data_ptr(),
+                                          n, s) == 0
+        want = from_padded(L, want, cn)
+        for planes in (0, 1, 3, 8, cn):
+            L.pb_tune_set(tune.RESTRICT_PLANES, n, planes)
+            got = out()
+            assert L.pb_residual_restrict_tma_f32(e.data_ptr(), r32.data_ptr(), D.data_ptr(), W.data_ptr(),
+                                                  got.data_ptr(), n, status.data_ptr(), s) == 0
+            assert np.array_equal(from_padded(L, got, cn), want), planes
+        assert int(status.item()) == 0
+    finally:
+        L.pb_tune_clear()
+
+
+def test_residual_restrict_tma_rejects_bad_sides(L):
+    t = torch.zeros(64, dtype=torch.float32, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    for n in (17, 31, 34, 4099):
+        assert L.pb_residual_restrict_tma_f32(t.data_ptr(), t.data_ptr(), t.data_ptr(), t.data_ptr(), t.data_ptr(),
+                                              n, status.data_ptr(), s) != 0
