@@ -168,7 +168,9 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
 
         found = tune.autotune((1 << args.depth) + 1, device=dev, write=True)  # cached for later processes
         tuning = {k: {"chosen": v["best"], "default_us": round(v["default_s"] * 1e6, 1),
-                      "tuned_us": round(v["best_s"] * 1e6, 1)} for k, v in found.items()}  # name@side: a level
+                      "tuned_us": round(v["best_s"] * 1e6, 1),
+                      "candidates_us": {c: round(t * 1e6, 1) for c, t in v["timings"].items()}}
+                  for k, v in found.items()}  # name@side: a level
 
     def barrier():
         if dist is not None:
@@ -303,13 +305,18 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
             avg_ms = statistics.mean(sweep_ms)
             algorithmic = 16.0 * n**3  # read e, rhs, 1/D and write e, FP32, per launch
             gbs = algorithmic / (avg_ms / 1e3) / 1e9
+            sweep_variant = int(_native.lib().pb_tune_get(7, n))
+            name = "tma::sweep_kernel" + {3: "<5, 2, split>", 4: "<6, 2, split>", 5: "<4, 3, split>",
+                                          6: "<5, 2, split, one barrier>", 7: "<6, 2, split, one barrier>",
+                                          8: "<4, 3, split, one barrier>"}.get(sweep_variant, "")
             kernel_table.insert(0, {
-                "kernel": "tma::sweep_kernel (fused red-black sweep, level 0; ring/occupancy variant "
-                          f"{int(_native.lib().pb_tune_get(7, n))})", "us": round(avg_ms * 1e3, 1),
+                "kernel": f"{name} (fused red-black sweep, level 0; variant {sweep_variant})",
+                "us": round(avg_ms * 1e3, 1),
                 "algorithmic_bytes": int(algorithmic), "achieved_gbs": round(gbs, 1),
                 "frac_of_measured_hbm": round(gbs / hbm_peak()[0], 3),
-                "traffic": read_profile_traffic(SWEEP_PROFILE),
                 "timing": "CUDA events around each finest-level sweep of 5 eager V-cycles"})
+            if sweep_variant in (0, 1, 2):  # the committed capture is of sweep_kernel
+                kernel_table[0]["traffic"] = read_profile_traffic(SWEEP_PROFILE)
         # the dominant kernel of the launch list (profiles/launches_refined_d8.md)
         top = next(k for k in kernel_table if k["kernel"].startswith("fcg::update_residual"))
         peak, peak_src = hbm_peak()
@@ -399,8 +406,8 @@ def kernel_rooflines(eng, n: int, L) -> list:
     rr_name = {1: "residual_restrict32_paired_kernel", 2: "tma::residual_restrict_tma_kernel"}.get(
         var["restrict"], "residual_restrict32_kernel")
     dir_name = f"fcg::direction_sums_kernel<{(4, 6, 8)[var['direction']]}>"
-    upd_name = ("fcg::update_residual_prefetch_kernel" if var["update"] == 3
-                else f"fcg::update_residual_kernel<{(5, 6, 8)[var['update']]}>")
+    upd_name = ({3: "fcg::update_residual_prefetch_kernel<24, 3>", 4: "fcg::update_residual_prefetch_kernel<24, 4>"}
+                .get(var["update"]) or f"fcg::update_residual_kernel<{(5, 6, 8)[var['update']]}>")
     rr_at = len(out)
     rr_args = (l0.ea.data_ptr(), l0.rhs.data_ptr(), l0.D.data_ptr(), l0.weights.data_ptr(), l1.rhs.data_ptr(), n)
     if var["restrict"] == 2:

@@ -332,17 +332,18 @@ int pb_relax27p_f32(const float *e_prev, float *e_next, const float *rhs, const 
 int pb_residual_restrict27p_f32(const float *e, const float *rhs, const void *h0, const void *h1,
                                 const float *inv0, const float *inv1, const float *weights, int64_t n,
                                 float *res, float *coarse_rhs, void *stream);
-/* Inverse (27 x 27, FP32 row-major) of the 27-point level of side 3. */
-int pb_coarse_inverse_f32(const float *coef, int64_t n, float *inverse, void *stream);
+/* Inverse (27 x 27, FP64 row-major, by FP64 Gauss-Jordan) of the 27-point level
+ * of side 3; the single-block cycle applies it in FP64. */
+int pb_coarse_inverse_f64(const float *coef, int64_t n, double *inverse, void *stream);
 /* Levels of side <= 9 (sizes: count levels halving down to 3, finest first)
  * run in one block from a compact image written at set-up: per level but the
  * last, the 27 couplings of each node, 1/diagonal and prolongation weights
  * (host arrays of device pointers to each level's 14 planes, invD and
- * weights), then the 3^3 inverse.  image: 16-byte aligned, of
+ * weights), then the 3^3 inverse (FP64).  image: 16-byte aligned, of
  * pb_coarse27_image_size bytes (0 for invalid sizes). */
 size_t pb_coarse27_image_size(int64_t count, const int64_t *sizes);
 int pb_coarse27_image_f32(int64_t count, const int64_t *sizes, const float *const *coef,
-                          const float *const *invD, const float *const *weights, const float *inverse,
+                          const float *const *invD, const float *const *weights, const double *inverse,
                           float *image, size_t image_bytes, void *stream);
 /* The V-cycle over those levels in shared memory: (pre, post) sweeps on the
  * first, `inner` each way on the others, the last solved with its inverse.
@@ -355,7 +356,7 @@ int pb_coarse27_cycle_f32(int64_t count, const int64_t *sizes, const float *imag
  * pb_level_setup_f32 (level 0 from the FP64 screen; for a 27-point level 0 also
  * pb_level27_from7_f32 and pb_level27_finish_f32), then per level l >= 1
  * pb_galerkin_f32 from level l-1, pb_level27_finish_f32, and pb_pack27_f32 of
- * level l-1 when it is packed; pb_coarse_inverse_f32 of the last level and
+ * level l-1 when it is packed; pb_coarse_inverse_f64 of the last level and
  * pb_coarse27_image_f32 of the levels from first_coarse on — in that order, so
  * the results are those of the separate calls.  arrays: PB_LEVEL_ARRAYS device
  * pointers per level, in the order D, invD, weights, coef, h0, h1, inv0, inv1
@@ -365,7 +366,7 @@ int pb_coarse27_cycle_f32(int64_t count, const int64_t *sizes, const float *imag
 enum { PB_LEVEL_ARRAYS = 8 };
 int pb_hierarchy_setup_f32(int64_t levels, const int64_t *sides, const void *const *arrays, int64_t first_coarse,
                            const double *screen, double point_weight, void *galerkin_ws, size_t galerkin_bytes,
-                           float *inverse, float *image, size_t image_bytes, void *stream);
+                           double *inverse, float *image, size_t image_bytes, void *stream);
 
 /* ---- batches of clouds: one grouped launch per solver step ------------------
  * No counterpart in the reference, which solves one cloud at a time and level
@@ -459,10 +460,14 @@ int pb_batch_loop_condition(unsigned long long handle, const double *scal, const
  *   RESIDUAL27_VARIANT     pb_residual_restrict27p_f32 (per level side): 1 = the
  *                          residual with e's planes staged in shared memory
  *   SWEEP_VARIANT          pb_sweep_tma_f32: 0 = a 5-plane shared ring with 2 resident
- *                          blocks per SM, 1 = 4 planes with 3 blocks, 2 = 3 planes with 3
+ *                          blocks per SM, 1 = 4 planes with 3 blocks, 2 = 3 planes with 3;
+ *                          3, 4, 5 = each warp's box rows of one parity, so a phase
+ *                          computes only the lanes it updates: (5 planes, 2 blocks),
+ *                          (6, 2), (4, 3); 6, 7, 8 = the same with one barrier per
+ *                          plane (a ring slot refilled one step earlier)
  *   FCG_UPDATE_VARIANT     pb_fcg_update_f64: 0 = 5 resident blocks per SM,
- *                          1 = 6 resident blocks per SM, 2 = 8, 3 = the next planes
- *                          prefetched into shared memory by cp.async
+ *                          1 = 6 resident blocks per SM, 2 = 8, 3 = the next two planes
+ *                          prefetched into shared memory by cp.async, 4 = three planes
  * The plane counts also apply to the grouped launches described after they are
  * set.  value 0 clears an entry.  Results do not depend on these values, except
  * the FCG passes' planes per block: they shape the inner products' partial-sum

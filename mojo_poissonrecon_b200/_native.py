@@ -89,7 +89,7 @@ _SIGNATURES = {
     "pb_pack27_f32": ([P, I, P, P, P, P, P], C),
     "pb_relax27p_f32": ([P, P, P, P, P, P, P, I, P], C),
     "pb_residual_restrict27p_f32": ([P, P, P, P, P, P, P, I, P, P, P], C),
-    "pb_coarse_inverse_f32": ([P, I, P, P], C),
+    "pb_coarse_inverse_f64": ([P, I, P, P], C),
     "pb_coarse27_image_size": ([I, P], S),
     "pb_coarse27_image_f32": ([I, P, P, P, P, P, P, S, P], C),
     "pb_coarse27_cycle_f32": ([I, P, P, P, P, I, I, I, P], C),

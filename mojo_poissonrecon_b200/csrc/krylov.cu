@@ -303,11 +303,12 @@ __device__ __forceinline__ void update_residual_body(const float* __restrict__ z
 
 // ---- pass 2 with the next planes prefetched by cp.async -------------------------
 // The same arithmetic as update_residual_body, in the same order.  Each
-// thread copies the values it will read of plane k + 2 (its x, z, p, b and
-// screen, and its halo node's x, z, p) into its own shared-memory slots with
-// cp.async while it works on plane k, so two planes of loads are in flight per
-// thread without holding registers; a thread only reads its own slots, so
-// cp.async.wait_group suffices (the tile of new iterates keeps its barrier).
+// thread copies the values it will read of plane k + RING - 1 (its x, z, p, b
+// and screen, and its halo node's x, z, p) into its own shared-memory slots
+// with cp.async while it works on plane k, so RING - 1 planes of loads are in
+// flight per thread without holding registers; a thread only reads its own
+// slots, so cp.async.wait_group suffices (the tile of new iterates keeps its
+// barrier).  RING = 3 by default, 4 as a tuning variant.
 constexpr int kRing = 3;
 
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
@@ -324,15 +325,19 @@ __device__ __forceinline__ void cp_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-template <int TZC>
+template <int TZC, int RING = kRing>
 __device__ __forceinline__ void update_residual_prefetch_body(
     const float* __restrict__ z, Pad g, float* p0, float* p1, double* x0, double* x1, const double* __restrict__ b,
     const double* __restrict__ screen, double pw, const double* __restrict__ scal, const int* __restrict__ flags,
     float* __restrict__ r32, double* __restrict__ part, int tz, int tile_x, int tile_y, int tile_z, int64_t block) {
+    static_assert(RING >= 3 && RING <= 4, "two or three planes in flight");
     __shared__ double tiles[2][kUY + 2][kUX + 2];
     __shared__ double shared[1][32];
-    __shared__ double rd[kRing][4][kUThreads];  // own x, b, screen; halo x
-    __shared__ float rf[kRing][4][kUThreads];   // own z, p; halo z, p
+    constexpr int kHalo = 2 * (kUX + kUY);     // the threads tid < kHalo own a halo node
+    __shared__ double rd[RING][3][kUThreads];  // own x, b, screen
+    __shared__ double hd[RING][kHalo];         // halo x
+    __shared__ float rf[RING][2][kUThreads];   // own z, p
+    __shared__ float hf[RING][2][kHalo];       // halo z, p
     const int n = g.n;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kUX + tx;
     const int bx = tile_x * kUX, by = tile_y * kUY;
@@ -365,8 +370,8 @@ __device__ __forceinline__ void update_residual_prefetch_body(
     const int64_t c0 = inside ? g.at(x, y, z0) : 0;
     const int64_t hi0 = halo_in ? (int64_t)z0 * nn + (int64_t)hl.hy * n + hl.hx : 0;
     const int64_t hc0 = halo_in ? g.at(hl.hx, hl.hy, z0) : 0;
-    auto issue = [&](int p) {  // plane p's values into slot p % kRing, one commit group
-        const int sl = p % kRing;
+    auto issue = [&](int p) {  // plane p's values into slot p % RING, one commit group
+        const int sl = p % RING;
         const int64_t dz = p - z0;
         if (inside && p < n && p <= z1) {  // own x, z, p of planes z0 .. z1 (z1: the last plane's upper neighbour)
             const int64_t ip = i0 + dz * nn, cq = c0 + dz * g.plane;
@@ -380,18 +385,19 @@ __device__ __forceinline__ void update_residual_prefetch_body(
         }
         if (halo_in && p < z1) {
             const int64_t hp = hi0 + dz * nn, hq = hc0 + dz * g.plane;
-            cp_async8(&rd[sl][3][tid], xc + hp);
-            cp_async4(&rf[sl][2][tid], z + hq);
-            if (!first) cp_async4(&rf[sl][3][tid], pp + hp);
+            cp_async8(&hd[sl][tid], xc + hp);
+            cp_async4(&hf[sl][0][tid], z + hq);
+            if (!first) cp_async4(&hf[sl][1][tid], pp + hp);
         }
         cp_commit();
     };
     issue(z0);
     issue(z0 + 1);
-    cp_wait<1>();
+    if (RING == 4) issue(z0 + 2);
+    cp_wait<RING - 2>();
     double dm = 0.0, xm = 0.0, xb = 0.0;
     if (inside) {
-        const int sl = z0 % kRing;
+        const int sl = z0 % RING;
         dm = dir_of(rf[sl][0][tid], rf[sl][1][tid]);
         xm = rd[sl][0][tid] + alpha * dm;
         xb = z0 > 0 ? xc[i0 - nn] + alpha * dir_at(i0 - nn, c0 - g.plane) : 0.0;
@@ -400,10 +406,10 @@ __device__ __forceinline__ void update_residual_prefetch_body(
     const int degxy = (x > 0) + (x + 1 < n) + (y > 0) + (y + 1 < n);
     double v[1] = {0.0};
     for (int k = z0; k < z1; ++k) {
-        issue(k + 2);  // into the slot of plane k - 1, read for the last time before the previous barrier
-        cp_wait<1>();  // planes up to k + 1 have landed
-        const int sk = k % kRing, sn = (k + 1) % kRing;
-        const double hv = halo_in ? rd[sk][3][tid] + alpha * dir_of(rf[sk][2][tid], rf[sk][3][tid]) : 0.0;
+        issue(k + RING - 1);  // into the slot of plane k - 1, read by this thread alone in the previous step
+        cp_wait<RING - 2>();  // planes up to k + 1 have landed
+        const int sk = k % RING, sn = (k + 1) % RING;
+        const double hv = halo_in ? hd[sk][tid] + alpha * dir_of(hf[sk][0][tid], hf[sk][1][tid]) : 0.0;
         const bool up = k + 1 < n;
         double da = 0.0, xa = 0.0, bi = 0.0, sc = 0.0;
         if (inside) {
@@ -444,13 +450,13 @@ __device__ __forceinline__ void update_residual_prefetch_body(
     if (lin_tid() == 0) part[block] = v[0];
 }
 
-template <int TZC>
+template <int TZC, int RING = kRing>
 __global__ void __launch_bounds__(kUThreads) update_residual_prefetch_kernel(
     const float* __restrict__ z, Pad g, float* p0, float* p1, double* x0, double* x1, const double* __restrict__ b,
     const double* __restrict__ screen, double pw, const double* __restrict__ scal, const int* __restrict__ flags,
     float* __restrict__ r32, double* __restrict__ part, int tz) {
-    update_residual_prefetch_body<TZC>(z, g, p0, p1, x0, x1, b, screen, pw, scal, flags, r32, part, tz, blockIdx.x,
-                                  blockIdx.y, blockIdx.z, block_index());
+    update_residual_prefetch_body<TZC, RING>(z, g, p0, p1, x0, x1, b, screen, pw, scal, flags, r32, part, tz,
+                                             blockIdx.x, blockIdx.y, blockIdx.z, block_index());
 }
 
 // MINB as above (PB_TUNE_FCG_UPDATE_VARIANT; the default 5 matches a 48-register budget).
@@ -733,6 +739,7 @@ extern "C" int pb_fcg_update_f64(const float* z, float* p0, float* p1, double* x
         case 1: upd = fixed ? update_residual_kernel<6, kTZ> : update_residual_kernel<6, 0>; break;
         case 2: upd = fixed ? update_residual_kernel<8, kTZ> : update_residual_kernel<8, 0>; break;
         case 3: upd = fixed ? update_residual_prefetch_kernel<kTZ> : update_residual_prefetch_kernel<0>; break;
+        case 4: upd = fixed ? update_residual_prefetch_kernel<kTZ, 4> : update_residual_prefetch_kernel<0, 4>; break;
         default: break;
     }
     upd<<<grid, dim3(kUX, kUY), 0, s>>>(z, pad_of((int)n), p0, p1, x0, x1, b, screen, point_weight, scal, flags,

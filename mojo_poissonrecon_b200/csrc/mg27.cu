@@ -630,11 +630,12 @@ __global__ void __launch_bounds__(kTRx* kTRy) residual27p_tiled_kernel(
 // ---- exact solve on the 3^3 level -----------------------------------------------
 // The 27 x 27 operator of the coarsest level inverted once per set-up by one
 // warp: FP64 Gauss-Jordan without pivoting (the Galerkin operator is
-// symmetric positive definite), lane i owning row i; stored FP32 row-major.
+// symmetric positive definite), lane i owning row i; stored FP64 row-major and
+// applied in FP64 (the coarsest-level solve stays in double precision).
 constexpr int kInvN = 27;
 
 __global__ void __launch_bounds__(32) coarse_inverse_kernel(const float* __restrict__ c, int64_t cs, Geom g,
-                                                            float* __restrict__ inv) {
+                                                            double* __restrict__ inv) {
     __shared__ double a[kInvN][kInvN + 1];
     const int lane = threadIdx.x;
     if (lane < kInvN) {
@@ -664,7 +665,7 @@ __global__ void __launch_bounds__(32) coarse_inverse_kernel(const float* __restr
         __syncwarp();
     }
     if (lane < kInvN)
-        for (int j = 0; j < kInvN; ++j) inv[lane * kInvN + j] = (float)a[lane][j];
+        for (int j = 0; j < kInvN; ++j) inv[lane * kInvN + j] = a[lane][j];
 }
 
 // ---- levels of side <= 9 in one block, from shared memory -------------------------
@@ -673,7 +674,7 @@ __global__ void __launch_bounds__(32) coarse_inverse_kernel(const float* __restr
 // into a compact image (pb_coarse27_image_f32): per level above the last, the
 // 27 couplings of every node (offsets (dz, dy, dx) in lexicographic order, zero
 // outside the grid), 1/diagonal and the prolongation weights, node-major; then
-// the 3^3 inverse.  Each cycle copies the image into shared memory and keeps e,
+// the 3^3 inverse (FP64).  Each cycle copies the image into shared memory and keeps e,
 // rhs and the residual of every level there in padded cubes ((n+2)^3 floats,
 // zero ghosts), so global memory sees only the first level's rhs and its
 // correction.
@@ -710,8 +711,8 @@ __host__ __device__ inline CoarseLayout coarse_layout(int count, const int* size
         c.fac[l] = off;
         off += round4(N);
     }
-    c.inverse = off;
-    off += round4(kInvN * kInvN);
+    c.inverse = off;  // 16-byte aligned: doubles
+    off += round4(2 * kInvN * kInvN);
     c.image = off;
     for (int l = 0; l < count; ++l) {
         const int m = round4(cube_size(sizes[l]));
@@ -816,10 +817,11 @@ __device__ __forceinline__ void coarse27_body(const float4* __restrict__ image, 
         const float* rhs = sm + lay.rhs[l];
         if (l == count - 1) {  // side 3: e = A^-1 rhs
             if (tid < kInvN) {
-                const float* inv = sm + lay.inverse;
-                float v = 0.0f;
-                for (int j = 0; j < kInvN; ++j) v += inv[tid * kInvN + j] * rhs[cube_at(j % 3, (j / 3) % 3, j / 9, 3)];
-                e[cube_at(tid % 3, (tid / 3) % 3, tid / 9, 3)] = v;
+                const double* inv = reinterpret_cast<const double*>(sm + lay.inverse);
+                double v = 0.0;
+                for (int j = 0; j < kInvN; ++j)
+                    v += inv[tid * kInvN + j] * (double)rhs[cube_at(j % 3, (j / 3) % 3, j / 9, 3)];
+                e[cube_at(tid % 3, (tid / 3) % 3, tid / 9, 3)] = (float)v;
             }
             __syncthreads();
             break;
@@ -1018,7 +1020,7 @@ extern "C" int pb_level27_finish_f32(const float* coef, int64_t n, float* invD, 
 }
 
 // Inverse (27 x 27, FP32 row-major) of a 27-point level of side 3.
-extern "C" int pb_coarse_inverse_f32(const float* coef, int64_t n, float* inverse, void* stream) {
+extern "C" int pb_coarse_inverse_f64(const float* coef, int64_t n, double* inverse, void* stream) {
     if (n != 3 || !coef || !inverse) return fail(PB_ERR_INVALID, "coarse inverse: side must be 3");
     coarse_inverse_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(coef, padded_size(3), geom(3), inverse);
     PB_CHECK_LAUNCH("coarse_inverse_kernel");
@@ -1045,9 +1047,9 @@ extern "C" size_t pb_coarse27_image_size(int64_t count, const int64_t* sizes) {
 
 // The image the single-block cycle reads: per level but the last, couplings
 // (from its 14 planes), 1/diagonal and prolongation weights; then the 3^3
-// inverse (from pb_coarse_inverse_f32).  image: 16-byte aligned.
+// inverse (FP64, from pb_coarse_inverse_f64).  image: 16-byte aligned.
 extern "C" int pb_coarse27_image_f32(int64_t count, const int64_t* sizes, const float* const* coef,
-                                     const float* const* invD, const float* const* weights, const float* inverse,
+                                     const float* const* invD, const float* const* weights, const double* inverse,
                                      float* image, size_t image_bytes, void* stream) {
     int sz[kC27MaxLevels];
     PB_TRY(coarse_sizes(count, sizes, sz));
@@ -1064,7 +1066,7 @@ extern "C" int pb_coarse27_image_f32(int64_t count, const int64_t* sizes, const 
                                                             image + lay.fac[l]);
         PB_CHECK_LAUNCH("coarse_image_kernel");
     }
-    PB_CHECK_CUDA(cudaMemcpyAsync(image + lay.inverse, inverse, sizeof(float) * kInvN * kInvN,
+    PB_CHECK_CUDA(cudaMemcpyAsync(image + lay.inverse, inverse, sizeof(double) * kInvN * kInvN,
                                   cudaMemcpyDeviceToDevice, s),
                   "coarse27 image inverse");
     return PB_OK;
@@ -1286,7 +1288,7 @@ int launch_coarse27(const GridDesc* descs, int count, int64_t blocks, int first_
 // Same launches in the same order as the separate entry points.
 extern "C" int pb_hierarchy_setup_f32(int64_t levels, const int64_t* sides, const void* const* arrays,
                                       int64_t first_coarse, const double* screen, double point_weight,
-                                      void* galerkin_ws, size_t galerkin_bytes, float* inverse, float* image,
+                                      void* galerkin_ws, size_t galerkin_bytes, double* inverse, float* image,
                                       size_t image_bytes, void* stream) {
     constexpr int A = PB_LEVEL_ARRAYS;
     if (levels < 2 || levels > 13 || !sides || !arrays || !screen || !inverse || !image || first_coarse < 0 ||
@@ -1323,7 +1325,7 @@ extern "C" int pb_hierarchy_setup_f32(int64_t levels, const int64_t* sides, cons
                                  (void*)arrays[(l - 1) * A + 5], (float*)arrays[(l - 1) * A + 6],
                                  (float*)arrays[(l - 1) * A + 7], stream));
     }
-    PB_TRY(pb_coarse_inverse_f32(coef(levels - 1), 3, inverse, stream));
+    PB_TRY(pb_coarse_inverse_f64(coef(levels - 1), 3, inverse, stream));
     const int64_t tail = levels - first_coarse;
     const float* tc[kC27MaxLevels];
     const float* ti[kC27MaxLevels];

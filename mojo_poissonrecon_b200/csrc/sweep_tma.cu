@@ -110,12 +110,23 @@ __device__ __forceinline__ float4 lds4(const float* p) { return *reinterpret_cas
 // the updated columns of a group on box row br are j = s and s + 2 with
 // s = (br + t) & 1 in both phases.
 constexpr int kThreads = 352;  // 19 box rows x 18 groups = 342 work items, one per thread
+// SPLIT mapping: threads 0..191 take the odd box rows 1..19 (180 items) and
+// threads 192..383 the even rows 2..18 (162 items), so every warp's rows share
+// one parity, s is warp-uniform, and each phase computes only the two lanes it
+// updates (the others are selected away in the default mapping).
+constexpr int kSplitHalf = 192, kSplitThreads = 2 * kSplitHalf;
+static_assert(10 * kGroups <= kSplitHalf && 9 * kGroups <= kSplitHalf, "one item per thread");
 
 // The sweep of tile (bx, by) and z chunk bz; the maps may live in kernel
 // parameters (single grid) or in global memory (grouped launches).
-template <bool ZERO_IN, int SLOTS>
+// ONE_BAR: the ring slot of plane t - 2 is refilled right after plane t's first
+// barrier (plane t - 2 was last read by the previous step's colour-1 pass), so
+// the barrier at the end of each step goes; needs SLOTS >= 4 (plane t + 1,
+// waited for at step t, is issued at step t + 3 - SLOTS).
+template <bool ZERO_IN, int SLOTS, bool SPLIT = false, bool ONE_BAR = false>
 __device__ __forceinline__ void sweep_body(const CUtensorMap* map_e, const CUtensorMap* map_rhs,
                                            const CUtensorMap* map_invD, const Params& p, int bx, int by, int bz) {
+    static_assert(!ONE_BAR || SLOTS >= 4, "the early refill needs four ring slots");
     constexpr int TY = kTY;
     using G = Geo2<TY, SLOTS>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -150,8 +161,17 @@ __device__ __forceinline__ void sweep_body(const CUtensorMap* map_e, const CUten
     if (tid == 0)
         for (; issued <= zlast && issued < zfirst + SLOTS; ++issued) issue(issued);
 
-    // this thread's work item
-    const int br = 1 + tid / kGroups, g = tid - (br - 1) * kGroups;
+    // this thread's work item (rows past the box: no work, barriers only)
+    int br, g;
+    if (SPLIT) {
+        const bool odd = tid < kSplitHalf;
+        const int item = odd ? tid : tid - kSplitHalf, r = item / kGroups;
+        br = (odd ? 1 : 2) + 2 * r;
+        g = item - r * kGroups;
+    } else {
+        br = 1 + tid / kGroups;
+        g = tid - (br - 1) * kGroups;
+    }
     const bool has_a = br <= H + 2;                                       // colour-0 region rows 1 .. H+2
     const bool has_b = br >= 2 && br <= H + 1 && g >= 1 && g <= (W + 3) / 4;  // output rows and groups
     const int base = br * kBoxX + 4 * g;
@@ -184,6 +204,21 @@ __device__ __forceinline__ void sweep_body(const CUtensorMap* map_e, const CUten
             float v[4];
             if (ZERO_IN) {
                 v[0] = r_cur.x * i_cur.x; v[1] = r_cur.y * i_cur.y; v[2] = r_cur.z * i_cur.z; v[3] = r_cur.w * i_cur.w;
+            } else if (SPLIT) {  // s is warp-uniform: only the updated lanes
+                e_next = lds4(S.slot[slot_of(t + 1)][0] + base);
+                const float4 u = lds4(e + base - kBoxX), d = lds4(e + base + kBoxX);
+                const float4 c = e_cur, zm = e_prev, zp = e_next;
+                if (s == 0) {
+                    const float L = g > 0 ? e[base - 1] : 0.0f;
+                    v[0] = (r_cur.x + (L + c.y + u.x + d.x + zm.x + zp.x) * h2) * i_cur.x;
+                    v[2] = (r_cur.z + (c.y + c.w + u.z + d.z + zm.z + zp.z) * h2) * i_cur.z;
+                    v[1] = v[3] = 0.0f;
+                } else {
+                    const float R = g < kGroups - 1 ? e[base + 4] : 0.0f;
+                    v[1] = (r_cur.y + (c.x + c.z + u.y + d.y + zm.y + zp.y) * h2) * i_cur.y;
+                    v[3] = (r_cur.w + (c.z + R + u.w + d.w + zm.w + zp.w) * h2) * i_cur.w;
+                    v[0] = v[2] = 0.0f;
+                }
             } else {
                 e_next = lds4(S.slot[slot_of(t + 1)][0] + base);
                 const float4 u = lds4(e + base - kBoxX), d = lds4(e + base + kBoxX);
@@ -200,22 +235,38 @@ __device__ __forceinline__ void sweep_body(const CUtensorMap* map_e, const CUten
             for (int j = 0; j < 4; ++j) cc[j] = ((j & 1) == s && upd_ok[j]) ? v[j] : cc[j];
             red_cur = make_float4(cc[0], cc[1], cc[2], cc[3]);
             *reinterpret_cast<float4*>(S.slot[slot_of(t)][0] + base) = red_cur;
+            if (ONE_BAR) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // before a TMA refill
         }
         ok = __syncthreads_and(arrived);
         if (!ok) break;
+        if (ONE_BAR && tid == 0 && t - 2 >= zfirst && issued <= zlast) issue(issued++);  // into plane t-2's slot
         if (has_b && t - 1 >= zb) {  // colour 1 of plane t-1, written out with its colour 0
             const int z = t - 1;
             const float* e = S.slot[slot_of(z)][0];
             const float4 u = lds4(e + base - kBoxX), d = lds4(e + base + kBoxX);
-            const float L = e[base - 1];
-            const float R = g < kGroups - 1 ? e[base + 4] : 0.0f;
             const float4 c = red_prev, zm = red_prev2, zp = red_cur;
             const int s = (br + t) & 1;
             float v[4];
-            v[0] = (r_prev.x + (L + c.y + u.x + d.x + zm.x + zp.x) * h2) * i_prev.x;
-            v[1] = (r_prev.y + (c.x + c.z + u.y + d.y + zm.y + zp.y) * h2) * i_prev.y;
-            v[2] = (r_prev.z + (c.y + c.w + u.z + d.z + zm.z + zp.z) * h2) * i_prev.z;
-            v[3] = (r_prev.w + (c.z + R + u.w + d.w + zm.w + zp.w) * h2) * i_prev.w;
+            if (SPLIT) {  // s is warp-uniform: only the updated lanes
+                if (s == 0) {
+                    const float L = e[base - 1];
+                    v[0] = (r_prev.x + (L + c.y + u.x + d.x + zm.x + zp.x) * h2) * i_prev.x;
+                    v[2] = (r_prev.z + (c.y + c.w + u.z + d.z + zm.z + zp.z) * h2) * i_prev.z;
+                    v[1] = v[3] = 0.0f;
+                } else {
+                    const float R = g < kGroups - 1 ? e[base + 4] : 0.0f;
+                    v[1] = (r_prev.y + (c.x + c.z + u.y + d.y + zm.y + zp.y) * h2) * i_prev.y;
+                    v[3] = (r_prev.w + (c.z + R + u.w + d.w + zm.w + zp.w) * h2) * i_prev.w;
+                    v[0] = v[2] = 0.0f;
+                }
+            } else {
+                const float L = e[base - 1];
+                const float R = g < kGroups - 1 ? e[base + 4] : 0.0f;
+                v[0] = (r_prev.x + (L + c.y + u.x + d.x + zm.x + zp.x) * h2) * i_prev.x;
+                v[1] = (r_prev.y + (c.x + c.z + u.y + d.y + zm.y + zp.y) * h2) * i_prev.y;
+                v[2] = (r_prev.z + (c.y + c.w + u.z + d.z + zm.z + zp.z) * h2) * i_prev.z;
+                v[3] = (r_prev.w + (c.z + R + u.w + d.w + zm.w + zp.w) * h2) * i_prev.w;
+            }
             float o[4] = {c.x, c.y, c.z, c.w};
 #pragma unroll
             for (int j = 0; j < 4; ++j) o[j] = ((j & 1) == s) ? v[j] : o[j];
@@ -235,8 +286,10 @@ __device__ __forceinline__ void sweep_body(const CUtensorMap* map_e, const CUten
         i_prev = i_cur;
         e_prev = e_cur;
         e_cur = e_next;
-        __syncthreads();  // plane t-1 is no longer read
-        if (tid == 0 && t - 1 >= zfirst && issued <= zlast) issue(issued++);
+        if (!ONE_BAR) {
+            __syncthreads();  // plane t-1 is no longer read
+            if (tid == 0 && t - 1 >= zfirst && issued <= zlast) issue(issued++);
+        }
     }
     if (!ok) {
         if (tid == 0) {
@@ -251,11 +304,11 @@ __device__ __forceinline__ void sweep_body(const CUtensorMap* map_e, const CUten
 // SLOTS planes in the shared ring (at least 3: planes t-1, t, t+1), MINB
 // resident blocks per SM the register budget must allow; the autotuner picks
 // among the compiled pairs (PB_TUNE_SWEEP_VARIANT).
-template <bool ZERO_IN, int SLOTS, int MINB>
-__global__ void __launch_bounds__(kThreads, MINB)
+template <bool ZERO_IN, int SLOTS, int MINB, bool SPLIT = false, bool ONE_BAR = false>
+__global__ void __launch_bounds__(SPLIT ? kSplitThreads : kThreads, MINB)
     sweep_kernel(const __grid_constant__ CUtensorMap map_e, const __grid_constant__ CUtensorMap map_rhs,
                  const __grid_constant__ CUtensorMap map_invD, Params p) {
-    sweep_body<ZERO_IN, SLOTS>(&map_e, &map_rhs, &map_invD, p, blockIdx.x, blockIdx.y, blockIdx.z);
+    sweep_body<ZERO_IN, SLOTS, SPLIT, ONE_BAR>(&map_e, &map_rhs, &map_invD, p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Grouped: one launch over the level-0 sweeps of many clouds (batch.cuh).
@@ -326,7 +379,10 @@ static int make_map(CUtensorMap* map, const float* base, int n, int P, int rows)
 constexpr int kRCX = 64, kRCY = 4;
 constexpr int kRFX = 2 * kRCX + 8, kRFY = 2 * kRCY + 1;  // 136 x 9 residuals: fine x from 2 xc0 - 4, y from 2 yc0 - 1
 constexpr int kREX = kRFX + 8, kREY = kRFY + 2;          // 144 x 11 of e: fine x from 2 xc0 - 8, y from 2 yc0 - 2
-constexpr int kRSlots = 4, kRRes = 3, kRThreads = 256;
+constexpr int kRSlots = 4;
+constexpr int kRRes = 3;  // residual planes 2zc-1 .. 2zc+1
+constexpr int kRThreads = 320;  // one float4 item of a fine plane per thread (306 items); 256 restrict
+static_assert(kRFY * (kRFX / 4) <= kRThreads && kRCX * kRCY <= kRThreads, "one round per plane");
 constexpr int kREStride = (kREX * kREY + 31) / 32 * 32;  // 128-byte aligned boxes
 constexpr int kRFStride = (kRFX * kRFY + 31) / 32 * 32;
 constexpr uint32_t kREBytes = kREX * kREY * 4, kRFBytes = kRFX * kRFY * 4;
@@ -421,7 +477,7 @@ __global__ void __launch_bounds__(kRThreads, 2)
             const int zc = (f - 1) / 2;
             const int cy = tid / kRCX, cx = tid - cy * kRCX;
             const int xc = xc0 + cx, yc = yc0 + cy;
-            if (xc < cn && yc < cn) {
+            if (cy < kRCY && xc < cn && yc < cn) {
                 float sum = 0.0f;
 #pragma unroll
                 for (int oz = -1; oz <= 1; ++oz) {
@@ -436,7 +492,7 @@ __global__ void __launch_bounds__(kRThreads, 2)
                 }
                 coarse[((int64_t)(zc + 1) * (cn + 2) + (yc + 1)) * cP + (xc + 4)] = sum * (1.0f / 64.0f);
             }
-            __syncthreads();  // before plane f + 1 overwrites the residual of plane 2 zc - 1
+            // plane 2zc+2 (the slot of 2zc-1) is written after the next step's barrier
         }
         if (tid == 0 && issued <= pe1) {  // into the slot of plane f - 1, read for the last time above
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -578,10 +634,13 @@ extern "C" int pb_sweep_tma_f32(const float* e_in, float* e_out, const float* rh
     prm.ntx = (N - 1) / kTX > 0 ? (N - 1) / kTX : 1;
     prm.nty = (N - 1) / kTY > 0 ? (N - 1) / kTY : 1;
     const int tiles = prm.ntx * prm.nty;
-    // ring slots and resident blocks per SM: (5, 2) built in, (4, 3) and (3, 3) as variants
+    // ring slots and resident blocks per SM: (5, 2) built in, (4, 3) and (3, 3) as
+    // variants 1 and 2; variants 3, 4 and 5: the SPLIT mapping with (5, 2), (6, 2),
+    // (4, 3); variants 6, 7 and 8: the same with ONE_BAR
     const int64_t variant = tuned(PB_TUNE_SWEEP_VARIANT, n, 0);
-    const int ring = variant == 1 ? 4 : variant == 2 ? 3 : kSlots;
-    const int per_sm = variant == 0 ? PB_SWEEP_MIN_BLOCKS : 3;
+    const int64_t v3 = variant >= 6 ? variant - 3 : variant;
+    const int ring = v3 == 1 || v3 == 5 ? 4 : v3 == 2 ? 3 : v3 == 4 ? 6 : kSlots;
+    const int per_sm = v3 == 1 || v3 == 2 || v3 == 5 ? 3 : PB_SWEEP_MIN_BLOCKS;
     if (z_chunk <= 0) z_chunk = tuned(PB_TUNE_SWEEP_Z_CHUNK, n, 0);
     if (z_chunk <= 0) {
         // c chunks per tile: minimise waves x (planes per chunk + the 4 planes a
@@ -613,15 +672,33 @@ extern "C" int pb_sweep_tma_f32(const float* e_in, float* e_out, const float* rh
     PB_TRY(make_map(&me, mode == 1 ? rhs : e_in, N, prm.P, kBoxY));
     const dim3 grid(prm.ntx, prm.nty, (N + prm.z_chunk - 1) / prm.z_chunk);
     cudaStream_t s = (cudaStream_t)stream;
+    const bool split = variant >= 3 && variant <= 8;
     auto launch = [&](auto kernel, size_t smem) -> int {
         PB_CHECK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                       "sweep_tma smem");
-        kernel<<<grid, kThreads, smem, s>>>(me, mr, mi, prm);
+        kernel<<<grid, split ? kSplitThreads : kThreads, smem, s>>>(me, mr, mi, prm);
         PB_CHECK_LAUNCH("sweep_tma kernel");
         return PB_OK;
     };
     const size_t s5 = sizeof(Geo2<kTY, kSlots>::Smem) + 128, s4 = sizeof(Geo2<kTY, 4>::Smem) + 128,
                  s3 = sizeof(Geo2<kTY, 3>::Smem) + 128;
+    if (variant == 3)
+        return mode == 1 ? launch(sweep_kernel<true, 5, 2, true>, sizeof(Geo2<kTY, 5>::Smem) + 128)
+                         : launch(sweep_kernel<false, 5, 2, true>, sizeof(Geo2<kTY, 5>::Smem) + 128);
+    if (variant == 4)
+        return mode == 1 ? launch(sweep_kernel<true, 6, 2, true>, sizeof(Geo2<kTY, 6>::Smem) + 128)
+                         : launch(sweep_kernel<false, 6, 2, true>, sizeof(Geo2<kTY, 6>::Smem) + 128);
+    if (variant == 5)
+        return mode == 1 ? launch(sweep_kernel<true, 4, 3, true>, s4) : launch(sweep_kernel<false, 4, 3, true>, s4);
+    if (variant == 6)
+        return mode == 1 ? launch(sweep_kernel<true, 5, 2, true, true>, s5)
+                         : launch(sweep_kernel<false, 5, 2, true, true>, s5);
+    if (variant == 7)
+        return mode == 1 ? launch(sweep_kernel<true, 6, 2, true, true>, sizeof(Geo2<kTY, 6>::Smem) + 128)
+                         : launch(sweep_kernel<false, 6, 2, true, true>, sizeof(Geo2<kTY, 6>::Smem) + 128);
+    if (variant == 8)
+        return mode == 1 ? launch(sweep_kernel<true, 4, 3, true, true>, s4)
+                         : launch(sweep_kernel<false, 4, 3, true, true>, s4);
     if (ring == 4)
         return mode == 1 ? launch(sweep_kernel<true, 4, 3>, s4) : launch(sweep_kernel<false, 4, 3>, s4);
     if (ring == 3)

@@ -76,7 +76,7 @@ def hierarchy_bytes(n: int) -> int:
         total += 20 * 4 * _padded(m)
         if m > solver32.COARSE_N:  # packed per colour
             total += 2 * 68 * (m * m * ((m + 1) // 2))
-    return total + 4 * 27 * 27 + 64 * 1024  # 3^3 inverse, coarse image
+    return total + 8 * 27 * 27 + 64 * 1024  # 3^3 inverse (FP64), coarse image
 
 
 def footprint_bytes(depth: int, points: int) -> int:

@@ -163,7 +163,7 @@ class Hierarchy32:
                 lv.pack(device, self.lib)
                 if self.transient_coef:
                     lv.coef = None
-        self.inverse = torch.zeros(27 * 27, dtype=torch.float32, device=device)  # of the 3^3 level
+        self.inverse = torch.zeros(27 * 27, dtype=torch.float64, device=device)  # of the 3^3 level, FP64
         # scratch of the separable Galerkin products (27-point fine levels), at most GALERKIN_SCRATCH bytes;
         # hierarchies set up one after another on one stream may share one (galerkin_ws)
         size = galerkin_scratch_bytes(n, self.levels)
@@ -191,7 +191,7 @@ class Hierarchy32:
 
     def nbytes(self) -> int:
         return sum(t.numel() * t.element_size() for lv in self.levels for t in lv.tensors()) + \
-            self.inverse.numel() * 4 + self.image.numel() * 4 + self.galerkin_ws.numel() * 4
+            self.inverse.numel() * 8 + self.image.numel() * 4 + self.galerkin_ws.numel() * 4
 
     def setup(self, screen: torch.Tensor, point_weight: float) -> None:
         """Level 0 from the FP64 screen (D = (deg + pw*screen) h^-2, core.py:150-163),

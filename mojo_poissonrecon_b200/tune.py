@@ -71,9 +71,9 @@ def candidates(param: int, n: int) -> list[int]:
     if param == FCG_DIRECTION_VARIANT:
         return [0, 1, 2]
     if param == FCG_UPDATE_VARIANT:
-        return [0, 1, 2, 3]
+        return [0, 1, 2, 3, 4]
     if param == SWEEP_VARIANT:
-        return [0, 1, 2]
+        return list(range(9))
     if param == RESTRICT_VARIANT:
         return [0, 1, 2]
     if param in (RELAX27_VARIANT, RESIDUAL27_VARIANT):

@@ -226,7 +226,7 @@ def test_fcg_launch_variants_are_bit_identical(L, n):
     L.pb_tune_clear()
     try:
         want = run()
-        for param, value in [(tune.FCG_UPDATE_VARIANT, v) for v in (1, 2, 3)] + \
+        for param, value in [(tune.FCG_UPDATE_VARIANT, v) for v in (1, 2, 3, 4)] + \
                             [(tune.FCG_DIRECTION_VARIANT, v) for v in (1, 2)]:
             assert param in tune.SEARCHED
             assert L.pb_tune_set(param, n, value) == 0

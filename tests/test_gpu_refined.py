@@ -180,10 +180,11 @@ def test_engine_graphs_replay_new_inputs():
     assert torch.equal(replayed, fresh)
 
 
-@pytest.mark.parametrize("n", [65, 257])
+@pytest.mark.parametrize("n", [33, 65, 257])
 def test_sweep_variants_bit_identical(L, n):
-    """The sweep's autotuned variants (shared-ring depth, resident blocks per SM)
-    and z chunks compute the same bits as the built-in launch shape."""
+    """The sweep's autotuned variants (shared-ring depth, resident blocks per SM,
+    rows grouped by parity per warp, one barrier per plane) and z chunks (odd and
+    even chunk starts) compute the same bits as the built-in launch shape."""
     from mojo_poissonrecon_b200 import tune
 
     screen, rhs, x, D, invD, W = setup(L, n, 31 * n)
@@ -201,8 +202,8 @@ def test_sweep_variants_bit_identical(L, n):
     L.pb_tune_clear()
     try:
         want = [sweep(0), sweep(1)]
-        for variant in (1, 2):
-            for z_chunk in (0, 17):
+        for variant in range(1, 9):
+            for z_chunk in (0, 4, 5, 17):
                 L.pb_tune_set(tune.SWEEP_VARIANT, n, variant)
                 L.pb_tune_set(tune.SWEEP_Z_CHUNK, n, z_chunk)
                 got = [sweep(0), sweep(1)]
