@@ -403,7 +403,8 @@ def kernel_rooflines(eng, n: int, L) -> list:
 
     var = {name: int(L.pb_tune_get(code, n)) for name, code in
            (("sweep", 7), ("restrict", 8), ("direction", 5), ("update", 6))}  # PB_TUNE_*_VARIANT
-    rr_name = {1: "residual_restrict32_paired_kernel", 2: "tma::residual_restrict_tma_kernel"}.get(
+    rr_name = {1: "residual_restrict32_paired_kernel", 2: "tma::residual_restrict_tma_kernel",
+               3: "residual_restrict32_paired320_kernel"}.get(
         var["restrict"], "residual_restrict32_kernel")
     dir_name = f"fcg::direction_sums_kernel<{(4, 6, 8)[var['direction']]}>"
     upd_name = ({3: "fcg::update_residual_prefetch_kernel<24, 3>", 4: "fcg::update_residual_prefetch_kernel<24, 4>"}

@@ -46,6 +46,14 @@ const char *pb_last_error(void);
 int pb_version(void);
 /* Number of kernels this library has launched in the process so far. */
 long long pb_launch_count(void);
+/* 1 in the checked build (libpoisson_b200_checked.so, compiled with
+ * -DPB_CHECKED), 0 otherwise.  No counterpart in the reference. */
+int pb_checked_build(void);
+/* The checked build's device error word: 0, or (site << 56) | index of the
+ * first padded index or guarded store found outside its array (the access was
+ * redirected to index 0 or skipped).  clear != 0 resets it.  Synchronous.  The
+ * normal build reports 0. */
+int pb_check_status(uint64_t *word, int clear);
 
 /* Replaces mpr_parallel_init (_lib.py:21; capi.mojo:36-38): selects `device`
  * and checks it is an sm_100 part.  Optional; every call works without it. */
@@ -454,7 +462,8 @@ int pb_batch_loop_condition(unsigned long long handle, const double *scal, const
  *                          blocks per SM, 1 = 6, 2 = 8
  *   RESTRICT_VARIANT       pb_residual_restrict_f32: 1 = both fine planes of a coarse
  *                          plane in one loop over their items; 2 = the FP32 cycle
- *                          calls pb_residual_restrict_tma_f32 instead
+ *                          calls pb_residual_restrict_tma_f32 instead; 3 = as 1 with
+ *                          320 threads per block
  *   RELAX27_VARIANT        pb_relax27p_f32 (per level side): 1 = the neighbour planes
  *                          staged in shared memory
  *   RESIDUAL27_VARIANT     pb_residual_restrict27p_f32 (per level side): 1 = the

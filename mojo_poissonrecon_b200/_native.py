@@ -103,9 +103,14 @@ _SIGNATURES = {
     "pb_tune_set": ([I, I, I], C),
     "pb_tune_get": ([I, I], I),
     "pb_tune_clear": ([], C),
+    "pb_checked_build": ([], C),
+    "pb_check_status": ([ctypes.POINTER(ctypes.c_uint64), C], C),
 }
 
-LIBRARY_PATH = _build.LIBRARY
+# MPR_B200_CHECKED=1 loads the checked build (bounds-checked indices and stores
+# reporting to a device word; pb_check_status) in place of the normal one.
+CHECKED = os.environ.get("MPR_B200_CHECKED", "0") == "1"
+LIBRARY_PATH = _build.CHECKED_LIBRARY if CHECKED else _build.LIBRARY
 _loaded: ctypes.CDLL | None = None
 
 
@@ -123,7 +128,7 @@ def lib() -> ctypes.CDLL:
     if _loaded is None:
         path = LIBRARY_PATH
         if not os.path.exists(path):
-            path = _build.build()
+            path = _build.build(checked=CHECKED)
         cdll = ctypes.CDLL(path)
         for name, (argtypes, restype) in _SIGNATURES.items():
             fn = getattr(cdll, name)
@@ -135,6 +140,23 @@ def lib() -> ctypes.CDLL:
 
 def exported_symbols() -> list[str]:
     return list(_SIGNATURES)
+
+
+CHECK_SITES = {1: "padded FP32 level index", 2: "padded index in the FCG passes", 3: "TMA sweep store",
+               4: "FCG pass-2 store", 5: "FP32 prolongation store", 6: "FP64 red-black store"}
+
+
+def decode_check_word(word: int) -> tuple[int, int]:
+    """(site, index) of a check word (site 0: no failure); sites in CHECK_SITES."""
+    return int(word) >> 56, int(word) & ((1 << 56) - 1)
+
+
+def check_word(clear: bool = True) -> int:
+    """The checked build's device error word (0: no index left its array);
+    always 0 in the normal build.  Synchronises the device."""
+    word = ctypes.c_uint64()
+    check(lib().pb_check_status(ctypes.byref(word), int(clear)), "check status")
+    return int(word.value)
 
 
 def check(status: int, what: str = "") -> None:

@@ -42,7 +42,7 @@ import numpy as np
 import torch
 
 from . import _native as nat
-from . import _sync, core
+from . import _sync, _trace, core
 from .solver import SolveStats, norm
 from .solver32 import (GRAPH_CAPTURE_LOCK, MAX_ITER, TMA_MIN_N, Hierarchy32, apply_tuning, galerkin_scratch_bytes,
                        level0_sweeps)
@@ -486,6 +486,13 @@ def reconstruct_many(clouds, *, depth: int = 6, point_weight: float = 4.0, confi
 
 def _run_wave(wave, out, dev, point_weight, confidence, scale, samples_per_node, tol, max_cycles, device_out,
               phases: _Phases):
+    with _trace.stage(f"batch wave of {len(wave)}"):
+        _run_wave_body(wave, out, dev, point_weight, confidence, scale, samples_per_node, tol, max_cycles,
+                       device_out, phases)
+
+
+def _run_wave_body(wave, out, dev, point_weight, confidence, scale, samples_per_node, tol, max_cycles, device_out,
+                   phases: _Phases):
     L = nat.lib()
     ctx = core._Context()
     s = ctx.stream

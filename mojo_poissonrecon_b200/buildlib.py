@@ -6,7 +6,12 @@ for bit are compiled with `-fmad=false` (no fused multiply-add); the FP32
 solver units keep FMA.  The CUDA runtime is linked statically, so the library
 needs only the driver at run time.
 
-    python -m mojo_poissonrecon_b200.buildlib [--force] [--verbose]
+`--checked` builds `libpoisson_b200_checked.so` instead: the same sources with
+`-DPB_CHECKED` and relocatable device code (one device error word shared by
+every unit), whose index helpers and guarded stores report out-of-range
+indices to that word instead of touching memory (`csrc/checked.cuh`).
+
+    python -m mojo_poissonrecon_b200.buildlib [--force] [--verbose] [--checked]
 """
 
 from __future__ import annotations
@@ -22,7 +27,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 LIBRARY = os.path.join(HERE, "libpoisson_b200.so")
+CHECKED_LIBRARY = os.path.join(HERE, "libpoisson_b200_checked.so")
 OBJDIR = os.path.join(HERE, "_build")
+CHECKED_OBJDIR = os.path.join(HERE, "_build_checked")
+CHECKED_FLAGS = ["-DPB_CHECKED", "-rdc=true"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
           "--expt-relaxed-constexpr"]
@@ -49,9 +57,9 @@ def _deps_mtime() -> float:
     return max(newest, os.path.getmtime(__file__))
 
 
-def _compile(src: str, verbose: bool) -> tuple[str, str]:
-    obj = os.path.join(OBJDIR, src[:-3] + ".o")
-    flags = ARCH + COMMON + ["-I", INCLUDE]
+def _compile(src: str, verbose: bool, checked: bool = False) -> tuple[str, str]:
+    obj = os.path.join(CHECKED_OBJDIR if checked else OBJDIR, src[:-3] + ".o")
+    flags = ARCH + COMMON + ["-I", INCLUDE] + (CHECKED_FLAGS if checked else [])
     if src in EXACT_FP64:
         flags += ["-fmad=false"]
     if verbose:
@@ -63,30 +71,33 @@ def _compile(src: str, verbose: bool) -> tuple[str, str]:
     return obj, proc.stderr
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    """Build (if stale) and return the path of libpoisson_b200.so."""
-    if not force and os.path.exists(LIBRARY) and os.path.getmtime(LIBRARY) >= _deps_mtime():
-        return LIBRARY
-    os.makedirs(OBJDIR, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, checked: bool = False) -> str:
+    """Build (if stale) and return the path of libpoisson_b200.so (checked=True:
+    libpoisson_b200_checked.so)."""
+    library = CHECKED_LIBRARY if checked else LIBRARY
+    if not force and os.path.exists(library) and os.path.getmtime(library) >= _deps_mtime():
+        return library
+    os.makedirs(CHECKED_OBJDIR if checked else OBJDIR, exist_ok=True)
     srcs = sources()
     with concurrent.futures.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as pool:
-        results = list(pool.map(lambda s: _compile(s, verbose), srcs))
+        results = list(pool.map(lambda s: _compile(s, verbose, checked), srcs))
     if verbose:
         for (_, log), src in zip(results, srcs):
             if log.strip():
                 print(f"== {src}\n{log}", file=sys.stderr)
-    tmp = LIBRARY + ".tmp"
-    cmd = [nvcc(), "-shared", "-o", tmp] + ARCH + [obj for obj, _ in results]
+    tmp = library + ".tmp"
+    cmd = [nvcc(), "-shared", "-o", tmp] + ARCH + (["-rdc=true"] if checked else []) + [obj for obj, _ in results]
     proc = subprocess.run(cmd, capture_output=True, text=True)
     if proc.returncode:
         raise RuntimeError(f"nvcc link failed:\n{proc.stderr[-6000:]}")
-    os.replace(tmp, LIBRARY)
-    return LIBRARY
+    os.replace(tmp, library)
+    return library
 
 
 if __name__ == "__main__":
     parser = argparse.ArgumentParser()
     parser.add_argument("--force", action="store_true")
     parser.add_argument("--verbose", action="store_true")
+    parser.add_argument("--checked", action="store_true")
     args = parser.parse_args()
-    print(build(force=args.force, verbose=args.verbose))
+    print(build(force=args.force, verbose=args.verbose, checked=args.checked))

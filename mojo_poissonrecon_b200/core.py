@@ -20,7 +20,7 @@ import numpy as np
 import torch
 
 from . import _native as nat
-from . import _sync, solver
+from . import _sync, _trace, solver
 from ._convert import f64, i64
 
 MAX_DEPTH = 10
@@ -273,20 +273,24 @@ def _iso_value(ctx: _Context, field: torch.Tensor, points: torch.Tensor, normals
 def _solve_device(ctx: _Context, points: torch.Tensor, normals: torch.Tensor, *, depth: int, point_weight: float,
                   confidence: bool, cycles: int, samples_per_node: float, precision: str, tol, max_cycles: int,
                   octree: bool, refine_method: str = "fcg"):
-    tree = _octree_device(ctx, points, depth) if octree else None
-    grids, accepted = _splat_assemble(ctx, points, normals, depth, point_weight, confidence, samples_per_node)
+    with _trace.stage("octree"):
+        tree = _octree_device(ctx, points, depth) if octree else None
+    with _trace.stage("splat"):
+        grids, accepted = _splat_assemble(ctx, points, normals, depth, point_weight, confidence, samples_per_node)
     ctx.ws = nat.Workspace(ctx.device)  # the splat's scratch (GBs at 20M points) is not needed past here
     count = points.shape[0]
-    if precision == "fp64":
-        field, stats = solver.solve_fp64(grids["rhs"], grids["screen"], point_weight, ctx.ws, cycles=cycles,
-                                         tol=tol, max_cycles=max_cycles, has_points=count > 0)
-    else:
-        from . import solver32
-        field, stats = solver32.solve_refined(grids["rhs"], grids["screen"], point_weight, ctx.ws,
-                                              tol=1e-8 if tol is None else tol, max_cycles=max_cycles,
-                                              has_points=count > 0,
-                                              method="defect" if precision == "fp32_defect" else refine_method)
-    iso = _iso_value(ctx, field, points, normals, confidence)
+    with _trace.stage("solve"):
+        if precision == "fp64":
+            field, stats = solver.solve_fp64(grids["rhs"], grids["screen"], point_weight, ctx.ws, cycles=cycles,
+                                             tol=tol, max_cycles=max_cycles, has_points=count > 0)
+        else:
+            from . import solver32
+            field, stats = solver32.solve_refined(grids["rhs"], grids["screen"], point_weight, ctx.ws,
+                                                  tol=1e-8 if tol is None else tol, max_cycles=max_cycles,
+                                                  has_points=count > 0,
+                                                  method="defect" if precision == "fp32_defect" else refine_method)
+    with _trace.stage("iso"):
+        iso = _iso_value(ctx, field, points, normals, confidence)
     if count and int(accepted.item()) != count:
         raise RuntimeError(f"splat accepted {int(accepted.item())} of {count} validated samples")
     return field, grids, iso, stats, tree
@@ -486,17 +490,20 @@ def reconstruct(
     if points.shape[0] == 0:
         return empty()
     ctx = _Context()
-    dp, dn, count, fmap = _prepare(ctx, _to_device(points, ctx.device), _to_device(normals, ctx.device), scale)
+    with _trace.stage("prepare"):
+        dp, dn, count, fmap = _prepare(ctx, _to_device(points, ctx.device), _to_device(normals, ctx.device), scale)
     if count == 0:
         return empty()
     # The reference also builds the octree here and discards it; it feeds no output.
     field, grids, iso, stats, _ = _solve_device(
         ctx, dp, dn, depth=depth, point_weight=point_weight, confidence=confidence, cycles=cycles,
         samples_per_node=samples_per_node, precision=precision, tol=tol, max_cycles=max_cycles, octree=False)
-    vertices, faces, vdens = _extract_device(ctx, field, grids["density"], iso)
-    ctx.check(ctx.lib.pb_map_vertices_f64(vertices.data_ptr(), vertices.shape[0], fmap.data_ptr(), ctx.stream),
-              "map vertices")
-    v, f, d, iso_h = _host_all([vertices, faces, vdens, iso], device_out)
+    with _trace.stage("extract"):
+        vertices, faces, vdens = _extract_device(ctx, field, grids["density"], iso)
+        ctx.check(ctx.lib.pb_map_vertices_f64(vertices.data_ptr(), vertices.shape[0], fmap.data_ptr(),
+                                              ctx.stream), "map vertices")
+    with _trace.stage("copy-out"):
+        v, f, d, iso_h = _host_all([vertices, faces, vdens, iso], device_out)
     return Mesh(v, f, d, float(iso_h[0]), float(stats.residual_norm))
 
 

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include "../../include/poisson_b200.h"
+#include "checked.cuh"
 
 namespace pb {
 

@@ -45,7 +45,7 @@ struct Pad {  // padded FP32 layout of the multigrid levels
     int n, P;
     int64_t plane;
     __device__ __forceinline__ int64_t at(int x, int y, int z) const {
-        return ((int64_t)(z + 1) * (n + 2) + (y + 1)) * P + (x + 4);
+        return checked_at(((int64_t)(z + 1) * (n + 2) + (y + 1)) * P + (x + 4), (int64_t)(n + 2) * plane, kSitePad);
     }
 };
 
@@ -283,9 +283,12 @@ __device__ __forceinline__ void update_residual_body(const float* __restrict__ z
             s += xb;
             s += xa;
             const int deg = degxy + (k > 0) + up;
-            pn[i] = (float)dm;
-            xn[i] = xm;
+            PB_GUARD(i, nn * n, kSiteFcgStore) {
+                pn[i] = (float)dm;
+                xn[i] = xm;
+            }
             const double r = bi - (((double)deg * h2 + pw * sc * h2) * xm - s * h2);
+            PB_GUARD(c, (int64_t)(n + 2) * g.plane, kSiteFcgStore)
             r32[c] = (float)r;
             v[0] += r * r;
             i += nn;
@@ -433,9 +436,12 @@ __device__ __forceinline__ void update_residual_prefetch_body(
             s += xb;
             s += xa;
             const int deg = degxy + (k > 0) + up;
-            pn[i] = (float)dm;
-            xn[i] = xm;
+            PB_GUARD(i, nn * n, kSiteFcgStore) {
+                pn[i] = (float)dm;
+                xn[i] = xm;
+            }
             const double r = bi - (((double)deg * h2 + pw * sc * h2) * xm - s * h2);
+            PB_GUARD(c, (int64_t)(n + 2) * g.plane, kSiteFcgStore)
             r32[c] = (float)r;
             v[0] += r * r;
             i += nn;

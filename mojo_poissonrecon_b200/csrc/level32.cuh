@@ -11,6 +11,8 @@
 
 #include <stdint.h>
 
+#include "checked.cuh"
+
 namespace pb {
 
 struct Geom {
@@ -18,7 +20,8 @@ struct Geom {
     int P;          // row pitch (floats)
     int64_t plane;  // (n+2)*P
     __host__ __device__ __forceinline__ int64_t at(int x, int y, int z) const {
-        return ((int64_t)(z + 1) * (n + 2) + (y + 1)) * P + (x + 4);
+        return checked_at(((int64_t)(z + 1) * (n + 2) + (y + 1)) * P + (x + 4), (int64_t)(n + 2) * plane,
+                          kSitePadded);
     }
 };
 

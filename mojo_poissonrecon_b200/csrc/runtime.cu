@@ -40,6 +40,37 @@ int64_t tuned(int param, int64_t n, int64_t fallback) {
 
 }  // namespace pb
 
+#ifdef PB_CHECKED
+namespace pb {
+__device__ unsigned long long g_check_word = 0;
+}
+#endif
+
+extern "C" int pb_checked_build(void) {
+#ifdef PB_CHECKED
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+extern "C" int pb_check_status(uint64_t* word, int clear) {
+    if (!word) return pb::fail(PB_ERR_INVALID, "check status: null output");
+    *word = 0;
+#ifdef PB_CHECKED
+    unsigned long long w = 0;
+    PB_CHECK_CUDA(cudaMemcpyFromSymbol(&w, pb::g_check_word, sizeof(w)), "check status: read");
+    *word = w;
+    if (clear) {
+        const unsigned long long zero = 0;
+        PB_CHECK_CUDA(cudaMemcpyToSymbol(pb::g_check_word, &zero, sizeof(zero)), "check status: clear");
+    }
+#else
+    (void)clear;
+#endif
+    return PB_OK;
+}
+
 extern "C" const char* pb_last_error(void) { return pb::g_last_error; }
 
 extern "C" int pb_version(void) { return 10000; }

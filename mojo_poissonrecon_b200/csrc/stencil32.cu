@@ -129,8 +129,9 @@ constexpr int kRrThreads = 256;
 // PAIRED: the two fine planes of a coarse plane are computed in one loop over
 // their 612 float4 items (three rounds of 256 threads instead of two rounds per
 // plane, 80 % of the lanes busy instead of 60 %); each item's arithmetic is the
-// same, so the results are too.
-template <bool PAIRED>
+// same, so the results are too.  THREADS = 320 (tuning variant 3, paired):
+// the 612 items in two rounds (96 % busy); the first 256 threads restrict.
+template <bool PAIRED, int THREADS = kRrThreads>
 __device__ __forceinline__ void residual_restrict32_body(const float* __restrict__ e, const float* __restrict__ rhs,
                                                          const float* __restrict__ D, const float* __restrict__ w,
                                                          Geom gf, float h2, float* __restrict__ coarse, Geom gc,
@@ -173,12 +174,12 @@ __device__ __forceinline__ void residual_restrict32_body(const float* __restrict
         }
     };
     auto fine_plane = [&](int f) {
-        for (int i = tid; i < kItems; i += kRrThreads) fine_item(f, i);
+        for (int i = tid; i < kItems; i += THREADS) fine_item(f, i);
     };
     fine_plane(2 * zc0 - 1);
     for (int zc = zc0; zc < zc1; ++zc) {
         if (PAIRED) {
-            for (int j = tid; j < 2 * kItems; j += kRrThreads) {
+            for (int j = tid; j < 2 * kItems; j += THREADS) {
                 const int second = j >= kItems;
                 fine_item(2 * zc + second, j - second * kItems);
             }
@@ -190,7 +191,7 @@ __device__ __forceinline__ void residual_restrict32_body(const float* __restrict
         {
             const int cy = tid / kRrCX, cx = tid - cy * kRrCX;  // 256 threads = the 64 x 4 coarse tile
             const int xc = xc0 + cx, yc = yc0 + cy;
-            if (xc < cn && yc < cn) {
+            if (cy < kRrCY && xc < cn && yc < cn) {
                 float sum = 0.0f;
 #pragma unroll
                 for (int oz = -1; oz <= 1; ++oz) {
@@ -228,6 +229,15 @@ __global__ void __launch_bounds__(kRrThreads) residual_restrict32_paired_kernel(
                                                                                  float h2, float* __restrict__ coarse,
                                                                                  Geom gc, int cz) {
     residual_restrict32_body<true>(e, rhs, D, w, gf, h2, coarse, gc, cz, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+__global__ void __launch_bounds__(320) residual_restrict32_paired320_kernel(const float* __restrict__ e,
+                                                                          const float* __restrict__ rhs,
+                                                                          const float* __restrict__ D,
+                                                                          const float* __restrict__ w, Geom gf,
+                                                                          float h2, float* __restrict__ coarse,
+                                                                          Geom gc, int cz) {
+    residual_restrict32_body<true, 320>(e, rhs, D, w, gf, h2, coarse, gc, cz, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Grouped (batch.cuh): ptr[0] e, ptr[1] rhs, ptr[2] D, ptr[3] weights, ptr[4] coarse rhs.
@@ -307,10 +317,12 @@ extern "C" int pb_residual_restrict_f32(const float* e, const float* rhs, const 
     const float h2 = (float)((n - 1) * (n - 1));
     const int cz = (int)tuned(PB_TUNE_RESTRICT_PLANES, n, kRrCZ);
     const dim3 grid((cn + kRrCX - 1) / kRrCX, (cn + kRrCY - 1) / kRrCY, (cn + cz - 1) / cz);
-    auto kernel = tuned(PB_TUNE_RESTRICT_VARIANT, n, 0) == 1 ? residual_restrict32_paired_kernel
-                                                              : residual_restrict32_kernel;
-    kernel<<<grid, kRrThreads, 0, (cudaStream_t)stream>>>(e, rhs, D, weights, geom((int)n), h2, coarse_rhs, geom(cn),
-                                                          cz);
+    const int64_t variant = tuned(PB_TUNE_RESTRICT_VARIANT, n, 0);
+    auto kernel = variant == 1 ? residual_restrict32_paired_kernel
+                  : variant == 3 ? residual_restrict32_paired320_kernel
+                                 : residual_restrict32_kernel;
+    kernel<<<grid, variant == 3 ? 320 : kRrThreads, 0, (cudaStream_t)stream>>>(e, rhs, D, weights, geom((int)n), h2,
+                                                                               coarse_rhs, geom(cn), cz);
     PB_CHECK_LAUNCH("residual_restrict32_kernel");
     return PB_OK;
 }

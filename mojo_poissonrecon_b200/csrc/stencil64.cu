@@ -83,6 +83,7 @@ __global__ void relax_colour_kernel(double* __restrict__ sol, const double* __re
         const double s = neighbour_sum(sol, idx, x, y, z, n, degree);
         const double screening = point_weight * screen[idx] * h_inv2;
         const double diagonal = (double)degree * h_inv2 + screening;
+        PB_GUARD(idx, n * n * n, kSiteRelax64)
         if (diagonal > 1.0e-30) sol[idx] = (rhs[idx] + s * h_inv2) / diagonal;
     }
 }

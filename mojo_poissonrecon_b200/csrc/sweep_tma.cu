@@ -270,8 +270,10 @@ __device__ __forceinline__ void sweep_body(const CUtensorMap* map_e, const CUten
             float o[4] = {c.x, c.y, c.z, c.w};
 #pragma unroll
             for (int j = 0; j < 4; ++j) o[j] = ((j & 1) == s) ? v[j] : o[j];
-            float* dst = p.e_out + ((int64_t)(z + 1) * (n + 2) + (y0 - 1 + br)) * p.P + (x0 + 4 * g);
+            const int64_t oi = ((int64_t)(z + 1) * (n + 2) + (y0 - 1 + br)) * p.P + (x0 + 4 * g);
+            float* dst = p.e_out + oi;
             const int valid = W + 4 - 4 * g;
+            PB_GUARD(oi + (valid < 4 ? valid : 4) - 1, (int64_t)(n + 2) * p.plane, kSiteSweepStore)
             if (valid >= 4) {
                 *reinterpret_cast<float4*>(dst) = make_float4(o[0], o[1], o[2], o[3]);
             } else {
@@ -572,6 +574,7 @@ __device__ __forceinline__ void prolong_add32_body(const float* __restrict__ c, 
         // x interpolation: t = 0 on even x, 1/2 on odd x (coarse 2k + 2 only weighs odd x < n - 1)
         const float v0 = q[0], v1 = q[0] * 0.5f + q[1] * 0.5f, v2 = q[1], v3 = q[1] * 0.5f + q[2] * 0.5f;
         const int64_t p = ((int64_t)(z + 1) * (n + 2) + (y + 1)) * P + (x + 4);
+        PB_GUARD(p + (valid < 4 ? valid : 4) - 1, (int64_t)(n + 2) * (n + 2) * P, kSiteProlong)
         if (valid == 4) {
             float4 e = *reinterpret_cast<const float4*>(f + p);
             const float4 s = *reinterpret_cast<const float4*>(w + p);

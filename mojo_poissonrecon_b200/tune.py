@@ -75,7 +75,7 @@ def candidates(param: int, n: int) -> list[int]:
     if param == SWEEP_VARIANT:
         return list(range(9))
     if param == RESTRICT_VARIANT:
-        return [0, 1, 2]
+        return [0, 1, 2, 3]
     if param in (RELAX27_VARIANT, RESIDUAL27_VARIANT):
         return [0, 1]
     raise ValueError(f"unknown tuning parameter {param}")

@@ -233,7 +233,7 @@ def test_residual_restrict_variants_bit_identical(L, n):
     L.pb_tune_clear()
     try:
         want = run()
-        for variant in (0, 1):
+        for variant in (0, 1, 3):
             for planes in (0, 1, 3, 8):
                 L.pb_tune_set(tune.RESTRICT_VARIANT, n, variant)
                 L.pb_tune_set(tune.RESTRICT_PLANES, n, planes)

@@ -140,3 +140,29 @@ def test_batch_descriptors_reject_bad_grids():
     assert _describe(lib, 99, [9], [fake])[0] == 1
     assert _describe(lib, 4, [17], [fake[:7]], clouds=[-1])[0] == 1
     assert lib.pb_batch_launch(4, None, 1, 1, None, 0, None) == 1
+
+
+def test_checked_build_exports_the_same_symbols():
+    """The bounds-checked variant (libpoisson_b200_checked.so) exports every
+    declared symbol and says it is the checked build; the normal library says
+    it is not and reports a clear check word without touching a device."""
+    from mojo_poissonrecon_b200 import _native, buildlib
+
+    if not os.path.exists(buildlib.CHECKED_LIBRARY):
+        pytest.skip("checked library not built (python -m mojo_poissonrecon_b200.buildlib --checked)")
+    checked = ctypes.CDLL(buildlib.CHECKED_LIBRARY)
+    missing = [s for s in declared_symbols() if not hasattr(checked, s)]
+    assert not missing, missing
+    assert checked.pb_checked_build() == 1
+    lib = _native.lib()
+    assert lib.pb_checked_build() == (1 if _native.CHECKED else 0)
+    if not _native.CHECKED:
+        assert _native.check_word() == 0
+
+
+def test_check_word_decoding():
+    from mojo_poissonrecon_b200 import _native
+
+    site, index = _native.decode_check_word((3 << 56) | 12345)
+    assert (site, index) == (3, 12345)
+    assert _native.decode_check_word(0) == (0, 0)

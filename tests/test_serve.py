@@ -340,3 +340,28 @@ def test_on_result_replaces_the_result():
     f = server.submit(*cloud(), depth=6, tag=5)
     assert f.result(timeout=10)[0] == 11
     server.close()
+
+
+def test_nvtx_stages_push_and_pop(monkeypatch):
+    """With tracing on, a stage pushes one NVTX range and pops it, also when
+    the stage raises; with tracing off it touches nothing."""
+    import torch
+
+    from mojo_poissonrecon_b200 import _trace
+
+    calls = []
+    monkeypatch.setattr(torch.cuda.nvtx, "range_push", lambda name: calls.append(("push", name)))
+    monkeypatch.setattr(torch.cuda.nvtx, "range_pop", lambda: calls.append(("pop",)))
+    monkeypatch.setattr(_trace, "ENABLED", False)
+    with _trace.stage("solve"):
+        pass
+    assert calls == []
+    monkeypatch.setattr(_trace, "ENABLED", True)
+    with _trace.stage("solve"):
+        pass
+    try:
+        with _trace.stage("extract"):
+            raise ValueError("x")
+    except ValueError:
+        pass
+    assert calls == [("push", "mpr:solve"), ("pop",), ("push", "mpr:extract"), ("pop",)]
