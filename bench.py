@@ -315,8 +315,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
                 "algorithmic_bytes": int(algorithmic), "achieved_gbs": round(gbs, 1),
                 "frac_of_measured_hbm": round(gbs / hbm_peak()[0], 3),
                 "timing": "CUDA events around each finest-level sweep of 5 eager V-cycles"})
-            if sweep_variant in (0, 1, 2):  # the committed capture is of sweep_kernel
-                kernel_table[0]["traffic"] = read_profile_traffic(SWEEP_PROFILE)
+            # the committed capture is of variant 7; every variant loads the same boxes
+            kernel_table[0]["traffic"] = read_profile_traffic(SWEEP_PROFILE)
         # the dominant kernel of the launch list (profiles/launches_refined_d8.md)
         top = next(k for k in kernel_table if k["kernel"].startswith("fcg::update_residual"))
         peak, peak_src = hbm_peak()
