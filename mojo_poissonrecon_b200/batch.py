@@ -34,6 +34,7 @@ cloud, and every kernel is deterministic.
 from __future__ import annotations
 
 import collections
+import concurrent.futures
 import ctypes
 import math
 import threading
@@ -127,6 +128,40 @@ def _stream(device: torch.device) -> torch.cuda.Stream:
     return table[device.index]
 
 
+# The per-cloud prologue (hierarchy set-up, x0 and its residual, ||b||) is ~50 small
+# launches per cloud; PROLOGUE_LANES host threads issue it on as many streams, each
+# with its own scratch, so the launches of different clouds overlap on the host and
+# on the device.  Only where one Galerkin scratch is at most PROLOGUE_SCRATCH bytes.
+PROLOGUE_LANES = 4
+PROLOGUE_SCRATCH = 256 << 20
+_PROLOGUE_POOL = concurrent.futures.ThreadPoolExecutor(max_workers=PROLOGUE_LANES,
+                                                       thread_name_prefix="mpr-prologue")
+
+
+def _lane_streams(device: torch.device, count: int) -> list:
+    """This thread's prologue streams on `device` (kept for the life of the thread)."""
+    table = getattr(_STREAMS, "lanes", None)
+    if table is None:
+        table = _STREAMS.lanes = {}
+    lanes = table.setdefault(device.index, [])
+    while len(lanes) < count:
+        lanes.append(torch.cuda.Stream(device=device))
+    return lanes[:count]
+
+
+class _PrologueLane:
+    """One prologue lane's stream and scratch (Galerkin, defect, norm)."""
+
+    def __init__(self, lib, device: torch.device, stream: torch.cuda.Stream, galerkin_ws: torch.Tensor,
+                 defect_bytes: int):
+        self.stream = stream
+        self.galerkin_ws = galerkin_ws
+        self.defect_ws = nat.Workspace(device)
+        self.defect_ptr, self.defect_size = self.defect_ws.get(defect_bytes)
+        self.norm_ws = nat.Workspace(device)
+        self.norm_ws.get(1 << 16)
+
+
 def _take_cloud(n: int, device: torch.device, galerkin_ws: torch.Tensor) -> _Cloud:
     with _POOL_LOCK:
         for key, c in _POOL.items():
@@ -193,10 +228,14 @@ class BatchSolver:
             self.part_offsets = np.concatenate([[0], np.cumsum(parts)]).astype(np.int64)
             self.partials = torch.zeros(int(self.part_offsets[-1]), dtype=torch.float64, device=self.device)
             defect = max(int(self.lib.pb_defect_workspace_size(n)) for n in set(self.sides))
-            self.defect_ws = nat.Workspace(self.device)
-            self.defect_ptr, self.defect_size = self.defect_ws.get(defect)
-            self.norm_ws = nat.Workspace(self.device)
-            self.norm_ws.get(1 << 16)
+            lanes = min(PROLOGUE_LANES, K) if scratch <= PROLOGUE_SCRATCH else 1
+            streams = [self.stream] if lanes == 1 else _lane_streams(self.device, lanes)
+            self.lanes = [_PrologueLane(self.lib, self.device, streams[0], self.galerkin_ws, defect)]
+            for j in range(1, lanes):
+                ws = torch.empty_like(self.galerkin_ws)
+                self.lanes.append(_PrologueLane(self.lib, self.device, streams[j], ws, defect))
+            for k, c in enumerate(self.clouds):  # cloud k's set-up runs on lane k % lanes
+                c.h.galerkin_ws = self.lanes[k % lanes].galerkin_ws
         self.graph = ctypes.c_void_p()
         self.exec = ctypes.c_void_p()
         self.body_launches = 0
@@ -358,19 +397,47 @@ class BatchSolver:
         caller.wait_stream(self.stream)
         return [x.clone() for x in xs], stats  # on the caller's stream
 
+    def _prologue_lane(self, j: int, start: torch.cuda.Event, rhs, screen, pws) -> None:
+        """Lane j's clouds (k = j, j + lanes, ...): levels' set-up, x0 = 0.5 and its
+        residual, ||b||; on the lane's stream, after `start`."""
+        L, lane = self.lib, self.lanes[j]
+        if lane.stream is not self.stream:
+            lane.stream.wait_event(start)
+        with torch.cuda.device(self.device), torch.cuda.stream(lane.stream):  # a worker thread's device too
+            s = nat.stream_handle()
+            for k in range(j, len(self.clouds), len(self.lanes)):
+                c = self.clouds[k]
+                c.h.setup(screen[k], pws[k])
+                x0 = c.xs[0]
+                nat.check(L.pb_fill_f64(x0.data_ptr(), x0.numel(), 0.5, s), "fill")  # core.py:270
+                nat.check(L.pb_defect_f64(x0.data_ptr(), None, None, rhs[k].data_ptr(), screen[k].data_ptr(),
+                                          c.n, pws[k], c.h.levels[0].rhs.data_ptr(), None,
+                                          self.norm2[k:k + 1].data_ptr(), lane.defect_ptr, lane.defect_size, s),
+                          "defect")
+                norm(rhs[k], lane.norm_ws, self.bnorm[k:k + 1])
+
+    def _prologue(self, rhs, screen, pws) -> None:
+        """Every cloud's prologue, spread over the prologue lanes (host threads
+        and streams), then joined back into the solver's stream."""
+        if len(self.lanes) == 1:
+            self._prologue_lane(0, None, rhs, screen, pws)
+            return
+        start = torch.cuda.Event()
+        start.record(self.stream)
+        jobs = [_PROLOGUE_POOL.submit(self._prologue_lane, j, start, rhs, screen, pws)
+                for j in range(len(self.lanes))]
+        errors = [f.exception() for f in jobs]
+        for lane in self.lanes:  # join every lane, also after an error
+            self.stream.wait_stream(lane.stream)
+        for e in errors:
+            if e is not None:
+                raise e
+
     def _solve(self, rhs, screen, pws, tol, max_cycles, phases=None):
         mark = phases.mark if phases is not None else (lambda name: None)
         L, s = self.lib, nat.stream_handle()
         K = len(self.clouds)
-        # prologue per cloud: levels' set-up, x0 = 0.5 and its residual, ||b||
-        for k, c in enumerate(self.clouds):
-            c.h.setup(screen[k], pws[k])
-            x0 = c.xs[0]
-            nat.check(L.pb_fill_f64(x0.data_ptr(), x0.numel(), 0.5, s), "fill")  # core.py:270
-            nat.check(L.pb_defect_f64(x0.data_ptr(), None, None, rhs[k].data_ptr(), screen[k].data_ptr(), c.n,
-                                      pws[k], c.h.levels[0].rhs.data_ptr(), None, self.norm2[k:k + 1].data_ptr(),
-                                      self.defect_ptr, self.defect_size, s), "defect")
-            norm(rhs[k], self.norm_ws, self.bnorm[k:k + 1])
+        self._prologue(rhs, screen, pws)
         # per-cloud control on the device: target ||r||^2, cap; active while above target
         target = tol * self.bnorm  # ||b|| (not squared), as the single-cloud engine forms it
         target2 = target * target
